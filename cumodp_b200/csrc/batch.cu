@@ -1,0 +1,462 @@
+// Batched products of uneven degree: size classes, autotuned splits, and one
+// CUDA-graph launch per batch.
+//
+// The reference batches only same-size items (list_stockham_dev,
+// src/list_stockham.cu:595-630, one root and one n for all m items, with the
+// geometry in __constant__ globals), and a list product is explicit pad +
+// list NTTs + list_pointwise_mul + list inverse + shrink
+// (src/list_pointwise_mul.cu:43-194), each a separate synchronised launch.
+// Here a batch of any degrees is planned once per shape:
+//   * products are grouped by transform length n = 2^ceil(log2(la+lb-1));
+//   * a class with n <= 2^14 is one launch of the fused single-CTA kernel
+//     (several products per CTA below 2^12);
+//   * a larger class is the three-pass product over all its jobs at once,
+//     with the column/row split chosen by the autotuner;
+//   * every class runs on its own branch of one CUDA graph (classes are
+//     independent, so their kernels overlap on the device), captured once and
+//     replayed; job tables live in device memory and are refreshed with one
+//     copy when the caller's pointers change.
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <unordered_map>
+
+#include "../../include/cumodp.h"
+#include "product.cuh"
+
+namespace cmb {
+
+// ------------------------------------------------------------ autotuner ----
+// Chooses the row length 2^l2 of the three-pass split for a size class by
+// timing each legal split on a synthetic class of the same shape.  Results
+// are cached per (device, logn, job bucket) in memory and, when
+// CUMODP_TUNE_FILE names a file, appended to it and reloaded at start-up.
+namespace {
+
+struct TuneKey {
+    int dev, logn, bucket;
+    bool operator<(const TuneKey& o) const {
+        return std::tie(dev, logn, bucket) < std::tie(o.dev, o.logn, o.bucket);
+    }
+};
+
+std::mutex g_tune_m;
+std::map<TuneKey, int> g_tune;
+bool g_tune_loaded = false;
+
+int job_bucket(int njobs) {
+    int b = 1;
+    while (b < njobs && b < 256) b <<= 1;
+    return b;
+}
+
+void tune_load_locked() {
+    if (g_tune_loaded) return;
+    g_tune_loaded = true;
+    const char* f = getenv("CUMODP_TUNE_FILE");
+    if (!f) return;
+    FILE* fh = fopen(f, "r");
+    if (!fh) return;
+    int dev, logn, bucket, l2;
+    while (fscanf(fh, "%d %d %d %d", &dev, &logn, &bucket, &l2) == 4) g_tune[TuneKey{dev, logn, bucket}] = l2;
+    fclose(fh);
+}
+
+}  // namespace
+
+std::vector<int> legal_row_logs(int logn) {
+    std::vector<int> v;
+    for (int l2 = kMinRowLog; l2 <= kMaxRowLog; ++l2) {
+        const int l1 = logn - l2;
+        if (l1 >= 1 && l1 <= kMaxColLog) v.push_back(l2);
+    }
+    return v;
+}
+
+int tune_row_log(const PrimeCtx& pc, int logn, int njobs, int dev, cudaStream_t st) {
+    const char* off = getenv("CUMODP_AUTOTUNE");
+    if (off && off[0] == '0') return default_row_log(logn);
+    const TuneKey key{dev, logn, job_bucket(njobs)};
+    {
+        std::lock_guard<std::mutex> g(g_tune_m);
+        tune_load_locked();
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) return it->second;
+    }
+    const std::vector<int> cands = legal_row_logs(logn);
+    if (cands.size() <= 1) return cands.empty() ? default_row_log(logn) : cands[0];
+    // synthetic class: `jobs` products of two length-n/2 operands
+    const int jobs = std::min(key.bucket, 32);
+    const long long n = 1ll << logn;
+    int err = OK;
+    u32* buf = nullptr;
+    LargeJob* djobs = nullptr;
+    if (cudaMalloc(&buf, (size_t)jobs * 4 * n * sizeof(u32)) != cudaSuccess ||
+        cudaMalloc(&djobs, jobs * sizeof(LargeJob)) != cudaSuccess) {
+        cudaGetLastError();
+        if (buf) cudaFree(buf);
+        return default_row_log(logn);
+    }
+    cudaMemsetAsync(buf, 0, (size_t)jobs * 4 * n * sizeof(u32), st);
+    std::vector<LargeJob> hj(jobs);
+    for (int j = 0; j < jobs; ++j) {
+        u32* base = buf + (size_t)j * 4 * n;
+        hj[j] = LargeJob{base, base + n / 2, base + n, (int)(n / 2), (int)(n / 2), (int)(n - 1), 0,
+                         base + 2 * n, base + 3 * n};
+    }
+    cudaMemcpyAsync(djobs, hj.data(), jobs * sizeof(LargeJob), cudaMemcpyHostToDevice, st);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int best = default_row_log(logn);
+    float best_ms = 1e30f;
+    const u32 root = canonical_root(pc, logn);
+    for (int l2 : cands) {
+        LargeArgs A;
+        if (large_args(pc, root, logn, l2, dev, &A) != OK) continue;
+        A.jobs = djobs;
+        A.njobs = jobs;
+        launch_large(A, jobs, st);  // warm-up
+        cudaEventRecord(e0, st);
+        for (int r = 0; r < 3; ++r) launch_large(A, jobs, st);
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (cudaGetLastError() == cudaSuccess && ms < best_ms) {
+            best_ms = ms;
+            best = l2;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(buf);
+    cudaFree(djobs);
+    (void)err;
+    std::lock_guard<std::mutex> g(g_tune_m);
+    g_tune[key] = best;
+    if (const char* f = getenv("CUMODP_TUNE_FILE")) {
+        if (FILE* fh = fopen(f, "a")) {
+            fprintf(fh, "%d %d %d %d\n", key.dev, key.logn, key.bucket, best);
+            fclose(fh);
+        }
+    }
+    return best;
+}
+
+// --------------------------------------------------------------- plans ----
+namespace {
+
+struct ClassPlan {
+    int logn = 0;
+    bool large = false;
+    int l2 = 0;
+    std::vector<int> members;  // job indices of the batch
+    size_t job_off = 0;        // byte offset of this class's job table
+    size_t ws_off = 0;         // word offset of this class's workspace (large)
+};
+
+struct BatchPlan {
+    u32 p = 0;
+    int dev = 0;
+    std::vector<long long> la, lb;
+    std::vector<ClassPlan> classes;
+    void* djobs = nullptr;     // device job tables
+    size_t jobs_bytes = 0;
+    std::vector<unsigned char> hjobs;  // host copy of what djobs holds
+    u32* ws = nullptr;
+    size_t ws_words = 0;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<cudaStream_t> side;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> joins;
+    size_t bytes = 0;
+
+    ~BatchPlan() {
+        if (exec) cudaGraphExecDestroy(exec);
+        for (auto s : side) cudaStreamDestroy(s);
+        if (fork) cudaEventDestroy(fork);
+        for (auto e : joins) cudaEventDestroy(e);
+        if (djobs) cudaFree(djobs);
+        if (ws) cudaFree(ws);
+        account_bytes(-(long long)bytes);
+    }
+};
+
+struct PlanCache {
+    std::mutex m;
+    std::unordered_map<size_t, std::unique_ptr<BatchPlan>> plans;
+};
+PlanCache& plan_cache() {
+    static PlanCache* c = new PlanCache();
+    return *c;
+}
+
+size_t shape_hash(u32 p, int dev, const std::vector<long long>& la, const std::vector<long long>& lb) {
+    size_t h = 1469598103934665603ull ^ p ^ ((size_t)dev << 40);
+    for (size_t i = 0; i < la.size(); ++i) {
+        h = (h ^ (size_t)la[i]) * 1099511628211ull;
+        h = (h ^ (size_t)lb[i]) * 1099511628211ull;
+    }
+    return h;
+}
+
+int build_plan(BatchPlan& P, const PrimeCtx& pc, cudaStream_t st) {
+    std::map<int, ClassPlan> by;
+    for (size_t i = 0; i < P.la.size(); ++i) {
+        const int logn = product_logn(P.la[i], P.lb[i]);
+        if (logn > pc.info.two_adic || logn > kMaxLog) return FFT_SIZE_TOO_LARGE;
+        ClassPlan& c = by[logn];
+        c.logn = logn;
+        c.large = logn > kMaxSmallLog;
+        c.members.push_back((int)i);
+    }
+    size_t jb = 0, ws = 0;
+    for (auto& kv : by) {
+        ClassPlan c = kv.second;
+        c.job_off = jb;
+        jb += c.members.size() * (c.large ? sizeof(LargeJob) : sizeof(ProdJob));
+        jb = (jb + 255) & ~(size_t)255;
+        if (c.large) {
+            c.l2 = tune_row_log(pc, c.logn, (int)c.members.size(), P.dev, st);
+            c.ws_off = ws;
+            ws += c.members.size() * (2ull << c.logn);
+        }
+        P.classes.push_back(c);
+    }
+    P.jobs_bytes = std::max<size_t>(jb, 256);
+    if (cudaMalloc(&P.djobs, P.jobs_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return OUT_OF_MEMORY;
+    }
+    P.bytes += P.jobs_bytes;
+    P.hjobs.assign(P.jobs_bytes, 0);
+    P.ws_words = ws;
+    if (ws) {
+        if (cudaMalloc(&P.ws, ws * sizeof(u32)) != cudaSuccess) {
+            cudaGetLastError();
+            return OUT_OF_MEMORY;
+        }
+        P.bytes += ws * sizeof(u32);
+    }
+    account_bytes((long long)P.bytes);
+    return OK;
+}
+
+// Everything graph capture must not do itself: branch streams and events,
+// twiddle tables (they are allocated and uploaded on first use).
+int prepare_capture(BatchPlan& P, const PrimeCtx& pc) {
+    if (!P.fork) {
+        cudaEventCreateWithFlags(&P.fork, cudaEventDisableTiming);
+        for (size_t i = 0; i < P.classes.size(); ++i) {
+            cudaStream_t s;
+            cudaEvent_t e;
+            cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+            cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+            P.side.push_back(s);
+            P.joins.push_back(e);
+        }
+    }
+    for (const ClassPlan& c : P.classes) {
+        const u32 root = canonical_root(pc, c.logn);
+        int err = OK;
+        if (!c.large) {
+            SmallArgs A;
+            err = small_args(pc, root, c.logn, P.dev, &A);
+        } else {
+            LargeArgs A;
+            err = large_args(pc, root, c.logn, c.l2, P.dev, &A);
+        }
+        if (err != OK) return err;
+    }
+    return OK;
+}
+
+// Enqueue every class on its own branch (fork/join through events).
+int enqueue_classes(BatchPlan& P, const PrimeCtx& pc, cudaStream_t st) {
+    int err = OK;
+    cudaEventRecord(P.fork, st);
+    for (size_t ci = 0; ci < P.classes.size(); ++ci) {
+        const ClassPlan& c = P.classes[ci];
+        cudaStream_t s = P.side[ci];
+        cudaStreamWaitEvent(s, P.fork, 0);
+        const u32 root = canonical_root(pc, c.logn);
+        if (!c.large) {
+            SmallArgs A;
+            if ((err = small_args(pc, root, c.logn, P.dev, &A)) != OK) return err;
+            A.jobs = (const ProdJob*)((char*)P.djobs + c.job_off);
+            A.njobs = (int)c.members.size();
+            launch_small(c.logn, A, A.njobs, s);
+        } else {
+            LargeArgs A;
+            if ((err = large_args(pc, root, c.logn, c.l2, P.dev, &A)) != OK) return err;
+            A.jobs = (const LargeJob*)((char*)P.djobs + c.job_off);
+            A.njobs = (int)c.members.size();
+            launch_large(A, A.njobs, s);
+        }
+        cudaEventRecord(P.joins[ci], s);
+        cudaStreamWaitEvent(st, P.joins[ci], 0);
+    }
+    return cuda_err(cudaGetLastError());
+}
+
+// Host job tables for the current pointers.
+void fill_jobs(BatchPlan& P, const u32* F, const int64_t* f_off, const u32* G, const int64_t* g_off, u32* H,
+               const int64_t* h_off, std::vector<unsigned char>& out) {
+    out.assign(P.jobs_bytes, 0);
+    for (const ClassPlan& c : P.classes) {
+        for (size_t k = 0; k < c.members.size(); ++k) {
+            const int i = c.members[k];
+            const int la = (int)P.la[i], lb = (int)P.lb[i], lh = la + lb - 1;
+            if (!c.large) {
+                ProdJob j{F + f_off[i], G + g_off[i], H + h_off[i], la, lb, lh, 0};
+                memcpy(out.data() + c.job_off + k * sizeof(ProdJob), &j, sizeof(j));
+            } else {
+                const size_t n = (size_t)1 << c.logn;
+                u32* w = P.ws + c.ws_off + k * 2 * n;
+                LargeJob j{F + f_off[i], G + g_off[i], H + h_off[i], la, lb, lh, 0, w, w + n};
+                memcpy(out.data() + c.job_off + k * sizeof(LargeJob), &j, sizeof(j));
+            }
+        }
+    }
+}
+
+}  // namespace
+
+int batch_mul_dev(int count, const sfixn* df, const int64_t* f_off, const u32* F, const sfixn* dg,
+                  const int64_t* g_off, const u32* G, const int64_t* h_off, u32* H, u32 p, cudaStream_t st) {
+    if (count < 0) return ASSUMPTION_ERROR;
+    if (count == 0) return OK;
+    if (!df || !dg || !f_off || !g_off || !h_off || !F || !G || !H) return ASSUMPTION_ERROR;
+    int err = OK;
+    const PrimeCtx* pc = prime_ctx(p, &err);
+    if (!pc) return err;
+    std::vector<long long> la(count), lb(count);
+    for (int i = 0; i < count; ++i) {
+        if (df[i] < 0 || dg[i] < 0) return ASSUMPTION_ERROR;
+        la[i] = (long long)df[i] + 1;
+        lb[i] = (long long)dg[i] + 1;
+    }
+    const int dev = current_device();
+    PlanCache& PC = plan_cache();
+    std::lock_guard<std::mutex> g(PC.m);
+    const size_t key = shape_hash(p, dev, la, lb);
+    auto it = PC.plans.find(key);
+    BatchPlan* P = nullptr;
+    if (it != PC.plans.end() && it->second->p == p && it->second->dev == dev && it->second->la == la &&
+        it->second->lb == lb) {
+        P = it->second.get();
+    } else {
+        if (PC.plans.size() >= 64) PC.plans.clear();  // bounded cache of batch shapes
+        std::unique_ptr<BatchPlan> np(new BatchPlan());
+        np->p = p;
+        np->dev = dev;
+        np->la = la;
+        np->lb = lb;
+        if ((err = build_plan(*np, *pc, st)) != OK) return err;
+        P = np.get();
+        PC.plans[key] = std::move(np);
+    }
+    std::vector<unsigned char> hj;
+    fill_jobs(*P, F, f_off, G, g_off, H, h_off, hj);
+    if (hj != P->hjobs) {
+        P->hjobs.swap(hj);
+        // pageable source: the call returns once the bytes are staged
+        cudaError_t ce = cudaMemcpyAsync(P->djobs, P->hjobs.data(), P->jobs_bytes, cudaMemcpyHostToDevice, st);
+        if (ce != cudaSuccess) return cuda_err(ce);
+    }
+    if (!P->exec) {
+        ensure_kernel_attrs();
+        if ((err = prepare_capture(*P, *pc)) != OK) return err;
+        cudaStream_t cap;
+        cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking);
+        cudaGraph_t graph;
+        cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+        err = enqueue_classes(*P, *pc, cap);
+        cudaError_t ce = cudaStreamEndCapture(cap, &graph);
+        cudaStreamDestroy(cap);
+        if (err != OK) return err;
+        if (ce != cudaSuccess) return cuda_err(ce);
+        ce = cudaGraphInstantiate(&P->exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) {
+            P->exec = nullptr;
+            return cuda_err(ce);
+        }
+    }
+    return cuda_err(cudaGraphLaunch(P->exec, st));
+}
+
+// Kernel launches one batch issues (for reporting).
+int batch_launch_count(int count, const sfixn* df, const sfixn* dg) {
+    std::map<int, int> cls;
+    for (int i = 0; i < count; ++i) cls[product_logn((long long)df[i] + 1, (long long)dg[i] + 1)]++;
+    int n = 0;
+    for (auto& kv : cls) n += kv.first > kMaxSmallLog ? 3 : 1;
+    return n;
+}
+
+}  // namespace cmb
+
+using namespace cmb;
+
+extern "C" {
+
+cumodp_err cumodp_fftmul_batch_dev(int count, const sfixn* df, const int64_t* f_off, const sfixn* F,
+                                   const sfixn* dg, const int64_t* g_off, const sfixn* G, const int64_t* h_off,
+                                   sfixn* H, sfixn p, void* stream) {
+    int cnt = 0;
+    if (cudaGetDeviceCount(&cnt) != cudaSuccess || cnt == 0) {
+        cudaGetLastError();
+        return CUMODP_NO_CUDA_DEVICE;
+    }
+    std::lock_guard<std::mutex> g(lib_mutex());
+    cudaStream_t st = stream ? (cudaStream_t)stream : lib_stream(current_device());
+    int e = batch_mul_dev(count, df, f_off, (const u32*)F, dg, g_off, (const u32*)G, h_off, (u32*)H, (u32)p, st);
+    if (e == OK && !stream) e = cuda_err(cudaStreamSynchronize(st));
+    return (cumodp_err)e;
+}
+
+cumodp_err cumodp_fftmul_batch(int count, const sfixn* df, const int64_t* f_off, const sfixn* F,
+                               const sfixn* dg, const int64_t* g_off, const sfixn* G, const int64_t* h_off,
+                               sfixn* H, sfixn p) {
+    int cnt = 0;
+    if (cudaGetDeviceCount(&cnt) != cudaSuccess || cnt == 0) {
+        cudaGetLastError();
+        return CUMODP_NO_CUDA_DEVICE;
+    }
+    if (count < 0 || (count > 0 && (!df || !dg || !f_off || !g_off || !h_off || !F || !G || !H)))
+        return CUMODP_ASSUMPTION_ERROR;
+    if (count == 0) return CUMODP_SUCCESS;
+    std::lock_guard<std::mutex> g(lib_mutex());
+    const int dev = current_device();
+    cudaStream_t st = lib_stream(dev);
+    // extents of the three host arrays
+    size_t nf = 0, ng = 0, nh = 0;
+    for (int i = 0; i < count; ++i) {
+        if (df[i] < 0 || dg[i] < 0 || f_off[i] < 0 || g_off[i] < 0 || h_off[i] < 0) return CUMODP_ASSUMPTION_ERROR;
+        nf = std::max(nf, (size_t)f_off[i] + df[i] + 1);
+        ng = std::max(ng, (size_t)g_off[i] + dg[i] + 1);
+        nh = std::max(nh, (size_t)h_off[i] + df[i] + dg[i] + 1);
+    }
+    int err = OK;
+    u32* d = (u32*)workspace(dev, kWsBatch, (nf + ng + nh) * sizeof(u32), &err);
+    if (!d) return (cumodp_err)err;
+    u32 *dF = d, *dG = d + nf, *dH = d + nf + ng;
+    cudaError_t ce = cudaMemcpyAsync(dF, F, nf * 4, cudaMemcpyHostToDevice, st);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(dG, G, ng * 4, cudaMemcpyHostToDevice, st);
+    if (ce != cudaSuccess) return (cumodp_err)cuda_err(ce);
+    err = batch_mul_dev(count, df, f_off, dF, dg, g_off, dG, h_off, dH, (u32)p, st);
+    if (err != OK) {
+        cudaStreamSynchronize(st);
+        return (cumodp_err)err;
+    }
+    ce = cudaMemcpyAsync(H, dH, nh * 4, cudaMemcpyDeviceToHost, st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    return (cumodp_err)cuda_err(ce);
+}
+
+}  // extern "C"

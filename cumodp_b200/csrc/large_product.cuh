@@ -1,0 +1,322 @@
+// Three-pass product for transform lengths n = n1 * n2 > 2^14.
+//
+// The reference runs log2(n) radix-2 Stockham steps, each three HBM round
+// trips (src/stockham.cu:437-453).  Here the length-n transform is the
+// four-step split x[r*n2 + c]: a length-n1 DFT down every column, a twiddle
+// w_n^(c*k1), and a length-n2 DFT along every row.  The whole product needs
+// three passes over HBM:
+//   A  k_col_fwd    column DFTs of both operands (tile of 32 columns x n1
+//                   rows in shared memory; the zero pad is never read);
+//   B  k_row_fused  per row: twiddle, row DFT of both operands, pointwise
+//                   product, inverse row DFT, inverse twiddle with the 1/n
+//                   scale folded in;
+//   C  k_col_inv    inverse column DFTs, truncation, canonical residues.
+// Rows leave pass A in digit-reversed order of k1 and are consumed in that
+// order by passes B and C, so nothing is ever permuted.
+#pragma once
+#include "small_product.cuh"
+
+namespace cmb {
+
+struct LargeJob {
+    const u32* a;
+    const u32* b;
+    u32* h;
+    int la, lb, lh;
+    int pad;
+    u32* wa;  // workspace, n words: column spectra of a, then the row pass output
+    u32* wb;  // workspace, n words: column spectra of b
+};
+
+struct LargeArgs {
+    PrimeK pk;                   // row transform constants (root w_n2)
+    PrimeK pkc;                  // column transform constants (root w_n1)
+    const Tw* __restrict__ twr;  // row plan tables (length n2)
+    const Tw* __restrict__ twc;  // column plan tables (length n1)
+    int twr_inv, twc_inv;        // inverse table offsets
+    const u32* __restrict__ seeds;  // w_n^e * 2^32 mod p: lo_f, hi_f, lo_i, hi_i
+    int nlo, nhi;
+    u32 scale_rn;                // 2^32 / n mod p
+    int l1, l2;                  // n1 = 2^l1 (columns), n2 = 2^l2 (rows)
+    const LargeJob* __restrict__ jobs;  // device job table, or nullptr: use job0
+    int njobs;
+    LevelPlan colpl;             // column plan (row slot -> k1 map)
+    LargeJob job0;
+};
+
+#ifdef __CUDACC__
+
+template <int LOGL, int LEV>
+struct ColLevel {
+    static constexpr LevelPlan PL = col_plan(LOGL);
+    static constexpr int R = 1 << PL.logr[LEV];
+    static constexpr int LOGB = [] {
+        int lb = LOGL;
+        for (int i = 0; i < LEV; ++i) lb -= PL.logr[i];
+        return lb;
+    }();
+    static constexpr int B = 1 << LOGB;
+    static constexpr int TB = B / R;
+    static constexpr int TWOFF = [] {
+        int n = 0, lb = LOGL;
+        for (int i = 0; i < LEV; ++i) { n += 1 << lb; lb -= PL.logr[i]; }
+        return n;
+    }();
+};
+
+// Row slot -> frequency index k1 of the column transform (digit reversal of
+// the column plan).
+__device__ __forceinline__ u32 col_slot_to_k1(u32 s, const LevelPlan& PL, int L1) {
+    u32 k = 0, mul = 1;
+    int lb = L1;
+    for (int i = 0; i < PL.nlev; ++i) {
+        const int r = PL.logr[i];
+        lb -= r;
+        const u32 j = (s >> lb) & ((1u << r) - 1);
+        k += (__brev(j) >> (32 - r)) * mul;
+        mul <<= r;
+    }
+    return k;
+}
+
+// ------------------------------------------------------------- pass A ----
+// Forward column level LEV on the 32-column tile.  The first level reads the
+// operand from global memory, the last writes the workspace.
+template <int L1, int LEV, int NW>
+__device__ __forceinline__ void col_fwd_level(u32* tile, const LargeArgs& A, const u32* src, int len,
+                                              u32* dst, int c, int n2) {
+    using LV = ColLevel<L1, LEV>;
+    constexpr LevelPlan PL = col_plan(L1);
+    constexpr int R = LV::R, TB = LV::TB, B = LV::B;
+    constexpr bool FIRST = LEV == 0, LAST = LEV + 1 == PL.nlev;
+    constexpr int TASKS = (1 << L1) / R;
+    const u32 p = A.pkc.p, p2 = A.pkc.p2;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int id = warp; id < TASKS; id += NW) {
+        const int blk = id / TB, o = id % TB;
+        const int row0 = blk * B + o;
+        u32 x[R];
+#pragma unroll
+        for (int m = 0; m < R; ++m) {
+            const int row = row0 + TB * m;
+            if constexpr (FIRST) {
+                const long long gi = (long long)row * n2 + c;
+                u32 v = gi < len ? __ldg(src + gi) : 0u;
+                x[m] = mul_shoup(v, 1u, A.pkc.one_q, p);
+            } else {
+                x[m] = tile[row * 32 + lane];
+            }
+        }
+        dif_regs<R>(x, A.pkc.rc.f, p, p2);
+        if constexpr (!LAST) {
+            const Tw* t = A.twc + LV::TWOFF + o * R;
+#pragma unroll
+            for (int j = 1; j < R; ++j) {
+                const Tw w = t[j];  // uniform across the warp: broadcast
+                x[j] = mul_shoup(x[j], w.w, w.wq, p);
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < R; ++m) {
+            const int row = row0 + TB * m;
+            if constexpr (LAST) dst[(size_t)row * n2 + c] = x[m];
+            else tile[row * 32 + lane] = x[m];
+        }
+    }
+}
+
+template <int L1, int LEV, int NW>
+__device__ __forceinline__ void col_fwd_levels(u32* tile, const LargeArgs& A, const u32* src, int len,
+                                               u32* dst, int c, int n2) {
+    constexpr LevelPlan PL = col_plan(L1);
+    if constexpr (LEV < PL.nlev) {
+        col_fwd_level<L1, LEV, NW>(tile, A, src, len, dst, c, n2);
+        if constexpr (LEV + 1 < PL.nlev) __syncthreads();
+        col_fwd_levels<L1, LEV + 1, NW>(tile, A, src, len, dst, c, n2);
+    }
+}
+
+// grid: (n2/32 column tiles, 2 operands, jobs)
+template <int L1, int NW>
+__global__ void __launch_bounds__(NW * 32) k_col_fwd(const __grid_constant__ LargeArgs A) {
+    extern __shared__ __align__(16) u32 tile[];
+    const LargeJob& J = A.jobs ? A.jobs[blockIdx.z] : A.job0;
+    const int op = blockIdx.y;
+    const u32* src = op ? J.b : J.a;
+    const int len = op ? J.lb : J.la;
+    u32* dst = op ? J.wb : J.wa;
+    const int n2 = 1 << A.l2;
+    const int c = blockIdx.x * 32 + (threadIdx.x & 31);
+    col_fwd_levels<L1, 0, NW>(tile, A, src, len, dst, c, n2);
+}
+
+// ------------------------------------------------------------- pass C ----
+template <int L1, int LEV, int NW>
+__device__ __forceinline__ void col_inv_level(u32* tile, const LargeArgs& A, const u32* src, u32* h,
+                                              int lh, int c, int n2) {
+    using LV = ColLevel<L1, LEV>;
+    constexpr LevelPlan PL = col_plan(L1);
+    constexpr int R = LV::R, TB = LV::TB, B = LV::B;
+    constexpr bool DEEPEST = LEV + 1 == PL.nlev, OUTER = LEV == 0;
+    constexpr int TASKS = (1 << L1) / R;
+    const u32 p = A.pkc.p, p2 = A.pkc.p2;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int id = warp; id < TASKS; id += NW) {
+        const int blk = id / TB, o = id % TB;
+        const int row0 = blk * B + o;
+        u32 x[R];
+#pragma unroll
+        for (int m = 0; m < R; ++m) {
+            const int row = row0 + TB * m;
+            if constexpr (DEEPEST) x[m] = src[(size_t)row * n2 + c];
+            else x[m] = tile[row * 32 + lane];
+        }
+        if constexpr (!DEEPEST) {
+            const Tw* t = A.twc + A.twc_inv + LV::TWOFF + o * R;
+#pragma unroll
+            for (int j = 1; j < R; ++j) {
+                const Tw w = t[j];
+                x[j] = mul_shoup(x[j], w.w, w.wq, p);
+            }
+        }
+        dit_regs<R>(x, A.pkc.rc.i, p, p2);
+#pragma unroll
+        for (int m = 0; m < R; ++m) {
+            const int row = row0 + TB * m;
+            if constexpr (OUTER) {
+                const long long gi = (long long)row * n2 + c;
+                if (gi < lh) h[gi] = red1(red2(x[m], p2), p);
+            } else {
+                tile[row * 32 + lane] = x[m];
+            }
+        }
+    }
+}
+
+template <int L1, int LEV, int NW>
+__device__ __forceinline__ void col_inv_levels(u32* tile, const LargeArgs& A, const u32* src, u32* h,
+                                               int lh, int c, int n2) {
+    if constexpr (LEV >= 0) {
+        col_inv_level<L1, LEV, NW>(tile, A, src, h, lh, c, n2);
+        if constexpr (LEV > 0) __syncthreads();
+        col_inv_levels<L1, LEV - 1, NW>(tile, A, src, h, lh, c, n2);
+    }
+}
+
+// grid: (n2/32 column tiles, 1, jobs)
+template <int L1, int NW>
+__global__ void __launch_bounds__(NW * 32) k_col_inv(const __grid_constant__ LargeArgs A) {
+    extern __shared__ __align__(16) u32 tile[];
+    const LargeJob& J = A.jobs ? A.jobs[blockIdx.z] : A.job0;
+    const int n2 = 1 << A.l2;
+    const int c = blockIdx.x * 32 + (threadIdx.x & 31);
+    col_inv_levels<L1, col_plan(L1).nlev - 1, NW>(tile, A, J.wa, J.h, J.lh, c, n2);
+}
+
+// ------------------------------------------------------------- pass B ----
+// Shoup pair of w_n^(+-e) (times an optional extra factor) from the seeds.
+__device__ __forceinline__ u32 seed_mont(const LargeArgs& A, u32 e, bool inv) {
+    const u32* s = A.seeds + (inv ? (A.nlo + A.nhi) : 0);
+    return mul_mont(__ldg(s + (e & 4095u)), __ldg(s + A.nlo + (e >> 12)), A.pk.p, A.pk.pinv_neg);
+}
+
+template <int L2>
+__global__ void __launch_bounds__(small_threads(L2), 1) k_row_fused(const __grid_constant__ LargeArgs A) {
+    constexpr int n2 = 1 << L2;
+    constexpr int T = small_threads(L2);
+    constexpr LevelPlan PL = row_plan(L2);
+    static_assert(PL.nlev >= 2, "row pass needs at least two levels");
+    using LV0 = SmallLevel<L2, 0>;
+    constexpr int R0 = LV0::R, TB0 = LV0::TB;  // level 0: tasks o < TB0 = n2 / R0
+    extern __shared__ __align__(16) u32 sm[];   // [F row | G row], swizzled
+    __shared__ Tw bf[R0], bi[R0];
+
+    const LargeJob& J = A.jobs ? A.jobs[blockIdx.y] : A.job0;
+    const u32 s = blockIdx.x;
+    const u32 k1 = col_slot_to_k1(s, A.colpl, A.l1);
+    const u32 nmask = (1u << (A.l1 + L2)) - 1;
+    const u32 p = A.pk.p, p2 = A.pk.p2, pinv = A.pk.pinv_neg;
+
+    // slot factors w^(+-k1*TB0*m), the inverse one carrying 2^32/n
+    if (threadIdx.x < 2 * R0) {
+        const bool inv = threadIdx.x >= R0;
+        const u32 m = threadIdx.x % R0;
+        const u32 e = (k1 * (u32)TB0 * m) & nmask;
+        u32 v = red1(mul_mont(seed_mont(A, e, inv), 1u, p, pinv), p);  // plain w^(+-e)
+        if (inv) v = (u32)(((u64)v * A.scale_rn) % p);
+        const Tw t{v, (u32)(((u64)v << 32) / p)};
+        if (inv) bi[m] = t; else bf[m] = t;
+    }
+    __syncthreads();
+
+    const u32* rowF = J.wa + (size_t)s * n2;
+    const u32* rowG = J.wb + (size_t)s * n2;
+    RowCtx ctx{A.pk, A.twr, A.twr_inv};
+
+    // level 0 forward with the inter-pass twiddle, from global memory
+    for (int o = threadIdx.x; o < TB0; o += T) {
+        const u32 mo = seed_mont(A, (k1 * (u32)o) & nmask, false);  // w^(k1 o) * 2^32
+        u32 xf[R0], xg[R0];
+#pragma unroll
+        for (int m = 0; m < R0; ++m) {
+            const u32 cm = mul_shoup(mo, bf[m].w, bf[m].wq, p);  // w^(k1 (o + TB0 m)) * 2^32
+            xf[m] = mul_mont(__ldg(rowF + o + TB0 * m), cm, p, pinv);
+            xg[m] = mul_mont(__ldg(rowG + o + TB0 * m), cm, p, pinv);
+        }
+        dif_regs<R0>(xf, A.pk.rc.f, p, p2);
+        dif_regs<R0>(xg, A.pk.rc.f, p, p2);
+        Tw t[R0];
+        load_tw<R0>(t, A.twr + o * R0);
+#pragma unroll
+        for (int j = 1; j < R0; ++j) {
+            xf[j] = mul_shoup(xf[j], t[j].w, t[j].wq, p);
+            xg[j] = mul_shoup(xg[j], t[j].w, t[j].wq, p);
+        }
+#pragma unroll
+        for (int m = 0; m < R0; ++m) {
+            sm[swz(o + TB0 * m)] = xf[m];
+            sm[swz(n2 + o + TB0 * m)] = xg[m];
+        }
+    }
+    __syncthreads();
+    small_fwd_levels<L2, 1, T, 1>(sm, ctx);
+
+    // last level: forward both, pointwise (Montgomery; the 2^-32 is undone by
+    // the inverse twiddle), inverse
+    for (int row = threadIdx.x; row < n2 / 32; row += T) {
+        u32 xf[32], xg[32];
+        load_row32(xf, sm, row * 32);
+        load_row32(xg, sm, n2 + row * 32);
+        dif_regs<32>(xf, A.pk.rc.f, p, p2);
+        dif_regs<32>(xg, A.pk.rc.f, p, p2);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) xf[j] = mul_mont(xf[j], xg[j], p, pinv);
+        dit_regs<32>(xf, A.pk.rc.i, p, p2);
+        store_row32(sm, row * 32, xf);
+    }
+    __syncthreads();
+    small_inv_levels<L2, PL.nlev - 2, T, 1, 1>(sm, ctx);
+
+    // level 0 inverse, inverse twiddle and scale, to global memory
+    u32* rowH = J.wa + (size_t)s * n2;
+    for (int o = threadIdx.x; o < TB0; o += T) {
+        u32 x[R0];
+#pragma unroll
+        for (int m = 0; m < R0; ++m) x[m] = sm[swz(o + TB0 * m)];
+        Tw t[R0];
+        load_tw<R0>(t, A.twr + A.twr_inv + o * R0);
+#pragma unroll
+        for (int j = 1; j < R0; ++j) x[j] = mul_shoup(x[j], t[j].w, t[j].wq, p);
+        dit_regs<R0>(x, A.pk.rc.i, p, p2);
+        const u32 mo = seed_mont(A, (k1 * (u32)o) & nmask, true);  // w^-(k1 o) * 2^32
+#pragma unroll
+        for (int m = 0; m < R0; ++m) {
+            const u32 d = mul_shoup(mo, bi[m].w, bi[m].wq, p);  // w^-(k1 c) * 2^64 / n
+            rowH[o + TB0 * m] = mul_mont(red2(x[m], p2), d, p, pinv);
+        }
+    }
+}
+
+#endif  // __CUDACC__
+
+}  // namespace cmb

@@ -1,0 +1,410 @@
+// Natural-order transforms behind cumodp_fft_uni / cumodp_invfft_uni and
+// the bivariate entry points.
+//
+// Reference behaviour: stockham_host / inverse_stockham_host
+// (src/stockham.cu:479-503) compute X[j] = sum_i X[i] w^(ij) in natural
+// order with the caller's root; bivariate_stockham_host
+// (src/list_stockham.cu:1224-1245) computes the row-column 2-D DFT
+// (DFT_m (x) I_n)(I_m (x) DFT_n) of a row-major 2^em x 2^en array.
+//
+// Here a transform of length <= 2^14 is one CTA (levels in shared memory,
+// then an in-CTA reorder to natural order).  Longer 1-D transforms use the
+// four-step split of the product path: a column pass (k_col_fwd), a row
+// pass that applies w_n^(k1*c), transforms the row and writes it back in
+// natural order as row k1, and a tiled transpose.  The 2-D transform is the
+// column pass plus the row pass with no inter-pass twiddle: its rows land
+// directly in natural order.
+#include <algorithm>
+#include <cstring>
+
+#include "../../include/cumodp.h"
+#include "product.cuh"
+
+namespace cmb {
+
+struct RowNttArgs {
+    PrimeK pk;
+    const Tw* __restrict__ twr;
+    const u32* __restrict__ seeds;  // inter-pass twiddles w_n^(k1 c) (nullptr: none)
+    int nlo, nhi;
+    int l1;                         // rows come from a column pass of length 2^l1 (0: none)
+    LevelPlan colpl;
+    const u32* src;                 // row slot s at src + s * n2
+    u32* dst;                       // natural row k1 at dst + k1 * n2
+    Tw scale;                       // applied to every output
+};
+
+__device__ __forceinline__ u32 seed_mont_at(const u32* __restrict__ seeds, int nlo, u32 e, u32 p, u32 pinv) {
+    return mul_mont(__ldg(seeds + (e & 4095u)), __ldg(seeds + nlo + (e >> 12)), p, pinv);
+}
+
+// Position in a row after the row plan's DIF levels -> frequency index.
+template <int L2>
+__device__ __forceinline__ u32 row_pos_to_freq(u32 P) {
+    constexpr LevelPlan PL = row_plan(L2);
+    u32 f = 0, mul = 1;
+    int lb = L2;
+#pragma unroll
+    for (int i = 0; i < PL.nlev; ++i) {
+        const int r = PL.logr[i];
+        lb -= r;
+        const u32 j = (P >> lb) & ((1u << r) - 1);
+        f += (__brev(j) >> (32 - r)) * mul;
+        mul <<= r;
+    }
+    return f;
+}
+
+// Single-operand forward level LEV (not the last) on a row in shared memory.
+template <int LOGL, int LEV, int T>
+__device__ __forceinline__ void fwd1_level(u32* sm, const PrimeK& pk, const Tw* __restrict__ tw) {
+    using LV = SmallLevel<LOGL, LEV>;
+    constexpr int L = 1 << LOGL, R = LV::R, TB = LV::TB, B = LV::B;
+    const u32 p = pk.p, p2 = pk.p2;
+    for (int id = threadIdx.x; id < L / R; id += T) {
+        const int blk = id / TB, o = id % TB;
+        const int base = blk * B + o;
+        u32 x[R];
+#pragma unroll
+        for (int m = 0; m < R; ++m) x[m] = sm[swz(base + TB * m)];
+        dif_regs<R>(x, pk.rc.f, p, p2);
+        Tw t[R];
+        load_tw<R>(t, tw + LV::TWOFF + o * R);
+#pragma unroll
+        for (int j = 1; j < R; ++j) x[j] = mul_shoup(x[j], t[j].w, t[j].wq, p);
+#pragma unroll
+        for (int m = 0; m < R; ++m) sm[swz(base + TB * m)] = x[m];
+    }
+}
+
+template <int LOGL, int LEV, int T>
+__device__ __forceinline__ void fwd1_levels(u32* sm, const PrimeK& pk, const Tw* __restrict__ tw) {
+    constexpr LevelPlan PL = row_plan(LOGL);
+    if constexpr (LEV + 1 < PL.nlev) {
+        fwd1_level<LOGL, LEV, T>(sm, pk, tw);
+        __syncthreads();
+        fwd1_levels<LOGL, LEV + 1, T>(sm, pk, tw);
+    }
+}
+
+template <int L2>
+__global__ void __launch_bounds__(small_threads(L2), 1) k_row_ntt(const __grid_constant__ RowNttArgs A) {
+    constexpr int n2 = 1 << L2;
+    constexpr int T = small_threads(L2);
+    constexpr LevelPlan PL = row_plan(L2);
+    static_assert(PL.nlev >= 2, "row transform needs two levels");
+    using LV0 = SmallLevel<L2, 0>;
+    constexpr int R0 = LV0::R, TB0 = LV0::TB;
+    extern __shared__ __align__(16) u32 sm[];  // [levels | natural order]
+    __shared__ Tw bf[R0];
+
+    const u32 s = blockIdx.x;
+    const u32 k1 = A.l1 ? col_slot_to_k1(s, A.colpl, A.l1) : 0u;
+    const bool twid = A.seeds != nullptr;
+    const u32 nmask = (1u << (A.l1 + L2)) - 1;
+    const u32 p = A.pk.p, p2 = A.pk.p2, pinv = A.pk.pinv_neg;
+    if (twid && threadIdx.x < R0) {
+        const u32 e = (k1 * (u32)TB0 * threadIdx.x) & nmask;
+        const u32 v = red1(mul_mont(seed_mont_at(A.seeds, A.nlo, e, p, pinv), 1u, p, pinv), p);
+        bf[threadIdx.x] = Tw{v, (u32)(((u64)v << 32) / p)};
+    }
+    __syncthreads();
+
+    const u32* row = A.src + (size_t)s * n2;
+    for (int o = threadIdx.x; o < TB0; o += T) {
+        u32 x[R0];
+        const u32 mo = twid ? seed_mont_at(A.seeds, A.nlo, (k1 * (u32)o) & nmask, p, pinv) : 0u;
+#pragma unroll
+        for (int m = 0; m < R0; ++m) {
+            const u32 v = row[o + TB0 * m];
+            if (twid) x[m] = mul_mont(v, mul_shoup(mo, bf[m].w, bf[m].wq, p), p, pinv);
+            else x[m] = mul_shoup(v, 1u, A.pk.one_q, p);
+        }
+        dif_regs<R0>(x, A.pk.rc.f, p, p2);
+        Tw t[R0];
+        load_tw<R0>(t, A.twr + o * R0);
+#pragma unroll
+        for (int j = 1; j < R0; ++j) x[j] = mul_shoup(x[j], t[j].w, t[j].wq, p);
+#pragma unroll
+        for (int m = 0; m < R0; ++m) sm[swz(o + TB0 * m)] = x[m];
+    }
+    __syncthreads();
+    fwd1_levels<L2, 1, T>(sm, A.pk, A.twr);
+
+    for (int r = threadIdx.x; r < n2 / 32; r += T) {
+        u32 x[32];
+        load_row32(x, sm, r * 32);
+        dif_regs<32>(x, A.pk.rc.f, p, p2);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            const u32 f = row_pos_to_freq<L2>((u32)(r * 32 + j));
+            sm[n2 + swz((int)f)] = red1(mul_shoup(x[j], A.scale.w, A.scale.wq, p), p);
+        }
+    }
+    __syncthreads();
+    u32* out = A.dst + (size_t)k1 * n2;
+    for (int i = threadIdx.x * 4; i < n2; i += T * 4) {
+        uint4 v = *reinterpret_cast<const uint4*>(sm + n2 + swz(i));
+        *reinterpret_cast<uint4*>(out + i) = v;
+    }
+}
+
+// out[c * rows + r] = in[r * cols + c]: 32 x 32 tiles through shared memory.
+__global__ void k_transpose(const u32* __restrict__ in, u32* __restrict__ out, int rows, int cols) {
+    __shared__ u32 t[32][33];
+    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+    for (int y = threadIdx.y; y < 32; y += blockDim.y)
+        t[y][threadIdx.x] = in[(size_t)(r0 + y) * cols + c0 + threadIdx.x];
+    __syncthreads();
+    for (int y = threadIdx.y; y < 32; y += blockDim.y)
+        out[(size_t)(c0 + y) * rows + r0 + threadIdx.x] = t[threadIdx.x][y];
+}
+
+// Direct DFT for n <= 32 (one CTA of n threads): out[j] = scale * sum x_i w^(ij).
+__global__ void k_tiny_dft(const u32* __restrict__ x, u32* __restrict__ y, int n, u32 w, u32 p, u32 scale) {
+    __shared__ u32 xs[32], pw[32];
+    const int j = threadIdx.x;
+    xs[j] = x[j] % p;
+    u32 t = 1;
+    for (int i = 0; i < j; ++i) t = (u32)(((u64)t * w) % p);
+    pw[j] = t;
+    __syncthreads();
+    u64 acc = 0;
+    for (int i = 0; i < n; ++i) acc = (acc + (u64)xs[i] * pw[(i * j) & (n - 1)]) % p;
+    y[j] = (u32)((acc * scale) % p);
+}
+
+namespace {
+
+template <int L2>
+void launch_row_ntt_t(const RowNttArgs& a, int rows, cudaStream_t st) {
+    const size_t smem = (size_t)2 * (1 << L2) * sizeof(u32);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_row_ntt<L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    k_row_ntt<L2><<<rows, small_threads(L2), smem, st>>>(a);
+}
+typedef void (*RowNttFn)(const RowNttArgs&, int, cudaStream_t);
+const RowNttFn kRowNtt[15] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                              launch_row_ntt_t<6>, launch_row_ntt_t<7>, launch_row_ntt_t<8>,
+                              launch_row_ntt_t<9>, launch_row_ntt_t<10>, launch_row_ntt_t<11>,
+                              launch_row_ntt_t<12>, launch_row_ntt_t<13>, launch_row_ntt_t<14>};
+
+// Forward-column launchers shared with the product path (single operand).
+template <int L1>
+void launch_colfwd1_t(const LargeArgs& a, int tiles, cudaStream_t st) {
+    const size_t smem = (size_t)(1 << L1) * 32 * sizeof(u32);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_col_fwd<L1, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    k_col_fwd<L1, 8><<<dim3(tiles, 1, 1), 256, smem, st>>>(a);
+}
+typedef void (*ColFn)(const LargeArgs&, int, cudaStream_t);
+const ColFn kColFwd1[11] = {nullptr, launch_colfwd1_t<1>, launch_colfwd1_t<2>, launch_colfwd1_t<3>,
+                            launch_colfwd1_t<4>, launch_colfwd1_t<5>, launch_colfwd1_t<6>,
+                            launch_colfwd1_t<7>, launch_colfwd1_t<8>, launch_colfwd1_t<9>,
+                            launch_colfwd1_t<10>};
+
+// w is a primitive 2^k-th root of unity mod p.
+bool root_has_order(u32 w, int k, u32 p) {
+    if (w == 0 || w >= p) return false;
+    if (k == 0) return w == 1;
+    return powmod_exact(w, 1ull << k, p) == 1 && powmod_exact(w, 1ull << (k - 1), p) == p - 1;
+}
+
+u32 inv_of(u32 a, u32 p) { return powmod_exact(a, p - 2, p); }
+
+// Column pass of a single array (rows of n2 words, 2^l1 rows) into dst.
+int column_pass(const PrimeCtx& pc, u32 root_c, int l1, int l2, const u32* src, long long len, u32* dst,
+                int dev, cudaStream_t st) {
+    int err = OK;
+    const u32 p = pc.info.p;
+    const Tw* twc = col_tables(dev, p, root_c, l1, &err);
+    if (!twc) return err;
+    LargeArgs A;
+    memset(&A, 0, sizeof(A));
+    A.pk = A.pkc = make_prime_k_for(pc.info, root_c, l1);
+    A.twc = twc;
+    A.twc_inv = plan_tw_entries(col_plan(l1), l1);
+    A.l1 = l1;
+    A.l2 = l2;
+    A.colpl = col_plan(l1);
+    A.job0 = LargeJob{src, nullptr, nullptr, (int)std::min<long long>(len, 1ll << 30), 0, 0, 0, dst, nullptr};
+    A.njobs = 1;
+    kColFwd1[l1](A, (1 << l2) / 32, st);
+    return OK;
+}
+
+}  // namespace
+
+// x_out = DFT(x_in) with root w (inverse: root w^-1 and scaling by 2^-k).
+int ntt_natural_dev(const u32* x_in, u32* x_out, int k, u32 w, u32 p, bool inverse, cudaStream_t st) {
+    int err = OK;
+    const PrimeCtx* pc = prime_ctx(p, &err);
+    if (!pc) return err;
+    if (k < 0) return ASSUMPTION_ERROR;
+    if (k > pc->info.two_adic) return FFT_SIZE_TOO_LARGE;
+    if (!root_has_order(w, k, p)) return ASSUMPTION_ERROR;
+    if (k > kMaxLog) return FFT_SIZE_TOO_LARGE;
+    const int dev = current_device();
+    const u32 root = inverse ? inv_of(w, p) : w;
+    const u32 sc = inverse ? inv_of((u32)((1ull << k) % p), p) : 1u;
+    if (k <= 5) {
+        k_tiny_dft<<<1, 1 << k, 0, st>>>(x_in, x_out, 1 << k, root, p, sc);
+        return cuda_err(cudaGetLastError());
+    }
+    if (k <= kMaxSmallLog) {
+        RowNttArgs A;
+        memset(&A, 0, sizeof(A));
+        const Tw* twr = row_tables(dev, p, root, k, &err);
+        if (!twr) return err;
+        A.pk = make_prime_k_for(pc->info, root, k);
+        A.twr = twr;
+        A.src = x_in;
+        A.dst = x_out;
+        A.scale = tw_of(sc, p);
+        kRowNtt[k](A, 1, st);
+        return cuda_err(cudaGetLastError());
+    }
+    const int l1 = std::max(5, k - kMaxRowLog), l2 = k - l1;
+    const long long n = 1ll << k;
+    u32* ws = (u32*)workspace(dev, kWsNtt, (size_t)2 * n * sizeof(u32), &err);
+    if (!ws) return err;
+    u32 *w1 = ws, *w2 = ws + n;
+    const u32 root_c = powmod_exact(root, 1ull << l2, p), root_r = powmod_exact(root, 1ull << l1, p);
+    if ((err = column_pass(*pc, root_c, l1, l2, x_in, n, w1, dev, st)) != OK) return err;
+    RowNttArgs A;
+    memset(&A, 0, sizeof(A));
+    const Tw* twr = row_tables(dev, p, root_r, l2, &err);
+    const u32* seeds = seed_tables(dev, p, root, k, &err);
+    if (!twr || !seeds) return err ? err : OUT_OF_MEMORY;
+    A.pk = make_prime_k_for(pc->info, root_r, l2);
+    A.twr = twr;
+    A.seeds = seeds;
+    A.nlo = (int)std::min<long long>(n, 4096);
+    A.nhi = (int)std::max<long long>(1, n / 4096);
+    A.l1 = l1;
+    A.colpl = col_plan(l1);
+    A.src = w1;
+    A.dst = w2;
+    A.scale = tw_of(sc, p);
+    kRowNtt[l2](A, 1 << l1, st);
+    k_transpose<<<dim3((1 << l2) / 32, (1 << l1) / 32), dim3(32, 8), 0, st>>>(w2, x_out, 1 << l1, 1 << l2);
+    return cuda_err(cudaGetLastError());
+}
+
+// 2-D DFT of a row-major 2^em x 2^en array, in place.
+int bivariate_dev(u32* x, int em, u32 wm, int en, u32 wn, u32 p, bool inverse, cudaStream_t st) {
+    int err = OK;
+    const PrimeCtx* pc = prime_ctx(p, &err);
+    if (!pc) return err;
+    if (em < 0 || en < 0) return ASSUMPTION_ERROR;
+    if (em > pc->info.two_adic || en > pc->info.two_adic) return FFT_SIZE_TOO_LARGE;
+    if (!root_has_order(wm, em, p) || !root_has_order(wn, en, p)) return ASSUMPTION_ERROR;
+    if (en < 6) return FFT_SIZE_TOO_SMALL;
+    if (en > kMaxRowLog || em > kMaxColLog) return FFT_SIZE_TOO_LARGE;
+    const int dev = current_device();
+    const u32 rm = inverse ? inv_of(wm, p) : wm, rn = inverse ? inv_of(wn, p) : wn;
+    const u32 sc = inverse ? inv_of((u32)((1ull << (em + en)) % p), p) : 1u;
+    const long long total = 1ll << (em + en);
+    const Tw* twr = row_tables(dev, p, rn, en, &err);
+    if (!twr) return err;
+    RowNttArgs A;
+    memset(&A, 0, sizeof(A));
+    A.pk = make_prime_k_for(pc->info, rn, en);
+    A.twr = twr;
+    A.scale = tw_of(sc, p);
+    A.dst = x;
+    if (em == 0) {
+        A.src = x;
+        kRowNtt[en](A, 1, st);
+        return cuda_err(cudaGetLastError());
+    }
+    u32* w1 = (u32*)workspace(dev, kWsNtt, (size_t)total * sizeof(u32), &err);
+    if (!w1) return err;
+    if ((err = column_pass(*pc, rm, em, en, x, total, w1, dev, st)) != OK) return err;
+    A.l1 = em;
+    A.colpl = col_plan(em);
+    A.src = w1;
+    kRowNtt[en](A, 1 << em, st);
+    return cuda_err(cudaGetLastError());
+}
+
+}  // namespace cmb
+
+using namespace cmb;
+
+namespace {
+
+cumodp_err host_ntt(sfixn* X, sfixn n, sfixn k, sfixn w, sfixn p, bool inverse) {
+    int cnt = 0;
+    if (cudaGetDeviceCount(&cnt) != cudaSuccess || cnt == 0) {
+        cudaGetLastError();
+        return CUMODP_NO_CUDA_DEVICE;
+    }
+    if (!X || k < 0 || k > 30 || n != (sfixn)(1u << k) || p <= 0) return CUMODP_ASSUMPTION_ERROR;
+    std::lock_guard<std::mutex> g(lib_mutex());
+    const int dev = current_device();
+    cudaStream_t st = lib_stream(dev);
+    int err = OK;
+    u32* d = (u32*)workspace(dev, kWsStage, (size_t)n * sizeof(u32), &err);
+    if (!d) return (cumodp_err)err;
+    cudaError_t ce = cudaMemcpyAsync(d, X, (size_t)n * 4, cudaMemcpyHostToDevice, st);
+    if (ce != cudaSuccess) return (cumodp_err)cuda_err(ce);
+    err = ntt_natural_dev(d, d, k, (u32)w, (u32)p, inverse, st);
+    if (err != OK) {
+        cudaStreamSynchronize(st);
+        return (cumodp_err)err;
+    }
+    ce = cudaMemcpyAsync(X, d, (size_t)n * 4, cudaMemcpyDeviceToHost, st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    return (cumodp_err)cuda_err(ce);
+}
+
+cumodp_err host_bivariate(sfixn* X, sfixn em, sfixn wm, sfixn en, sfixn wn, sfixn p, bool inverse) {
+    int cnt = 0;
+    if (cudaGetDeviceCount(&cnt) != cudaSuccess || cnt == 0) {
+        cudaGetLastError();
+        return CUMODP_NO_CUDA_DEVICE;
+    }
+    if (!X || em < 0 || en < 0 || em + en > 30 || p <= 0) return CUMODP_ASSUMPTION_ERROR;
+    std::lock_guard<std::mutex> g(lib_mutex());
+    const int dev = current_device();
+    cudaStream_t st = lib_stream(dev);
+    const size_t total = (size_t)1 << (em + en);
+    int err = OK;
+    u32* d = (u32*)workspace(dev, kWsStage, total * sizeof(u32), &err);
+    if (!d) return (cumodp_err)err;
+    cudaError_t ce = cudaMemcpyAsync(d, X, total * 4, cudaMemcpyHostToDevice, st);
+    if (ce != cudaSuccess) return (cumodp_err)cuda_err(ce);
+    err = bivariate_dev(d, em, (u32)wm, en, (u32)wn, (u32)p, inverse, st);
+    if (err != OK) {
+        cudaStreamSynchronize(st);
+        return (cumodp_err)err;
+    }
+    ce = cudaMemcpyAsync(X, d, total * 4, cudaMemcpyDeviceToHost, st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    return (cumodp_err)cuda_err(ce);
+}
+
+}  // namespace
+
+extern "C" {
+
+cumodp_err cumodp_fft_uni(sfixn* X, sfixn n, sfixn k, sfixn w, sfixn p) { return host_ntt(X, n, k, w, p, false); }
+
+cumodp_err cumodp_invfft_uni(sfixn* X, sfixn n, sfixn k, sfixn w, sfixn p) { return host_ntt(X, n, k, w, p, true); }
+
+cumodp_err cumodp_fft_bivariate(sfixn* X, sfixn em, sfixn wm, sfixn en, sfixn wn, sfixn p) {
+    return host_bivariate(X, em, wm, en, wn, p, false);
+}
+
+cumodp_err cumodp_invfft_bivariate(sfixn* X, sfixn em, sfixn wm, sfixn en, sfixn wn, sfixn p) {
+    return host_bivariate(X, em, wm, en, wn, p, true);
+}
+
+}  // extern "C"

@@ -1,0 +1,123 @@
+// CTA-level NTT building blocks for sm_100a.
+//
+// The reference computes every radix-2 Stockham step as three separate
+// kernels over HBM (butterfly, stride permutation, twiddle;
+// src/stockham.cu:75-397).  Here a transform of length L <= 2^14 lives in
+// shared memory and is computed in a few "levels".  A level of radix
+// R = 2^r splits each current block of size B into R strided sub-sequences
+// (task o in [0, B/R) owns elements o + (B/R)*m, m < R), runs an R-point DFT
+// in registers (r radix-2 stages, constants only), and multiplies output k
+// of task o by w_B^(o*k) (four-step / Gentleman-Sande decomposition).  The
+// forward transform is DIF (natural order in, digit-reversed order out); the
+// inverse runs the transposed levels (DIT with inverse roots, digit-reversed
+// in, natural out).  A product never needs natural-order spectra, so the
+// forward/inverse pair needs no permutation at all.
+//
+// Butterflies follow Harvey's lazy reduction ("Faster arithmetic for
+// number-theoretic transforms", J. Symb. Comp. 2014): forward values stay in
+// [0, 2p), inverse values in [0, 4p).
+#pragma once
+#include "field.cuh"
+
+namespace cmb {
+
+// Root constants shared by every register DFT of radix <= 32:
+// c[j] = w_32^j (forward) or w_32^-j (inverse) for j < 16, in Shoup form.
+struct RootConsts {
+    Tw f[16];
+    Tw i[16];
+};
+
+// Per-prime constants passed by value to kernels (live in the constant bank).
+struct PrimeK {
+    u32 p, p2, pinv_neg;
+    u32 one_q;  // shoup_quot(1, p): reduces any u32 to [0, 2p)
+    RootConsts rc;
+};
+
+#ifdef __CUDACC__
+
+// Shared-memory word index swizzle: the 16-byte quad inside each 32-word row
+// is XOR-ed with (row & 7).  Scalar accesses by 32 lanes to 32 consecutive
+// words and 16-byte accesses by lanes to consecutive 32-word rows (or to
+// consecutive 16/8/4-word groups) are both bank-conflict free.
+__device__ __forceinline__ int swz(int i) { return i ^ (((i >> 5) & 7) << 2); }
+
+// Forward R-point DIF on registers; x[j] ends holding X[bitrev_r(j)].
+// Inputs and outputs in [0, 2p).
+template <int R>
+__device__ __forceinline__ void dif_regs(u32 (&x)[R], const Tw* __restrict__ c, u32 p, u32 p2) {
+#pragma unroll
+    for (int half = R / 2; half >= 1; half >>= 1) {
+#pragma unroll
+        for (int g = 0; g < R; g += 2 * half) {
+#pragma unroll
+            for (int j = 0; j < half; ++j) {
+                const int e = j * (32 / (2 * half));  // w_{2half}^j = w_32^e
+                u32 a = x[g + j], b = x[g + j + half];
+                u32 s = a + b;
+                u32 d = a - b + p2;
+                x[g + j] = red2(s, p2);
+                x[g + j + half] = (e == 0) ? red2(d, p2) : mul_shoup(d, c[e].w, c[e].wq, p);
+            }
+        }
+    }
+}
+
+// Inverse R-point DIT on registers (roots c = w_32^-j); x[j] holds Y[bitrev(j)]
+// on entry and R * y[j] on exit.  Inputs and outputs in [0, 4p).
+template <int R>
+__device__ __forceinline__ void dit_regs(u32 (&x)[R], const Tw* __restrict__ c, u32 p, u32 p2) {
+#pragma unroll
+    for (int half = 1; half < R; half <<= 1) {
+#pragma unroll
+        for (int g = 0; g < R; g += 2 * half) {
+#pragma unroll
+            for (int j = 0; j < half; ++j) {
+                const int e = j * (32 / (2 * half));
+                u32 a = red2(x[g + j], p2);
+                u32 b = x[g + j + half];
+                u32 t = (e == 0) ? red2(b, p2) : mul_shoup(b, c[e].w, c[e].wq, p);
+                x[g + j] = a + t;
+                x[g + j + half] = a - t + p2;
+            }
+        }
+    }
+}
+
+template <int R>
+__device__ __forceinline__ void load_tw(Tw (&t)[R], const Tw* __restrict__ src) {
+    const uint4* s4 = reinterpret_cast<const uint4*>(src);
+#pragma unroll
+    for (int j = 0; j < R / 2; ++j) {
+        uint4 v = __ldg(s4 + j);
+        t[2 * j] = Tw{v.x, v.y};
+        t[2 * j + 1] = Tw{v.z, v.w};
+    }
+}
+
+#endif  // __CUDACC__
+
+// --------------------------------------------------------------------------
+// Level plans.  A plan is a list of log-radices r_1..r_m with sum = log2 L.
+// Level i acts on blocks of size B_i = L >> (r_1 + ... + r_{i-1}).  Its
+// twiddle table holds, for each task o < B_i / R_i and register slot j < R_i,
+// w_{B_i}^(o * bitrev(j)) (forward) and the inverse root power (inverse), as
+// Tw pairs; the last level needs none (B_m = R_m).
+// --------------------------------------------------------------------------
+struct LevelPlan {
+    int nlev;
+    int logr[6];
+};
+
+// Number of Tw entries one direction of a plan's tables needs.
+__host__ __device__ inline int plan_tw_entries(const LevelPlan& pl, int logl) {
+    int n = 0, lb = logl;
+    for (int i = 0; i + 1 < pl.nlev; ++i) {
+        n += 1 << lb;  // (B/R) * R entries
+        lb -= pl.logr[i];
+    }
+    return n;
+}
+
+}  // namespace cmb

@@ -1,0 +1,53 @@
+// Compile-time level plans for the shared-memory transforms.
+#pragma once
+#include "ntt_engine.cuh"
+
+namespace cmb {
+
+// Plan for a contiguous transform of length 2^logl held in shared memory.
+// The last level always has radix 32: every earlier level then has at least
+// 32 tasks per block, so 32 lanes touch 32 consecutive words (no bank
+// conflicts), and the last level reads whole 32-word rows with 16-byte
+// accesses through the swizzle.  Earlier levels use radix <= 16 so that a
+// thread can hold both operands of a product (2 x 16 registers).
+__host__ __device__ constexpr LevelPlan row_plan(int logl) {
+    switch (logl) {
+        case 5: return LevelPlan{1, {5}};
+        case 6: return LevelPlan{2, {1, 5}};
+        case 7: return LevelPlan{2, {2, 5}};
+        case 8: return LevelPlan{2, {3, 5}};
+        case 9: return LevelPlan{2, {4, 5}};
+        case 10: return LevelPlan{3, {2, 3, 5}};
+        case 11: return LevelPlan{3, {3, 3, 5}};
+        case 12: return LevelPlan{3, {3, 4, 5}};
+        case 13: return LevelPlan{3, {4, 4, 5}};
+        case 14: return LevelPlan{4, {2, 3, 4, 5}};
+        default: return LevelPlan{0, {0}};
+    }
+}
+
+// Plan for a batch of interleaved columns (lane = column): bank conflicts do
+// not depend on the radix, so fewer, wider levels are used.
+__host__ __device__ constexpr LevelPlan col_plan(int logl) {
+    switch (logl) {
+        case 1: return LevelPlan{1, {1}};
+        case 2: return LevelPlan{1, {2}};
+        case 3: return LevelPlan{1, {3}};
+        case 4: return LevelPlan{1, {4}};
+        case 5: return LevelPlan{2, {2, 3}};
+        case 6: return LevelPlan{2, {3, 3}};
+        case 7: return LevelPlan{2, {3, 4}};
+        case 8: return LevelPlan{2, {4, 4}};
+        case 9: return LevelPlan{3, {3, 3, 3}};
+        case 10: return LevelPlan{3, {3, 3, 4}};
+        case 11: return LevelPlan{3, {3, 4, 4}};
+        case 12: return LevelPlan{3, {4, 4, 4}};
+        default: return LevelPlan{0, {0}};
+    }
+}
+
+// Threads and products per CTA for the fused single-CTA product of length L.
+__host__ __device__ constexpr int small_threads(int logl) { return logl >= 12 ? (1 << (logl - 5)) : 128; }
+__host__ __device__ constexpr int small_ppc(int logl) { return logl >= 12 ? 1 : (1 << (12 - logl)); }
+
+}  // namespace cmb

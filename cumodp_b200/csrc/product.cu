@@ -1,0 +1,220 @@
+// Product dispatch: size classes, kernel instantiation tables, launches.
+#include "product.cuh"
+
+#include <algorithm>
+#include <cstring>
+
+namespace cmb {
+
+namespace {
+
+template <int LOGL>
+void launch_small_t(const SmallArgs& a, int nctas, cudaStream_t st) {
+    constexpr int L = 1 << LOGL;
+    const size_t smem = (size_t)small_ppc(LOGL) * 2 * L * sizeof(u32);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_small_product<LOGL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    k_small_product<LOGL><<<nctas, small_threads(LOGL), smem, st>>>(a);
+}
+
+typedef void (*SmallFn)(const SmallArgs&, int, cudaStream_t);
+const SmallFn kSmall[15] = {nullptr, nullptr, nullptr, nullptr, nullptr,
+                            launch_small_t<5>, launch_small_t<6>, launch_small_t<7>,
+                            launch_small_t<8>, launch_small_t<9>, launch_small_t<10>,
+                            launch_small_t<11>, launch_small_t<12>, launch_small_t<13>,
+                            launch_small_t<14>};
+
+constexpr int kColWarps = 8;
+
+template <int L1>
+void launch_col_fwd_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
+    const size_t smem = (size_t)(1 << L1) * 32 * sizeof(u32);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_col_fwd<L1, kColWarps>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    k_col_fwd<L1, kColWarps><<<grid, kColWarps * 32, smem, st>>>(a);
+}
+template <int L1>
+void launch_col_inv_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
+    const size_t smem = (size_t)(1 << L1) * 32 * sizeof(u32);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_col_inv<L1, kColWarps>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    k_col_inv<L1, kColWarps><<<grid, kColWarps * 32, smem, st>>>(a);
+}
+template <int L2>
+void launch_row_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
+    const size_t smem = (size_t)2 * (1 << L2) * sizeof(u32);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_row_fused<L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    k_row_fused<L2><<<grid, small_threads(L2), smem, st>>>(a);
+}
+
+typedef void (*PassFn)(const LargeArgs&, dim3, cudaStream_t);
+const PassFn kColFwd[11] = {nullptr, launch_col_fwd_t<1>, launch_col_fwd_t<2>, launch_col_fwd_t<3>,
+                            launch_col_fwd_t<4>, launch_col_fwd_t<5>, launch_col_fwd_t<6>,
+                            launch_col_fwd_t<7>, launch_col_fwd_t<8>, launch_col_fwd_t<9>,
+                            launch_col_fwd_t<10>};
+const PassFn kColInv[11] = {nullptr, launch_col_inv_t<1>, launch_col_inv_t<2>, launch_col_inv_t<3>,
+                            launch_col_inv_t<4>, launch_col_inv_t<5>, launch_col_inv_t<6>,
+                            launch_col_inv_t<7>, launch_col_inv_t<8>, launch_col_inv_t<9>,
+                            launch_col_inv_t<10>};
+const PassFn kRow[15] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                         launch_row_t<6>, launch_row_t<7>, launch_row_t<8>, launch_row_t<9>,
+                         launch_row_t<10>, launch_row_t<11>, launch_row_t<12>, launch_row_t<13>,
+                         launch_row_t<14>};
+
+template <int LOGL>
+void attr_small() {
+    cudaFuncSetAttribute(k_small_product<LOGL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)((size_t)small_ppc(LOGL) * 2 * (1 << LOGL) * sizeof(u32)));
+}
+template <int L1>
+void attr_col() {
+    const int smem = (1 << L1) * 32 * (int)sizeof(u32);
+    cudaFuncSetAttribute(k_col_fwd<L1, kColWarps>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_col_inv<L1, kColWarps>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+}
+template <int L2>
+void attr_row() {
+    cudaFuncSetAttribute(k_row_fused<L2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         2 * (1 << L2) * (int)sizeof(u32));
+}
+
+int ceil_log2(long long s) {
+    int k = 0;
+    while ((1ll << k) < s) ++k;
+    return k;
+}
+
+}  // namespace
+
+void ensure_kernel_attrs() {
+    static std::once_flag once;
+    std::call_once(once, [] {
+        attr_small<5>(); attr_small<6>(); attr_small<7>(); attr_small<8>(); attr_small<9>();
+        attr_small<10>(); attr_small<11>(); attr_small<12>(); attr_small<13>(); attr_small<14>();
+        attr_col<1>(); attr_col<2>(); attr_col<3>(); attr_col<4>(); attr_col<5>();
+        attr_col<6>(); attr_col<7>(); attr_col<8>(); attr_col<9>(); attr_col<10>();
+        attr_row<6>(); attr_row<7>(); attr_row<8>(); attr_row<9>(); attr_row<10>();
+        attr_row<11>(); attr_row<12>(); attr_row<13>(); attr_row<14>();
+    });
+}
+
+int product_logn(long long la, long long lb) {
+    return std::max(kMinLog, ceil_log2(la + lb - 1));
+}
+
+int default_row_log(int logn) {
+    // rows of 2^l2 words, columns of 2^(logn-l2): columns as long as the
+    // 32-column tile fits shared memory (n1 <= 2^10), rows as long as one
+    // CTA can hold both operands (n2 <= 2^14)
+    int l2 = std::max(logn - kMaxColLog, 7);
+    return std::min(l2, kMaxRowLog);
+}
+
+int small_args(const PrimeCtx& pc, u32 root, int logn, int dev, SmallArgs* a) {
+    int err = OK;
+    const Tw* tw = row_tables(dev, pc.info.p, root, logn, &err);
+    if (!tw) return err;
+    const u32 p = pc.info.p;
+    memset(a, 0, sizeof(*a));
+    a->pk = pc.pk;
+    // 2^32 / L: undoes the Montgomery 2^-32 of the pointwise product and
+    // the factor L of the unnormalised inverse
+    const u32 linv = powmod_exact((u32)((1ull << logn) % p), p - 2, p);
+    a->scale = tw_of(mulmod_exact(linv, pc.info.r1, p), p);
+    a->tw = tw;
+    a->tw_inv_off = plan_tw_entries(row_plan(logn), logn);
+    return OK;
+}
+
+int large_args(const PrimeCtx& pc, u32 root_n, int logn, int l2, int dev, LargeArgs* a) {
+    int err = OK;
+    const u32 p = pc.info.p;
+    const int l1 = logn - l2;
+    const u32 root_r = powmod_exact(root_n, 1ull << l1, p);  // w_n2
+    const u32 root_c = powmod_exact(root_n, 1ull << l2, p);  // w_n1
+    const Tw* twr = row_tables(dev, p, root_r, l2, &err);
+    const Tw* twc = col_tables(dev, p, root_c, l1, &err);
+    const u32* seeds = seed_tables(dev, p, root_n, logn, &err);
+    if (!twr || !twc || !seeds) return err ? err : OUT_OF_MEMORY;
+    memset(a, 0, sizeof(*a));
+    a->pk = pc.pk;
+    a->pkc = pc.pk;
+    a->twr = twr;
+    a->twc = twc;
+    a->twr_inv = plan_tw_entries(row_plan(l2), l2);
+    a->twc_inv = plan_tw_entries(col_plan(l1), l1);
+    a->seeds = seeds;
+    a->nlo = (int)std::min<long long>(1ll << logn, 4096);
+    a->nhi = (int)std::max<long long>(1, (1ll << logn) / 4096);
+    const u32 ninv = powmod_exact((u32)((1ull << logn) % p), p - 2, p);
+    a->scale_rn = mulmod_exact(ninv, pc.info.r1, p);
+    a->l1 = l1;
+    a->l2 = l2;
+    a->colpl = col_plan(l1);
+    return OK;
+}
+
+void launch_small(int logn, const SmallArgs& a, int njobs, cudaStream_t st) {
+    const int ppc = small_ppc(logn);
+    kSmall[logn](a, (njobs + ppc - 1) / ppc, st);
+}
+
+void launch_large(const LargeArgs& a, int njobs, cudaStream_t st) {
+    const int n1 = 1 << a.l1, n2 = 1 << a.l2;
+    kColFwd[a.l1](a, dim3(n2 / 32, 2, njobs), st);
+    kRow[a.l2](a, dim3(n1, njobs, 1), st);
+    kColInv[a.l1](a, dim3(n2 / 32, 1, njobs), st);
+}
+
+int mul_dev(const u32* a, long long la, const u32* b, long long lb, u32* h, long long lh, u32 p,
+            cudaStream_t st) {
+    if (la <= 0 || lb <= 0 || lh < 0) return ASSUMPTION_ERROR;
+    if (lh == 0) return OK;
+    int err = OK;
+    const PrimeCtx* pc = prime_ctx(p, &err);
+    if (!pc) return err;
+    const int logn = product_logn(la, lb);
+    if (logn > pc->info.two_adic) return FFT_SIZE_TOO_LARGE;
+    if (logn > kMaxLog) return FFT_SIZE_TOO_LARGE;
+    const long long n = 1ll << logn;
+    const int dev = current_device();
+    ensure_kernel_attrs();
+    if (lh > n) {  // coefficients beyond the transform length are zero
+        cudaError_t e = cudaMemsetAsync(h + n, 0, (size_t)(lh - n) * sizeof(u32), st);
+        if (e != cudaSuccess) return cuda_err(e);
+        lh = n;
+    }
+    const u32 root = canonical_root(*pc, logn);
+    if (logn <= kMaxSmallLog) {
+        SmallArgs A;
+        if ((err = small_args(*pc, root, logn, dev, &A)) != OK) return err;
+        A.job0 = ProdJob{a, b, h, (int)la, (int)lb, (int)lh, 0};
+        A.njobs = 1;
+        launch_small(logn, A, 1, st);
+    } else {
+        const int l2 = default_row_log(logn);
+        LargeArgs A;
+        if ((err = large_args(*pc, root, logn, l2, dev, &A)) != OK) return err;
+        u32* ws = (u32*)workspace(dev, kWsSingle, (size_t)2 * n * sizeof(u32), &err);
+        if (!ws) return err;
+        A.job0 = LargeJob{a, b, h, (int)la, (int)lb, (int)lh, 0, ws, ws + n};
+        A.njobs = 1;
+        launch_large(A, 1, st);
+    }
+    return cuda_err(cudaGetLastError());
+}
+
+}  // namespace cmb

@@ -1,0 +1,36 @@
+// Host-side product dispatch shared by the C entry points.
+#pragma once
+#include "large_product.cuh"
+#include "runtime.cuh"
+
+namespace cmb {
+
+constexpr int kMinLog = 5;        // smallest transform: one radix-32 row
+constexpr int kMaxSmallLog = 14;  // largest single-CTA product (2 x 64 KiB of shared memory)
+constexpr int kMaxColLog = 10;    // 32-column tile of 2^10 rows = 128 KiB of shared memory
+constexpr int kMaxRowLog = 14;
+constexpr int kMinRowLog = 6;
+constexpr int kMaxLog = kMaxColLog + kMaxRowLog;  // 2^24
+
+// workspace slots (runtime.cuh: workspace)
+enum WsSlot { kWsSingle = 0, kWsBatch = 1, kWsStage = 2, kWsNtt = 3, kWsTwoConv = 4, kWsServer = 5 };
+
+// Transform length log2 for a product of la and lb coefficients.
+int product_logn(long long la, long long lb);
+// Default row length log2 of the three-pass split.
+int default_row_log(int logn);
+
+int small_args(const PrimeCtx& pc, u32 root, int logn, int dev, SmallArgs* a);
+int large_args(const PrimeCtx& pc, u32 root_n, int logn, int l2, int dev, LargeArgs* a);
+void launch_small(int logn, const SmallArgs& a, int njobs, cudaStream_t st);
+void launch_large(const LargeArgs& a, int njobs, cudaStream_t st);
+
+// Sets the shared-memory limits of every product kernel once (must run
+// before any launch is captured into a graph).
+void ensure_kernel_attrs();
+
+// h[0..lh) = a[0..la) * b[0..lb) mod p on device pointers, on stream st.
+int mul_dev(const u32* a, long long la, const u32* b, long long lb, u32* h, long long lh, u32 p,
+            cudaStream_t st);
+
+}  // namespace cmb

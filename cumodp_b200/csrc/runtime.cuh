@@ -1,0 +1,83 @@
+// Host runtime shared by every entry point: prime set-up, resident twiddle
+// tables, per-device workspace and the error convention.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "ntt_engine.cuh"
+#include "plans.cuh"
+
+namespace cmb {
+
+// Numeric codes of the reference's cumodp_err (include/types.h:123-146).
+enum Err : int {
+    OK = 0x000,
+    FAILURE = 0x001,
+    ASSUMPTION_ERROR = 0x002,
+    NO_CUDA_DEVICE = 0x100,
+    FFT_ERROR = 0x200,
+    FOURIER_DEGREE_TOO_SMALL = 0x201,
+    FFT_SIZE_TOO_LARGE = 0x202,
+    FFT_SIZE_TOO_SMALL = 0x203,
+    OUT_OF_MEMORY = 0x401,
+};
+
+// Everything the kernels need to know about one prime (and one root family).
+struct PrimeCtx {
+    PrimeInfo info;
+    u32 root_max;  // canonical primitive 2^two_adic-th root
+    PrimeK pk;     // kernel constants for the canonical roots
+};
+
+// Validates p (odd prime < 2^30 with 2-adic order >= 5) and returns the
+// cached context, or nullptr with *err set.
+const PrimeCtx* prime_ctx(u32 p, int* err);
+
+// Root helpers (exact host arithmetic).
+u32 canonical_root(const PrimeCtx& pc, int logn);  // primitive 2^logn-th root
+PrimeK make_prime_k(const PrimeInfo& pi, u32 w32);  // w32: a primitive 32nd root
+// Constants for register DFTs of a transform of length 2^logl with the
+// primitive root `root`; below length 32 only the entries radix-2^logl
+// butterflies read are filled.
+PrimeK make_prime_k_for(const PrimeInfo& pi, u32 root, int logl);
+Tw tw_of(u32 w, u32 p);
+
+// Device-resident tables for the row (contiguous) plan of length 2^logl
+// built from the primitive 2^logl-th root `root`; forward tables first, the
+// inverse tables start at plan_tw_entries(row_plan(logl), logl).
+const Tw* row_tables(int dev, u32 p, u32 root, int logl, int* err);
+// Same for the interleaved-column plan.
+const Tw* col_tables(int dev, u32 p, u32 root, int logl, int* err);
+// Inter-pass twiddle seeds for a two-pass transform of length 2^logn:
+// lo[e] = w^e (e < 2^12) and hi[e] = w^(e << 12) (e < 2^(logn-12)), both in
+// Montgomery form times R (w^e * 2^64 mod p) so that one Montgomery product
+// of two entries yields w^(lo+hi) * 2^32.
+const u32* seed_tables(int dev, u32 p, u32 root, int logn, int* err);
+
+// Per-device scratch that grows on demand (never shrinks while the process
+// lives).  Each call site names a slot so concurrent users do not collide.
+void* workspace(int dev, int slot, size_t bytes, int* err);
+
+// The stream every synchronous entry point issues its work on.
+cudaStream_t lib_stream(int dev);
+
+// Serialises host entry points that share workspace and caches.
+std::mutex& lib_mutex();
+
+int current_device();
+
+// Device bytes held by the caches and workspace of this process.
+size_t bytes_in_use();
+// Records an allocation made outside the caches (plans, server pools).
+void account_bytes(long long delta);
+
+// Copies the last CUDA error (if any) into a library code.
+int cuda_err(cudaError_t e);
+
+}  // namespace cmb

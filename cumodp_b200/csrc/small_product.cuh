@@ -1,0 +1,226 @@
+// Fused single-CTA polynomial product for transform lengths L = 2^5 .. 2^14.
+//
+// One kernel does what the reference spreads over ~110 synchronised launches
+// for one product (src/stockham.cu:521-611: expand_to_fft_dev x2,
+// stockham_dev x3, get_powers_binary x2, pointwise_mul_dev,
+// scale_vector_dev): load both operands with the zero pad, forward DIF of
+// both (sharing every twiddle load), pointwise Montgomery product with the
+// 1/L scale folded in, inverse DIT, truncation and store of the canonical
+// residues.  Products of one size class are batched: each CTA holds
+// `small_ppc` products and the grid covers the whole class.
+#pragma once
+#include "plans.cuh"
+
+namespace cmb {
+
+// One product job: h[0..lh) = (a[0..la) * b[0..lb)) mod p, coefficient
+// order; a, b, h are device pointers (h may alias a or b only when the job
+// is the sole job reading them).
+struct ProdJob {
+    const u32* a;
+    const u32* b;
+    u32* h;
+    int la, lb, lh;
+    int pad;
+};
+
+// What the shared-memory row levels need: prime constants and the plan's
+// twiddle tables.
+struct RowCtx {
+    PrimeK pk;
+    const Tw* __restrict__ tw;  // forward level tables, then inverse tables
+    int tw_inv_off;
+};
+
+struct SmallArgs {
+    PrimeK pk;
+    Tw scale;               // 2^32 / L mod p in Shoup form (undoes Montgomery R and 1/L)
+    const Tw* __restrict__ tw;  // plan tables: forward levels then inverse levels
+    const ProdJob* __restrict__ jobs;  // device job table, or nullptr: use job0
+    int njobs;
+    int tw_inv_off;         // entries before the inverse tables
+    ProdJob job0;           // the single job when jobs == nullptr
+};
+
+#ifdef __CUDACC__
+
+template <int LOGL, int LEV>
+struct SmallLevel {
+    static constexpr LevelPlan PL = row_plan(LOGL);
+    static constexpr int R = 1 << PL.logr[LEV];
+    // block size and table offset of this level
+    static constexpr int LOGB = [] {
+        int lb = LOGL;
+        for (int i = 0; i < LEV; ++i) lb -= PL.logr[i];
+        return lb;
+    }();
+    static constexpr int B = 1 << LOGB;
+    static constexpr int TB = B / R;
+    static constexpr int TWOFF = [] {
+        int n = 0, lb = LOGL;
+        for (int i = 0; i < LEV; ++i) { n += 1 << lb; lb -= PL.logr[i]; }
+        return n;
+    }();
+};
+
+// Forward non-last level on both operands of every product in the CTA.
+template <int LOGL, int LEV, int T, int PPC, class Ctx>
+__device__ __forceinline__ void small_fwd_level(u32* sm, const Ctx& A) {
+    using LV = SmallLevel<LOGL, LEV>;
+    constexpr int L = 1 << LOGL, R = LV::R, TB = LV::TB, B = LV::B;
+    constexpr int TASKS = PPC * (L / R);
+    const u32 p = A.pk.p, p2 = A.pk.p2;
+    for (int id = threadIdx.x; id < TASKS; id += T) {
+        const int q = id / (L / R);
+        const int rest = id % (L / R);
+        const int blk = rest / TB, o = rest % TB;
+        const int base = q * 2 * L + blk * B + o;
+        u32 xf[R], xg[R];
+#pragma unroll
+        for (int m = 0; m < R; ++m) {
+            xf[m] = sm[swz(base + TB * m)];
+            xg[m] = sm[swz(base + L + TB * m)];
+        }
+        dif_regs<R>(xf, A.pk.rc.f, p, p2);
+        dif_regs<R>(xg, A.pk.rc.f, p, p2);
+        Tw t[R];
+        load_tw<R>(t, A.tw + LV::TWOFF + o * R);
+#pragma unroll
+        for (int j = 1; j < R; ++j) {
+            xf[j] = mul_shoup(xf[j], t[j].w, t[j].wq, p);
+            xg[j] = mul_shoup(xg[j], t[j].w, t[j].wq, p);
+        }
+#pragma unroll
+        for (int m = 0; m < R; ++m) {
+            sm[swz(base + TB * m)] = xf[m];
+            sm[swz(base + L + TB * m)] = xg[m];
+        }
+    }
+}
+
+// Inverse non-last level on the product held in the first operand slot.
+template <int LOGL, int LEV, int T, int PPC, class Ctx>
+__device__ __forceinline__ void small_inv_level(u32* sm, const Ctx& A) {
+    using LV = SmallLevel<LOGL, LEV>;
+    constexpr int L = 1 << LOGL, R = LV::R, TB = LV::TB, B = LV::B;
+    constexpr int TASKS = PPC * (L / R);
+    const u32 p = A.pk.p, p2 = A.pk.p2;
+    for (int id = threadIdx.x; id < TASKS; id += T) {
+        const int q = id / (L / R);
+        const int rest = id % (L / R);
+        const int blk = rest / TB, o = rest % TB;
+        const int base = q * 2 * L + blk * B + o;
+        u32 x[R];
+#pragma unroll
+        for (int m = 0; m < R; ++m) x[m] = sm[swz(base + TB * m)];
+        Tw t[R];
+        load_tw<R>(t, A.tw + A.tw_inv_off + LV::TWOFF + o * R);
+#pragma unroll
+        for (int j = 1; j < R; ++j) x[j] = mul_shoup(x[j], t[j].w, t[j].wq, p);
+        dit_regs<R>(x, A.pk.rc.i, p, p2);
+#pragma unroll
+        for (int m = 0; m < R; ++m) sm[swz(base + TB * m)] = x[m];
+    }
+}
+
+// Forward levels LEV .. nlev-2 (every level but the last).
+template <int LOGL, int LEV, int T, int PPC, class Ctx>
+__device__ __forceinline__ void small_fwd_levels(u32* sm, const Ctx& A) {
+    constexpr LevelPlan PL = row_plan(LOGL);
+    if constexpr (LEV + 1 < PL.nlev) {
+        small_fwd_level<LOGL, LEV, T, PPC>(sm, A);
+        __syncthreads();
+        small_fwd_levels<LOGL, LEV + 1, T, PPC>(sm, A);
+    }
+}
+
+// Inverse levels LEV, LEV-1, ..., STOP.
+template <int LOGL, int LEV, int T, int PPC, int STOP, class Ctx>
+__device__ __forceinline__ void small_inv_levels(u32* sm, const Ctx& A) {
+    if constexpr (LEV >= STOP) {
+        small_inv_level<LOGL, LEV, T, PPC>(sm, A);
+        __syncthreads();
+        small_inv_levels<LOGL, LEV - 1, T, PPC, STOP>(sm, A);
+    }
+}
+
+__device__ __forceinline__ void load_row32(u32 (&x)[32], const u32* sm, int base) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        uint4 v = *reinterpret_cast<const uint4*>(sm + swz(base + 4 * c));
+        x[4 * c] = v.x; x[4 * c + 1] = v.y; x[4 * c + 2] = v.z; x[4 * c + 3] = v.w;
+    }
+}
+__device__ __forceinline__ void store_row32(u32* sm, int base, const u32 (&x)[32]) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+        *reinterpret_cast<uint4*>(sm + swz(base + 4 * c)) =
+            make_uint4(x[4 * c], x[4 * c + 1], x[4 * c + 2], x[4 * c + 3]);
+}
+
+template <int LOGL>
+__global__ void __launch_bounds__(small_threads(LOGL), 1)
+k_small_product(const __grid_constant__ SmallArgs A) {
+    constexpr int L = 1 << LOGL;
+    constexpr int T = small_threads(LOGL);
+    constexpr int PPC = small_ppc(LOGL);
+    constexpr LevelPlan PL = row_plan(LOGL);
+    extern __shared__ __align__(16) u32 sm[];
+    __shared__ ProdJob jobs[PPC];
+
+    const int job0 = blockIdx.x * PPC;
+    for (int q = threadIdx.x; q < PPC; q += T) {
+        if (job0 + q < A.njobs) jobs[q] = A.jobs ? A.jobs[job0 + q] : A.job0;
+        else jobs[q] = ProdJob{nullptr, nullptr, nullptr, 0, 0, 0, 0};
+    }
+    __syncthreads();
+
+    const u32 p = A.pk.p, p2 = A.pk.p2, oneq = A.pk.one_q;
+    // load + zero pad + reduce to [0, 2p)
+    for (int idx = threadIdx.x; idx < PPC * 2 * L; idx += T) {
+        const int q = idx / (2 * L);
+        const int op = (idx / L) & 1;
+        const int i = idx % L;
+        const ProdJob& J = jobs[q];
+        const u32* src = op ? J.b : J.a;
+        const int len = op ? J.lb : J.la;
+        u32 v = (i < len) ? __ldg(src + i) : 0u;
+        sm[swz(idx)] = mul_shoup(v, 1u, oneq, p);
+    }
+    __syncthreads();
+
+    small_fwd_levels<LOGL, 0, T, PPC>(sm, A);
+
+    // last level (radix 32) forward on both operands, pointwise, inverse
+    for (int id = threadIdx.x; id < PPC * (L / 32); id += T) {
+        const int q = id / (L / 32);
+        const int row = id % (L / 32);
+        const int base = q * 2 * L + row * 32;
+        u32 xf[32], xg[32];
+        load_row32(xf, sm, base);
+        load_row32(xg, sm, base + L);
+        dif_regs<32>(xf, A.pk.rc.f, p, p2);
+        dif_regs<32>(xg, A.pk.rc.f, p, p2);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            u32 h = mul_mont(xf[j], xg[j], p, A.pk.pinv_neg);
+            xf[j] = mul_shoup(h, A.scale.w, A.scale.wq, p);
+        }
+        dit_regs<32>(xf, A.pk.rc.i, p, p2);
+        store_row32(sm, base, xf);
+    }
+    __syncthreads();
+
+    small_inv_levels<LOGL, PL.nlev - 2, T, PPC, 0>(sm, A);
+
+    // truncate + canonical residues
+    for (int idx = threadIdx.x; idx < PPC * L; idx += T) {
+        const int q = idx / L, i = idx % L;
+        const ProdJob& J = jobs[q];
+        if (i < J.lh) J.h[i] = red1(red2(sm[swz(q * 2 * L + i)], p2), p);
+    }
+}
+
+#endif  // __CUDACC__
+
+}  // namespace cmb

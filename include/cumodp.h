@@ -1,0 +1,168 @@
+/*
+ * cumodp.h -- C entry points of the B200 polynomial-product library.
+ *
+ * Drop-in for the reference's include/cumodp.h (FFT / FFT-multiplication
+ * part).  Every reference entry point keeps its name, argument meaning and
+ * numeric error codes; where the reference silently misbehaved the deviation
+ * is listed at the function.  Functions marked "addition" have no
+ * counterpart in the reference.
+ *
+ * Coefficients are sfixn = 32-bit int holding residues in [0, p); p is an
+ * odd "Fourier" prime p = c * 2^e + 1 below 2^30.  Unless noted, pointers
+ * are HOST pointers and results are complete when the call returns.  All
+ * entry points are thread-safe (calls are serialised per process).
+ */
+#ifndef CUMODP_B200_H
+#define CUMODP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The library is built with hidden visibility; everything declared here is
+ * exported. */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+/* include/types.h:45-53 under LINUXINTEL64 */
+typedef int32_t sfixn;
+
+/* Same numeric values as the reference enum (include/types.h:123-146). */
+typedef enum {
+    CUMODP_SUCCESS = 0x000,
+    CUMODP_FAILURE = 0x001,
+    CUMODP_ASSUMPTION_ERROR = 0x002,
+    CUMODP_NO_CUDA_DEVICE = 0x100,
+    CUMODP_HAS_CUDA_DEVICE = 0x101,
+    CUMODP_FFT_ERROR = 0x200,
+    CUMODP_FOURIER_DEGREE_TOO_SMALL = 0x201,
+    CUMODP_FFT_SIZE_TOO_LARGE = 0x202,
+    CUMODP_FFT_SIZE_TOO_SMALL = 0x203,
+    CUMODP_SUBRES_ERROR = 0x300,
+    CUMODP_SUBRES_COARSE_ERROR = 0x301,
+    CUMODP_SUBRES_FINE_ERROR = 0x302,
+    CUMODP_SUBRES_NON_REGULAR = 0x303,
+    CUMODP_RES2_ERROR = 0x304,
+    CUMODP_RES3_ERROR = 0x305,
+    CUMODP_OUT_OF_MEMORY = 0x401,
+    CUMODP_UNKNOWN_ERROR = 0x999
+} cumodp_err;
+
+/* ------------------------------------------------------ device queries -- */
+/* Replace src/modpn.cu:51-57. */
+int is_cuda_enabled(void);
+/* Replaces src/modpn.cu:62-67. */
+int num_of_cuda_devices(void);
+/* Replaces src/modpn.cu:72-88 (every sm_100 device has fp64: 1 with a device). */
+int is_double_float_enabled(void);
+/* Replaces src/modpn.cu:93-98; saturates at 4 GiB - 1 like the reference's
+ * unsigned int return type truncates. */
+unsigned int global_memory_in_bytes(void);
+/* Replaces src/modpn.cu:103-108. */
+float global_memory_in_megabytes(void);
+/* Replaces src/modpn.cu:113-126: nonzero when a product of degrees df, dg
+ * fits this library's transform limits and the device's memory. */
+int can_call_fftmul_uni(sfixn df, sfixn dg);
+/* Replace src/modpn.cu:142-173.  The subresultant GPU path is not part of
+ * this library: always 0, so modpn keeps its CPU subresultant code. */
+int can_call_subres2(sfixn dx, sfixn d1, sfixn d2);
+int can_call_subres3(sfixn dx, sfixn dy, sfixn d1, sfixn d2);
+
+/* ------------------------------------------- FFT and FFT multiplication -- */
+/* In-place natural-order DFT of X (n = 2^k words): X[j] <- sum_i X[i] w^(ij)
+ * mod p, w a primitive n-th root.  Replaces src/modpn.cu:181-192
+ * (stockham_host, src/stockham.cu:479-487).  Deviation: invalid p, n != 2^k,
+ * or a w that is not a primitive n-th root return CUMODP_ASSUMPTION_ERROR;
+ * n above the prime's 2-adic order returns CUMODP_FFT_SIZE_TOO_LARGE (the
+ * reference computes garbage); n < 256 is supported (the reference's grid
+ * arithmetic breaks below k = 8). */
+cumodp_err cumodp_fft_uni(sfixn *X, sfixn n, sfixn k, sfixn w, sfixn p);
+/* Inverse: DFT with w^-1 then scaling by n^-1.  Replaces src/modpn.cu:197-210
+ * (inverse_stockham_host, src/stockham.cu:489-503). */
+cumodp_err cumodp_invfft_uni(sfixn *X, sfixn n, sfixn k, sfixn w, sfixn p);
+/* 2-D DFT of a row-major 2^em x 2^en array X: w_m-DFT down the columns
+ * (length 2^em) and w_n-DFT along the rows (length 2^en).  Replaces
+ * src/modpn.cu:215-244 (bivariate_stockham_host, src/list_stockham.cu).
+ * Deviation: em != en is computed correctly (the reference is square-only). */
+cumodp_err cumodp_fft_bivariate(sfixn *X, sfixn em, sfixn wm, sfixn en, sfixn wn, sfixn p);
+cumodp_err cumodp_invfft_bivariate(sfixn *X, sfixn em, sfixn wm, sfixn en, sfixn wn, sfixn p);
+/* H = F * G mod p: F has df+1 coefficients, G dg+1, H receives dh+1 words.
+ * Replaces src/modpn.cu:249-261 (stockham_poly_mul_host, src/stockham.cu:
+ * 562-611).  H may alias F or G (modpn multiplies in place, FMUL.c:1949).
+ * Deviations (documented fixes): every size is computed (the reference
+ * returns SUCCESS with H untouched below transform size 256); exactly dh+1
+ * words are written, zero beyond df+dg (the reference writes 2^ceil(log2
+ * (df+dg+1)) words whenever dh >= df+dg+1); nothing is printed. */
+cumodp_err cumodp_fftmul_uni(sfixn dh, sfixn *H, sfixn df, const sfixn *F,
+                             sfixn dg, const sfixn *G, sfixn p);
+
+/* --------------------------------------------------- out-of-scope stubs -- */
+/* The subresultant-chain and scube GPU code of the reference
+ * (src/modpn.cu:272-408) is not part of this library.  These symbols exist
+ * so that modpn links unchanged; each reports "not available" the way the
+ * reference does for unsupported cases, and modpn falls back to its CPU
+ * code (modpn/src/IteratedResultant.c:421-1253). */
+sfixn cumodp_subres_chain2_fine(sfixn *S, sfixn B, sfixn w, sfixn npx, sfixn npy, const sfixn *P,
+                                sfixn nqx, sfixn nqy, const sfixn *Q, sfixn p);
+sfixn cumodp_subres_chain2_coarse(sfixn *S, sfixn B, sfixn w, sfixn npx, sfixn npy, const sfixn *P,
+                                  sfixn nqx, sfixn nqy, const sfixn *Q, sfixn p);
+sfixn cumodp_subres_chain3_fine(sfixn *S, sfixn Bx, sfixn By, sfixn wx, sfixn wy, sfixn npx, sfixn npy,
+                                sfixn npz, const sfixn *P, sfixn nqx, sfixn nqy, sfixn nqz,
+                                const sfixn *Q, sfixn p);
+sfixn cumodp_subres_chain3_coarse(sfixn *S, sfixn Bx, sfixn By, sfixn wx, sfixn wy, sfixn npx,
+                                  sfixn npy, sfixn npz, const sfixn *P, sfixn nqx, sfixn nqy,
+                                  sfixn nqz, const sfixn *Q, sfixn p);
+void *init_cuda_scube(sfixn N, const sfixn *sz_p, const sfixn *sz_q, sfixn fp);
+void free_cuda_scube(void *scb);
+void print_cuda_scube(const void *scb);
+cumodp_err build_cuda_scube(void *scb, const sfixn *sz_p, const sfixn *P, const sfixn *sz_q,
+                            const sfixn *Q);
+const sfixn *interp_subres_coeff2(sfixn *nx, void *scb, sfixn i, sfixn j);
+const sfixn *interp_subres_coeff3(sfixn *nx, sfixn *ny, void *scb, sfixn i, sfixn j);
+
+/* ------------------------------------------------------------ additions -- */
+/* Addition.  Device-pointer product on a caller stream (0 = the library's
+ * stream, then synchronised).  F, G, H are DEVICE pointers; lh words of H
+ * are written.  Counterpart of the reference's C++ stockham_poly_mul_dev
+ * (src/stockham.cu:521-542) without its size-padding contract: inputs need
+ * no padding and are not modified. */
+cumodp_err cumodp_fftmul_uni_dev(sfixn lh, sfixn *H, sfixn df, const sfixn *F,
+                                 sfixn dg, const sfixn *G, sfixn p, void *stream);
+
+/* Addition.  Batched products mod one prime, all on the device: product i is
+ * H_i = F_i * G_i with F_i = F + f_off[i] (df[i]+1 words), G_i = G + g_off[i]
+ * (dg[i]+1 words), H_i = H + h_off[i] (df[i]+dg[i]+1 words).  f_off, g_off,
+ * h_off, df, dg are HOST arrays of length count; F, G, H are DEVICE
+ * pointers.  Products are grouped by transform size and run as one
+ * CUDA-graph launch; the plan (grouping, job tables, workspace) is cached
+ * per batch shape.  stream: 0 = library stream, then synchronised. */
+cumodp_err cumodp_fftmul_batch_dev(int count, const sfixn *df, const int64_t *f_off, const sfixn *F,
+                                   const sfixn *dg, const int64_t *g_off, const sfixn *G,
+                                   const int64_t *h_off, sfixn *H, sfixn p, void *stream);
+
+/* Addition.  Same as cumodp_fftmul_batch_dev with HOST F, G, H: copies in,
+ * computes and copies out (pinned staging, one H2D and one D2H copy). */
+cumodp_err cumodp_fftmul_batch(int count, const sfixn *df, const int64_t *f_off, const sfixn *F,
+                               const sfixn *dg, const int64_t *g_off, const sfixn *G,
+                               const int64_t *h_off, sfixn *H, sfixn p);
+
+/* Addition.  Bytes of device memory the library currently holds (tables,
+ * workspace, plans). */
+size_t cumodp_device_bytes_in_use(void);
+
+/* Addition.  Human-readable text of an error code. */
+const char *cumodp_error_string(cumodp_err e);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUMODP_B200_H */

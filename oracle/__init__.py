@@ -1,0 +1,242 @@
+"""CPU oracle for the polynomial product path (test infrastructure only).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline /
+reference arm import this package, and only as the checker or the timed CPU
+reference.  The shipped library (``cumodp_b200``) never imports it.
+
+Two shared libraries are wrapped here:
+
+* ``liboracle.so`` -- our plain-C restatement of the reference arithmetic
+  (``oracle.c``; each function cites the reference file:line it follows);
+* ``_ref/libmodpn_ref.so`` -- the reference's own CPU FFT multiply, modpn's
+  ``EX_Mont_FFTMul`` (modpn/src/FMUL.c:2015-2030), compiled from the
+  reference sources by ``oracle/Makefile`` (``make ref``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libmodpn_ref.so")
+
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
+_u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+
+
+def build(ref: bool = False) -> None:
+    """Compile liboracle.so (and the modpn reference when ``ref``)."""
+    subprocess.check_call(["make", "-s", "-C", HERE, "oracle"])
+    if ref:
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
+
+
+_lib = None
+_ref = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            build()
+        L = C.CDLL(ORACLE_SO)
+        L.or_pow.restype = C.c_uint32
+        L.or_pow.argtypes = [C.c_uint32, C.c_uint64, C.c_uint32]
+        L.or_inv.restype = C.c_uint32
+        L.or_inv.argtypes = [C.c_uint32, C.c_uint32]
+        L.or_fourier_degree.restype = C.c_int
+        L.or_fourier_degree.argtypes = [C.c_uint32]
+        L.or_primitive_root.restype = C.c_uint32
+        L.or_primitive_root.argtypes = [C.c_int, C.c_uint32]
+        L.or_dft_naive.argtypes = [C.c_int, _u32p, C.c_uint32, C.c_uint32, _u32p]
+        L.or_ntt.argtypes = [_u32p, C.c_int, C.c_uint32, C.c_uint32]
+        L.or_intt.argtypes = [_u32p, C.c_int, C.c_uint32, C.c_uint32]
+        L.or_polymul_school.argtypes = [C.c_int, _u32p, C.c_int, _u32p, _u32p, C.c_uint32]
+        L.or_polymul_ntt.restype = C.c_int
+        L.or_polymul_ntt.argtypes = [C.c_int, _u32p, C.c_int, _u32p, _u32p, C.c_uint32]
+        L.or_polymul_i128.argtypes = [C.c_int, _i64p, C.c_int, _i64p, _u64p]
+        L.or_bit_width.restype = C.c_int
+        L.or_bit_width.argtypes = [C.c_int, _i64p, C.c_int, _i64p]
+        L.or_limb_split.argtypes = [C.c_int, _i64p, C.c_int, C.c_int, C.c_uint32, _u32p]
+        L.or_scale_x.argtypes = [C.c_int, _u32p, C.c_int, C.c_uint32, C.c_uint32]
+        L.or_crt_signed.argtypes = [C.c_int, _u32p, _u32p, C.POINTER(C.c_uint64),
+                                    C.POINTER(C.c_uint64)]
+        _lib = L
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    """The compiled reference (modpn) CPU product; raises if it was not built."""
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_SO):
+            raise FileNotFoundError(f"{REF_SO} not built (make -C oracle ref)")
+        L = C.CDLL(REF_SO)
+        L.ref_init_prime.restype = C.c_int
+        L.ref_init_prime.argtypes = [C.c_int32]
+        L.ref_fftmul.restype = C.c_int
+        L.ref_fftmul.argtypes = [C.c_int32, _i32p, C.c_int32, _i32p, _i32p, C.c_int32]
+        _l = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
+        L.ref_fftmul_batch.restype = C.c_int
+        L.ref_fftmul_batch.argtypes = [C.c_int, _i32p, _l, _i32p, _i32p, _l, _i32p, _l,
+                                       _i32p, C.c_int32, C.c_int]
+        _ref = L
+    return _ref
+
+
+# ------------------------------------------------------------ python API --
+
+def pow_mod(a: int, e: int, p: int) -> int:
+    return int(lib().or_pow(a, e, p))
+
+
+def inv_mod(a: int, p: int) -> int:
+    return int(lib().or_inv(a, p))
+
+
+def fourier_degree(p: int) -> int:
+    return int(lib().or_fourier_degree(p))
+
+
+def primitive_root(e: int, p: int) -> int:
+    """The reference's deterministic 2^e-th root (include/inlines.h:460-485)."""
+    return int(lib().or_primitive_root(e, p))
+
+
+def dft_naive(x: np.ndarray, w: int, p: int) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.uint32)
+    out = np.empty_like(x)
+    lib().or_dft_naive(len(x), x, w, p, out)
+    return out
+
+
+def ntt(x: np.ndarray, w: int, p: int) -> np.ndarray:
+    x = np.array(x, dtype=np.uint32, copy=True)
+    k = int(len(x)).bit_length() - 1
+    assert len(x) == 1 << k
+    lib().or_ntt(x, k, w, p)
+    return x
+
+
+def intt(x: np.ndarray, w: int, p: int) -> np.ndarray:
+    x = np.array(x, dtype=np.uint32, copy=True)
+    k = int(len(x)).bit_length() - 1
+    assert len(x) == 1 << k
+    lib().or_intt(x, k, w, p)
+    return x
+
+
+def polymul_school(a: np.ndarray, b: np.ndarray, p: int) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.uint32)
+    b = np.ascontiguousarray(b, dtype=np.uint32)
+    h = np.empty(len(a) + len(b) - 1, dtype=np.uint32)
+    lib().or_polymul_school(len(a) - 1, a, len(b) - 1, b, h, p)
+    return h
+
+
+def polymul(a: np.ndarray, b: np.ndarray, p: int) -> np.ndarray:
+    """Product mod p through the oracle's own radix-2 transforms."""
+    a = np.ascontiguousarray(a, dtype=np.uint32)
+    b = np.ascontiguousarray(b, dtype=np.uint32)
+    h = np.empty(len(a) + len(b) - 1, dtype=np.uint32)
+    if lib().or_polymul_ntt(len(a) - 1, a, len(b) - 1, b, h, p) != 0:
+        raise ValueError("transform size exceeds the prime's 2-adic order")
+    return h
+
+
+def polymul_i128(a: np.ndarray, b: np.ndarray) -> list[int]:
+    """Exact integer product (Python ints) by __int128 schoolbook."""
+    a = np.ascontiguousarray(a, dtype=np.int64)
+    b = np.ascontiguousarray(b, dtype=np.int64)
+    n = len(a) + len(b) - 1
+    h = np.empty(2 * n, dtype=np.uint64)
+    lib().or_polymul_i128(len(a) - 1, a, len(b) - 1, b, h)
+    return i128_pairs_to_int(h)
+
+
+def i128_pairs_to_int(h: np.ndarray) -> list[int]:
+    lo = h[0::2].astype(object)
+    hi = h[1::2].astype(object)
+    out = []
+    for l, hh in zip(lo, hi):
+        v = int(l) | (int(hh) << 64)
+        if v >= 1 << 127:
+            v -= 1 << 128
+        out.append(v)
+    return out
+
+
+def bit_width(a: np.ndarray, b: np.ndarray) -> int:
+    a = np.ascontiguousarray(a, dtype=np.int64)
+    b = np.ascontiguousarray(b, dtype=np.int64)
+    return int(lib().or_bit_width(len(a), a, len(b), b))
+
+
+def limb_split(a: np.ndarray, K: int, M: int, p: int) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.int64)
+    out = np.empty(len(a) * K, dtype=np.uint32)
+    lib().or_limb_split(len(a), a, K, M, p, out)
+    return out
+
+
+def scale_x(A: np.ndarray, K: int, theta: int, p: int) -> np.ndarray:
+    A = np.array(A, dtype=np.uint32, copy=True)
+    lib().or_scale_x(len(A), A, K, theta, p)
+    return A
+
+
+def crt_signed(residues, primes) -> int:
+    r = np.ascontiguousarray(residues, dtype=np.uint32)
+    p = np.ascontiguousarray(primes, dtype=np.uint32)
+    lo, hi = C.c_uint64(), C.c_uint64()
+    lib().or_crt_signed(len(r), r, p, C.byref(lo), C.byref(hi))
+    v = lo.value | (hi.value << 64)
+    return v - (1 << 128) if v >= 1 << 127 else v
+
+
+def ref_polymul(a: np.ndarray, b: np.ndarray, p: int) -> np.ndarray:
+    """The reference's own CPU product: modpn EX_Mont_FFTMul."""
+    L = ref()
+    if L.ref_init_prime(p) != 0:
+        raise RuntimeError("prime table full")
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    b = np.ascontiguousarray(b, dtype=np.int32)
+    h = np.empty(len(a) + len(b) - 1, dtype=np.int32)
+    if L.ref_fftmul(len(a) - 1, a, len(b) - 1, b, h, p) != 0:
+        raise RuntimeError("modpn product failed")
+    return h.view(np.uint32)
+
+
+def ref_polymul_batch(pairs, p: int, threads: int):
+    """Many independent modpn products over ``threads`` host threads.
+
+    ``pairs`` is a list of (a, b) uint32 arrays; returns the list of products.
+    """
+    L = ref()
+    L.ref_init_prime(p)
+    da = np.array([len(a) - 1 for a, _ in pairs], dtype=np.int32)
+    db = np.array([len(b) - 1 for _, b in pairs], dtype=np.int32)
+    a_off = np.zeros(len(pairs), dtype=np.int64)
+    b_off = np.zeros(len(pairs), dtype=np.int64)
+    h_off = np.zeros(len(pairs), dtype=np.int64)
+    a_off[1:] = np.cumsum(da + 1)[:-1]
+    b_off[1:] = np.cumsum(db + 1)[:-1]
+    h_off[1:] = np.cumsum(da + db + 1)[:-1]
+    A = np.concatenate([np.asarray(a, dtype=np.uint32) for a, _ in pairs]).view(np.int32)
+    B = np.concatenate([np.asarray(b, dtype=np.uint32) for _, b in pairs]).view(np.int32)
+    H = np.empty(int((da + db + 1).sum()), dtype=np.int32)
+    fails = L.ref_fftmul_batch(len(pairs), da, a_off, A, db, b_off, B, h_off, H, p, threads)
+    if fails:
+        raise RuntimeError(f"{fails} modpn products failed")
+    return [H[h_off[i]:h_off[i] + da[i] + db[i] + 1].view(np.uint32) for i in range(len(pairs))]

@@ -1,0 +1,49 @@
+"""The C-ABI library loads and exports every function include/*.h declares (CPU only)."""
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        src = re.sub(r"//[^\n]*", "", src)
+        for m in re.finditer(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\(", src):
+            name = m.group(1)
+            prefix = src[max(0, m.start() - 80):m.start()]
+            # a declaration: the name follows a type at the start of a statement
+            if re.search(r"(^|[;}\n])\s*(const\s+)?[A-Za-z_][A-Za-z0-9_ ]*[\s\*]+$", prefix) and \
+                    name not in ("if", "defined", "sizeof"):
+                names.add(name)
+    return sorted(names)
+
+
+def test_header_declares_reference_entry_points():
+    names = set(declared_functions())
+    for ref in ("is_cuda_enabled", "num_of_cuda_devices", "is_double_float_enabled",
+                "global_memory_in_bytes", "global_memory_in_megabytes", "can_call_fftmul_uni",
+                "cumodp_fft_uni", "cumodp_invfft_uni", "cumodp_fft_bivariate",
+                "cumodp_invfft_bivariate", "cumodp_fftmul_uni", "init_cuda_scube"):
+        assert ref in names
+
+
+def test_library_exports_every_declared_symbol():
+    from cumodp_b200 import LIB_PATH
+    lib = ctypes.CDLL(LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_queries_without_gpu_do_not_crash():
+    import cumodp_b200 as cm
+    # on a machine without a GPU these report "no device"; with one, a device
+    n = cm.num_of_cuda_devices()
+    assert n >= 0
+    assert cm.is_cuda_enabled() == (n > 0)

@@ -1,0 +1,104 @@
+"""Parity of the CUDA product path with the CPU oracle (bit-exact).
+
+Every case goes through the C ABI (libcumodp.so via ctypes).  The checker is
+the oracle's schoolbook product (small cases), its radix-2 transform product
+(large cases), and modpn's own FFT multiply when the compiled reference is
+present.
+"""
+import numpy as np
+import pytest
+
+from cumodp_b200.workloads import SplitMix64
+
+P0 = 469762049
+PRIMES = [469762049, 754974721, 962592769, 950009857, 940572673]
+
+pytestmark = pytest.mark.gpu
+
+
+def _rand(r, n, p):
+    return r.residues(n, p)
+
+
+@pytest.mark.parametrize("p", PRIMES)
+@pytest.mark.parametrize("da,db", [(0, 0), (1, 0), (5, 9), (31, 0), (16, 15), (100, 27), (255, 256),
+                                   (1000, 3), (2047, 2048), (4095, 4095), (3000, 5000), (8191, 8191)])
+def test_single_cta_products(cm, oracle_mod, p, da, db):
+    r = SplitMix64(hash((p, da, db)) & 0xFFFFFFFF)
+    a, b = _rand(r, da + 1, p), _rand(r, db + 1, p)
+    want = oracle_mod.polymul_school(a, b, p) if da * db < 4_000_000 else oracle_mod.polymul(a, b, p)
+    got = cm.fftmul_uni(a, b, p)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("p", [469762049, 962592769])
+@pytest.mark.parametrize("da,db", [(8192, 8191), (16383, 16383), (12345, 40000), (65535, 65535),
+                                   (100000, 1), (2**17 - 1, 2**17), (2**19 - 1, 2**19 - 1)])
+def test_three_pass_products(cm, oracle_mod, p, da, db):
+    r = SplitMix64(hash((p, da, db, 3)) & 0xFFFFFFFF)
+    a, b = _rand(r, da + 1, p), _rand(r, db + 1, p)
+    want = oracle_mod.polymul(a, b, p)
+    got = cm.fftmul_uni(a, b, p)
+    assert np.array_equal(got, want)
+
+
+def test_c1_config_vs_modpn(cm, oracle_mod):
+    """4095 x 4095 mod 469762049 (transform 8192) against modpn's own product."""
+    r = SplitMix64(0xC0DA0000)
+    a, b = _rand(r, 4096, P0), _rand(r, 4096, P0)
+    got = cm.fftmul_uni(a, b, P0)
+    assert np.array_equal(got, oracle_mod.polymul_school(a, b, P0))
+    if oracle_mod.ref_available():
+        assert np.array_equal(got, oracle_mod.ref_polymul(a, b, P0))
+
+
+def test_c2_product_2_24(cm, oracle_mod):
+    """Product of two degree 2^23-1 polynomials (transform 2^24) vs the oracle."""
+    r = SplitMix64(0xC0DA0001)
+    n = 1 << 23
+    a, b = _rand(r, n, P0), _rand(r, n, P0)
+    got = cm.fftmul_uni(a, b, P0)
+    want = oracle_mod.polymul(a, b, P0)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("da,db,dh", [(100, 50, 20), (100, 50, 150), (100, 50, 400), (4095, 4095, 9000),
+                                      (20000, 20000, 100), (20000, 20000, 70000)])
+def test_output_length_contract(cm, oracle_mod, da, db, dh):
+    """dh < da+db truncates; dh > da+db zero-fills exactly dh+1 words."""
+    r = SplitMix64(da * 7 + dh)
+    a, b = _rand(r, da + 1, P0), _rand(r, db + 1, P0)
+    full = oracle_mod.polymul(a, b, P0)
+    got = cm.fftmul_uni(a, b, P0, dh=dh)
+    want = np.zeros(dh + 1, dtype=np.uint32)
+    k = min(dh + 1, len(full))
+    want[:k] = full[:k]
+    assert np.array_equal(got, want)
+
+
+def test_small_fourier_primes(cm, oracle_mod):
+    for p, d in [(257, 100), (7681, 200), (12289, 1000), (40961, 4000)]:
+        r = SplitMix64(p)
+        a, b = _rand(r, d + 1, p), _rand(r, d + 1, p)
+        assert np.array_equal(cm.fftmul_uni(a, b, p), oracle_mod.polymul_school(a, b, p))
+
+
+def test_errors(cm):
+    with pytest.raises(cm.CumodpError) as e:
+        cm.fftmul_uni(np.ones(4, np.uint32), np.ones(4, np.uint32), 1000)  # not prime
+    assert e.value.code == cm.ASSUMPTION_ERROR
+    with pytest.raises(cm.CumodpError) as e:  # 257: 2-adic order 8 -> at most 256 points
+        cm.fftmul_uni(np.ones(200, np.uint32), np.ones(200, np.uint32), 257)
+    assert e.value.code == cm.FFT_SIZE_TOO_LARGE
+    # the library keeps working after an error
+    a = np.arange(10, dtype=np.uint32)
+    assert cm.fftmul_uni(a, a, P0)[0] == 0
+
+
+def test_inputs_above_p_are_reduced(cm, oracle_mod):
+    """Inputs are taken as unsigned 32-bit words and reduced mod p on load."""
+    r = SplitMix64(77)
+    a = r.next_u64(300).astype(np.uint32)
+    b = r.next_u64(200).astype(np.uint32)
+    want = oracle_mod.polymul_school(a % P0, b % P0, P0)
+    assert np.array_equal(cm.fftmul_uni(a, b, P0), want)
