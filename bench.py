@@ -1,0 +1,490 @@
+"""Benchmark of the FFT-based polynomial product on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the configuration the headline metric is quoted on, one GPU): the
+product of two dense degree-(2^23 - 1) polynomials mod p = 469762049
+(7 * 2^26 + 1), transform length n = 2^24, coefficients uniform in [0, p)
+from a fixed splitmix64 seed.  One step = one product.  Inputs are resident
+in HBM and rotate over 4 input sets (4 x 64 MiB > the 126 MB L2) so no step
+reads an operand the previous step left in L2.
+
+Printed JSON line (rank 0):
+  value        products/s over the K timed steps (device time, CUDA events,
+               max over ranks; N ranks run independent replicas)
+  e2e          the same metric through the host C entry point
+               cumodp_fftmul_uni with pinned host buffers: every step copies
+               both operands in and the product out
+  roofline     the dominant kernel: algorithmic bytes per launch / its mean
+               launch time (events around every launch), against the measured
+               HBM copy bandwidth
+  cpu_baseline modpn's own FFT multiply (the reference CPU path) on the host
+  extras       2^24-point forward+inverse transform GB/s; the batched
+               mixed-degree workload (4096 pairs) against one call per pair
+
+--impl reference runs the reference's CPU implementation of the same path
+(modpn EX_Mont_FFTMul, compiled from the reference sources into
+oracle/_ref) on all usable host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+P = 469762049
+LOGN = 24
+DEG = (1 << 23) - 1
+METRIC = "products/s & NTT HBM GB/s (% of peak), batched vs plain GPU, bit-exact"
+UNIT = "products/s"
+WORKLOAD = "poly_product_deg(2^23-1)x(2^23-1)_mod_469762049_n2^24"
+
+
+def peaks():
+    f = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(f):
+        d = json.load(open(f))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- clocks ----
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------ helpers ----
+def gen_operands(seed: int, sets: int):
+    from cumodp_b200.workloads import SplitMix64
+    r = SplitMix64(seed)
+    return [(r.residues(DEG + 1, P), r.residues(DEG + 1, P)) for _ in range(sets)]
+
+
+def powers_mod(x0: int, n: int) -> np.ndarray:
+    pw = np.ones(n, dtype=np.uint64)
+    m = 1
+    step = x0 % P
+    while m < n:
+        k = min(m, n - m)
+        pw[m:m + k] = (pw[:k] * np.uint64(step)) % np.uint64(P)
+        step = step * step % P
+        m *= 2
+    return pw
+
+
+def eval_mod(c: np.ndarray, pw: np.ndarray) -> int:
+    acc = 0
+    for i in range(0, len(c), 1 << 20):
+        acc += int(((c[i:i + (1 << 20)].astype(np.uint64) * pw[i:i + (1 << 20)]) % np.uint64(P)).sum())
+    return acc % P
+
+
+def product_check(a, b, h) -> bool:
+    """Size-independent check: H(x0) == A(x0) * B(x0) mod p at a fixed point."""
+    x0 = 123456789
+    pw = powers_mod(x0, len(h))
+    return eval_mod(h, pw) == eval_mod(a, pw[:len(a)]) * eval_mod(b, pw[:len(b)]) % P
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def modpn_sample(threads: int, products: int, seed: int):
+    """Time `products` modpn products of the workload's size on `threads` host threads."""
+    import oracle
+    from cumodp_b200.workloads import SplitMix64
+    r = SplitMix64(seed)
+    a, b = r.residues(DEG + 1, P), r.residues(DEG + 1, P)
+    pairs = [(a, b)] * products
+    t0 = time.perf_counter()
+    oracle.ref_polymul_batch(pairs, P, threads)
+    return time.perf_counter() - t0
+
+
+def ref_threads_bounded() -> int:
+    t = host_threads()
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+        t = min(t, max(1, int(avail * 0.5 // (3 * (1 << LOGN) * 4 + (3 << 24)))))
+    except ImportError:
+        pass
+    return max(1, min(t, 64))
+
+
+# ------------------------------------------------------- reference arm ----
+def run_reference(args, rank: int):
+    if rank != 0:
+        return
+    import oracle
+    if not oracle.ref_available():
+        try:
+            oracle.build(ref=True)
+        except Exception:
+            pass
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "modpn reference CPU build (oracle/_ref/libmodpn_ref.so) is not present"}))
+        return
+    threads = ref_threads_bounded()
+    per_step = threads  # one product per thread per step
+    for _ in range(args.warmup):
+        modpn_sample(threads, per_step, 0xC0DA0001)
+    times = [modpn_sample(threads, per_step, 0xC0DA0001) for _ in range(args.steps)]
+    total = sum(times)
+    value = args.steps * per_step / total
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded splitmix64)",
+            "impl": "reference",
+            "config": {"workload": WORKLOAD, "per_step": f"{per_step} independent products, one per host thread"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": f"{args.steps} steps x {per_step} products of degree 2^23-1 mod 469762049"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------- ours ----
+def run_ours(args, rank: int, world: int, local_rank: int):
+    import torch
+    import cumodp_b200 as cm
+
+    torch.cuda.set_device(local_rank)
+    cm.select_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = world > 1
+    if dist:
+        import torch.distributed as td
+
+    hbm_peak, peak_kind = peaks()
+    n = 1 << LOGN
+    sets = 4
+    ops = gen_operands(0xC0DA0001 + rank, sets)
+    dA = [torch.from_numpy(a.view(np.int32)).to(dev) for a, _ in ops]
+    dB = [torch.from_numpy(b.view(np.int32)).to(dev) for _, b in ops]
+    dH = torch.empty(n - 1, dtype=torch.int32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    sp = stream.cuda_stream
+
+    def step(i):
+        s = i % sets
+        cm.fftmul_uni_dev(dH.data_ptr(), n - 1, dA[s].data_ptr(), DEG, dB[s].data_ptr(), DEG, P, sp)
+
+    # correctness of the measured path (untimed): evaluation-point identity
+    step(0)
+    torch.cuda.synchronize()
+    ok = product_check(ops[0][0], ops[0][1], dH.cpu().numpy().view(np.uint32))
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    if dist:
+        td.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        # keep the GPU under this workload until the sampler reports (untimed),
+        # so the clock record covers load right up to and through the timed region
+        t_load = time.perf_counter()
+        i = 0
+        while (len(clk.lines) < 5 and time.perf_counter() - t_load < 4.0) or i < 4:
+            step(i)
+            i += 1
+            if i % 16 == 0:
+                torch.cuda.synchronize()
+        torch.cuda.synchronize()
+        cm.trace_passes(True)
+        cm.trace_report(reset=True)
+        e0.record(stream)
+        for i in range(args.steps):
+            step(i)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    cm.trace_passes(False)
+    passes = cm.trace_report(reset=True)
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        td.all_reduce(t, op=td.ReduceOp.MAX)
+        ms = float(t.item())
+        td.barrier()
+    value = world * args.steps / (ms / 1000.0)
+
+    # dominant kernel and its roofline
+    dom = max(passes.items(), key=lambda kv: kv[1][1])
+    dom_name, (dom_cnt, dom_ms) = dom
+    # algorithmic bytes per launch: one transform pass over n words moves 8n
+    # bytes (read + write); col_fwd runs the first pass of both operands
+    # (16n), row_fused the second passes of both forward transforms and the
+    # first of the inverse (24n), col_inv the last pass of the inverse (8n)
+    units = {"col_fwd": 2, "row_fused": 3, "col_inv": 1}
+    unit_key = dom_name.rsplit("_", 1)[0]
+    alg_bytes = units.get(unit_key, 1) * 8 * n
+    mean_s = dom_ms / dom_cnt / 1000.0
+    achieved = alg_bytes / mean_s / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        traffic = json.load(open(tf)).get(dom_name)
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+                "frac": round(achieved / hbm_peak, 4), "traffic": traffic, "kernel": dom_name,
+                "peak_kind": peak_kind, "alg_bytes_per_launch": alg_bytes,
+                "mean_launch_ms": round(mean_s * 1000, 5),
+                "passes_ms_per_step": {k: round(v[1] / v[0], 5) for k, v in passes.items()}}
+
+    # whole-product roofline (SURVEY/BASELINE definition: 24 n ceil(log2 n / 14) bytes)
+    prod_alg = 24 * n * 2
+    product_gbs = prod_alg / (ms / args.steps / 1000.0) / 1e9 / world
+
+    # e2e through the host C entry point, pinned host buffers
+    L = cm.lib()
+    hA = torch.from_numpy(ops[0][0].view(np.int32)).pin_memory()
+    hB = torch.from_numpy(ops[0][1].view(np.int32)).pin_memory()
+    hH = torch.empty(n - 1, dtype=torch.int32).pin_memory()
+    cm_fn = L.cumodp_fftmul_uni
+    cm_fn.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32,
+                      ctypes.c_void_p, ctypes.c_int32]
+    e2e_steps = max(3, min(args.steps, 20))
+    for _ in range(2):
+        cm_fn(n - 2, hH.data_ptr(), DEG, hA.data_ptr(), DEG, hB.data_ptr(), P)
+    if dist:
+        td.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        rc = cm_fn(n - 2, hH.data_ptr(), DEG, hA.data_ptr(), DEG, hB.data_ptr(), P)
+        assert rc == 0, rc
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device=dev)
+        td.all_reduce(t, op=td.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_ok = product_check(ops[0][0], ops[0][1], hH.numpy().view(np.uint32))
+    e2e = {"value": world * e2e_steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 2 * (DEG + 1) * 4,
+           "d2h_bytes_per_step": (n - 1) * 4, "steps": e2e_steps, "eval_point_identity": e2e_ok}
+
+    extras = {}
+    if rank == 0 and not args.no_extras:
+        extras["ntt_2_24"] = ntt_2_24(cm, torch, dev, stream, hbm_peak)
+        extras["batched_c4"] = batched_c4(cm, torch, dev, stream)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_extras:
+        cpu = cpu_baseline()
+
+    if rank == 0:
+        launches = args.steps * 3
+        line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 5), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+                "data": "synthetic (seeded splitmix64, uniform residues)",
+                "config": {"workload": WORKLOAD, "prime": P, "transform_log2": LOGN,
+                           "l2_policy": "inputs rotate over 4 sets of 64 MiB (> 126 MB L2)",
+                           "parallelism": f"replicas x{world}"},
+                "check": {"eval_point_identity": ok},
+                "product_alg_gbs": round(product_gbs, 1),
+                "roofline": roofline, "e2e": e2e, "gpu_launches": launches,
+                "clocks": dict(clk.summary(), window="sampled from 1 s of untimed load through the timed region"),
+                "cpu_baseline": cpu}
+        line.update(extras)
+        print(json.dumps(line))
+
+
+def ntt_2_24(cm, torch, dev, stream, hbm_peak):
+    """Forward + inverse natural-order 2^24 transform (device pointers): GB/s on 8n*ceil(24/14) per transform."""
+    from cumodp_b200.workloads import SplitMix64
+    n = 1 << LOGN
+    x = SplitMix64(0xC0DA0001).residues(n, P)
+    w = pow(3, (P - 1) >> LOGN, P)  # 3 generates the multiplicative group of 469762049
+    dx = torch.from_numpy(x.view(np.int32)).to(dev)
+    sp = stream.cuda_stream
+    for _ in range(2):
+        cm.fft_uni_dev(dx.data_ptr(), LOGN, w, P, False, sp)
+        cm.fft_uni_dev(dx.data_ptr(), LOGN, w, P, True, sp)
+    torch.cuda.synchronize()
+    reps = 10
+    cm.trace_passes(True)
+    cm.trace_report(reset=True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        cm.fft_uni_dev(dx.data_ptr(), LOGN, w, P, False, sp)
+        cm.fft_uni_dev(dx.data_ptr(), LOGN, w, P, True, sp)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    cm.trace_passes(False)
+    passes = cm.trace_report(reset=True)
+    ms = e0.elapsed_time(e1) / (2 * reps)
+    round_trip_ok = bool(np.array_equal(dx.cpu().numpy().view(np.uint32), x))
+    bio = 8 * n * 2
+    per_pass = {k: {"ms": round(v[1] / v[0], 5), "gbs": round(8 * n / (v[1] / v[0] / 1000) / 1e9, 1),
+                    "frac": round(8 * n / (v[1] / v[0] / 1000) / 1e9 / hbm_peak, 4)} for k, v in passes.items()}
+    return {"ms_per_transform": round(ms, 5), "gbs_bio": round(bio / (ms / 1000) / 1e9, 1),
+            "frac_bio": round(bio / (ms / 1000) / 1e9 / hbm_peak, 4),
+            "gbs_strict_8n": round(8 * n / (ms / 1000) / 1e9, 1), "per_pass": per_pass,
+            "round_trip_bit_exact": round_trip_ok}
+
+
+def batched_c4(cm, torch, dev, stream):
+    """4096 pairs, degrees log-uniform in [32, 65536]: one batched call vs one call per pair."""
+    from cumodp_b200.workloads import SplitMix64, seed_for
+    r = SplitMix64(seed_for(3))
+    cnt = 4096
+    da = r.log_uniform_int(cnt, 32, 65536).astype(np.int32)
+    db = r.log_uniform_int(cnt, 32, 65536).astype(np.int32)
+    f_off = np.zeros(cnt, np.int64)
+    g_off = np.zeros(cnt, np.int64)
+    h_off = np.zeros(cnt, np.int64)
+    f_off[1:] = np.cumsum(da.astype(np.int64) + 1)[:-1]
+    g_off[1:] = np.cumsum(db.astype(np.int64) + 1)[:-1]
+    h_off[1:] = np.cumsum(da.astype(np.int64) + db + 1)[:-1]
+    nf, ng, nh = int((da + 1).sum()), int((db + 1).sum()), int((da.astype(np.int64) + db + 1).sum())
+    F = torch.from_numpy(r.residues(nf, P).view(np.int32)).to(dev)
+    G = torch.from_numpy(r.residues(ng, P).view(np.int32)).to(dev)
+    H = torch.zeros(nh, dtype=torch.int32, device=dev)
+    H1 = torch.zeros(nh, dtype=torch.int32, device=dev)
+    sp = stream.cuda_stream
+    for _ in range(2):
+        cm.fftmul_batch_dev(da, f_off, F.data_ptr(), db, g_off, G.data_ptr(), h_off, H.data_ptr(), P, sp)
+    torch.cuda.synchronize()
+    reps = 5
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        cm.fftmul_batch_dev(da, f_off, F.data_ptr(), db, g_off, G.data_ptr(), h_off, H.data_ptr(), P, sp)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_batch = e0.elapsed_time(e1) / reps
+    # one call per pair (the plain path), same stream, device pointers
+    fp, gp, hp = F.data_ptr(), G.data_ptr(), H1.data_ptr()
+    for i in range(cnt):  # warm
+        cm.fftmul_uni_dev(hp + 4 * int(h_off[i]), int(da[i] + db[i] + 1), fp + 4 * int(f_off[i]), int(da[i]),
+                          gp + 4 * int(g_off[i]), int(db[i]), P, sp)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for i in range(cnt):
+        cm.fftmul_uni_dev(hp + 4 * int(h_off[i]), int(da[i] + db[i] + 1), fp + 4 * int(f_off[i]), int(da[i]),
+                          gp + 4 * int(g_off[i]), int(db[i]), P, sp)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_single_wall = (time.perf_counter() - t0) * 1000
+    t_single = e0.elapsed_time(e1)
+    same = bool(torch.equal(H, H1))
+    return {"pairs": cnt, "ms_batched": round(t_batch, 4), "products_per_s_batched": round(cnt / (t_batch / 1000), 1),
+            "ms_one_call_per_pair": round(t_single, 4), "ms_one_call_per_pair_wall": round(t_single_wall, 4),
+            "speedup_vs_one_call": round(t_single / t_batch, 2), "batched_equals_single": same}
+
+
+def cpu_baseline():
+    import oracle
+    if not oracle.ref_available():
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": "unavailable"}
+    threads = min(ref_threads_bounded(), 8)
+    secs = modpn_sample(threads, threads, 0xC0DA0001)
+    return {"value": round(threads / secs, 4), "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"{threads} products of degree 2^23-1 mod 469762049, one per host thread "
+                      f"({secs:.1f} s wall)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="headline only (no e2e extras, transform, batch or CPU legs); for profiling")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as td
+        torch.cuda.set_device(local_rank)
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                              device_id=torch.device("cuda", local_rank))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as td
+            td.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -46,6 +46,18 @@ class CumodpError(RuntimeError):
 
 _LIB = None
 
+
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int), ("memory_budget", C.c_size_t), ("max_batch", C.c_int),
+                ("batch_window_us", C.c_int), ("lanes", C.c_int), ("inject_fault_batch", C.c_int)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("completed", C.c_longlong), ("failed", C.c_longlong), ("batches", C.c_longlong),
+                ("pending", C.c_longlong), ("inflight_bytes", C.c_size_t), ("p50_us", C.c_double),
+                ("p99_us", C.c_double), ("max_us", C.c_double), ("products_per_s", C.c_double)]
+
+
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 _i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
 
@@ -72,6 +84,57 @@ def _lib():
         L.cumodp_fftmul_uni_dev.restype = C.c_int
         L.cumodp_fftmul_uni_dev.argtypes = [C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32,
                                             C.c_void_p, C.c_int32, C.c_void_p]
+        for name in ("cumodp_fft_uni", "cumodp_invfft_uni"):
+            getattr(L, name).restype = C.c_int
+            getattr(L, name).argtypes = [_i32p, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
+        for name in ("cumodp_fft_bivariate", "cumodp_invfft_bivariate"):
+            getattr(L, name).restype = C.c_int
+            getattr(L, name).argtypes = [_i32p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
+        L.cumodp_fftmul_batch.restype = C.c_int
+        L.cumodp_fftmul_batch.argtypes = [C.c_int, _i32p, _i64p, _i32p, _i32p, _i64p, _i32p, _i64p,
+                                          _i32p, C.c_int32]
+        L.cumodp_fftmul_batch_dev.restype = C.c_int
+        L.cumodp_fftmul_batch_dev.argtypes = [C.c_int, _i32p, _i64p, C.c_void_p, _i32p, _i64p, C.c_void_p,
+                                              _i64p, C.c_void_p, C.c_int32, C.c_void_p]
+        L.cumodp_fft_uni_dev.restype = C.c_int
+        L.cumodp_fft_uni_dev.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int,
+                                         C.c_void_p]
+        L.cumodp_select_device.restype = C.c_int
+        L.cumodp_select_device.argtypes = [C.c_int]
+        L.cumodp_trace_passes.restype = None
+        L.cumodp_trace_passes.argtypes = [C.c_int]
+        L.cumodp_trace_report.restype = C.c_size_t
+        L.cumodp_trace_report.argtypes = [C.c_char_p, C.c_size_t, C.c_int]
+        L.cumodp_twoconv_mul_i64.restype = C.c_int
+        L.cumodp_twoconv_mul_i64.argtypes = [C.c_longlong, _i64p, C.c_longlong, _i64p, _i64p, C.c_int]
+        L.cumodp_twoconv_mul_i64_dev.restype = C.c_int
+        L.cumodp_twoconv_mul_i64_dev.argtypes = [C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p,
+                                                 C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+        L.cumodp_twoconv_bit_width.restype = C.c_int
+        L.cumodp_twoconv_bit_width.argtypes = [C.c_longlong, _i64p, C.c_longlong, _i64p]
+        L.cumodp_twoconv_plan.restype = C.c_int
+        L.cumodp_twoconv_plan.argtypes = [C.c_int, C.c_int, C.c_longlong, C.c_longlong, C.c_int,
+                                          C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.cumodp_server_default_config.restype = None
+        L.cumodp_server_default_config.argtypes = [C.POINTER(ServerConfig)]
+        L.cumodp_server_create.restype = C.c_void_p
+        L.cumodp_server_create.argtypes = [C.POINTER(ServerConfig)]
+        L.cumodp_server_submit_mod.restype = C.c_longlong
+        L.cumodp_server_submit_mod.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p,
+                                               C.c_void_p]
+        L.cumodp_server_submit_i64.restype = C.c_longlong
+        L.cumodp_server_submit_i64.argtypes = [C.c_void_p, C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p,
+                                               C.c_void_p]
+        L.cumodp_server_poll.restype = C.c_int
+        L.cumodp_server_poll.argtypes = [C.c_void_p, C.c_longlong]
+        L.cumodp_server_wait.restype = C.c_int
+        L.cumodp_server_wait.argtypes = [C.c_void_p, C.c_longlong, C.c_longlong]
+        L.cumodp_server_get_stats.restype = None
+        L.cumodp_server_get_stats.argtypes = [C.c_void_p, C.POINTER(ServerStats)]
+        L.cumodp_server_reset_stats.restype = None
+        L.cumodp_server_reset_stats.argtypes = [C.c_void_p]
+        L.cumodp_server_destroy.restype = None
+        L.cumodp_server_destroy.argtypes = [C.c_void_p]
         L.cumodp_device_bytes_in_use.restype = C.c_size_t
         L.cumodp_device_bytes_in_use.argtypes = []
         _LIB = L
@@ -130,6 +193,208 @@ def fftmul_uni_dev(h_ptr: int, lh: int, f_ptr: int, df: int, g_ptr: int, dg: int
     """Device-pointer product: lh words of H = F * G mod p (``cumodp_fftmul_uni_dev``)."""
     _check(_lib().cumodp_fftmul_uni_dev(lh, h_ptr, df, f_ptr, dg, g_ptr, p, stream or None),
            "cumodp_fftmul_uni_dev")
+
+
+# ----------------------------------------------------------- transforms ----
+
+def fft_uni(X, w: int, p: int) -> np.ndarray:
+    """Natural-order DFT with root w (``cumodp_fft_uni``); returns a new array."""
+    x = _as_i32(X).copy()
+    n = len(x)
+    k = n.bit_length() - 1
+    _check(_lib().cumodp_fft_uni(x, n, k, w, p), "cumodp_fft_uni")
+    return x.view(np.uint32)
+
+
+def invfft_uni(X, w: int, p: int) -> np.ndarray:
+    """Inverse of fft_uni: DFT with w^-1 scaled by n^-1 (``cumodp_invfft_uni``)."""
+    x = _as_i32(X).copy()
+    n = len(x)
+    k = n.bit_length() - 1
+    _check(_lib().cumodp_invfft_uni(x, n, k, w, p), "cumodp_invfft_uni")
+    return x.view(np.uint32)
+
+
+def fft_bivariate(X, em: int, wm: int, en: int, wn: int, p: int, inverse: bool = False) -> np.ndarray:
+    """2-D DFT of a row-major 2^em x 2^en array (``cumodp_fft_bivariate``)."""
+    x = _as_i32(X).reshape(-1).copy()
+    assert len(x) == 1 << (em + en)
+    f = _lib().cumodp_invfft_bivariate if inverse else _lib().cumodp_fft_bivariate
+    _check(f(x, em, wm, en, wn, p), "cumodp_fft_bivariate")
+    return x.view(np.uint32)
+
+
+# ------------------------------------------------------------- batches ----
+
+def _batch_layout(pairs):
+    df = np.array([len(a) - 1 for a, _ in pairs], dtype=np.int32)
+    dg = np.array([len(b) - 1 for _, b in pairs], dtype=np.int32)
+    f_off = np.zeros(len(pairs), dtype=np.int64)
+    g_off = np.zeros(len(pairs), dtype=np.int64)
+    h_off = np.zeros(len(pairs), dtype=np.int64)
+    if len(pairs):
+        f_off[1:] = np.cumsum(df.astype(np.int64) + 1)[:-1]
+        g_off[1:] = np.cumsum(dg.astype(np.int64) + 1)[:-1]
+        h_off[1:] = np.cumsum(df.astype(np.int64) + dg + 1)[:-1]
+    return df, dg, f_off, g_off, h_off
+
+
+def fftmul_batch(pairs, p: int):
+    """Products of many (F, G) pairs mod p in one batched call (``cumodp_fftmul_batch``)."""
+    df, dg, f_off, g_off, h_off = _batch_layout(pairs)
+    F = np.concatenate([_as_i32(a) for a, _ in pairs]) if pairs else np.zeros(1, np.int32)
+    G = np.concatenate([_as_i32(b) for _, b in pairs]) if pairs else np.zeros(1, np.int32)
+    H = np.empty(max(1, int((df.astype(np.int64) + dg + 1).sum())), dtype=np.int32)
+    _check(_lib().cumodp_fftmul_batch(len(pairs), df, f_off, F, dg, g_off, G, h_off, H, p),
+           "cumodp_fftmul_batch")
+    Hu = H.view(np.uint32)
+    return [Hu[h_off[i]:h_off[i] + df[i] + dg[i] + 1] for i in range(len(pairs))]
+
+
+def fftmul_batch_dev(df, f_off, f_ptr: int, dg, g_off, g_ptr: int, h_off, h_ptr: int, p: int,
+                     stream: int = 0) -> None:
+    """Device-resident batch (``cumodp_fftmul_batch_dev``); offsets/degrees are host arrays."""
+    df = np.ascontiguousarray(df, dtype=np.int32)
+    dg = np.ascontiguousarray(dg, dtype=np.int32)
+    f_off = np.ascontiguousarray(f_off, dtype=np.int64)
+    g_off = np.ascontiguousarray(g_off, dtype=np.int64)
+    h_off = np.ascontiguousarray(h_off, dtype=np.int64)
+    _check(_lib().cumodp_fftmul_batch_dev(len(df), df, f_off, f_ptr, dg, g_off, g_ptr, h_off, h_ptr, p,
+                                          stream or None), "cumodp_fftmul_batch_dev")
+
+
+def fft_uni_dev(x_ptr: int, k: int, w: int, p: int, inverse: bool = False, stream: int = 0) -> None:
+    """In-place natural-order transform of 2^k device words (``cumodp_fft_uni_dev``)."""
+    _check(_lib().cumodp_fft_uni_dev(x_ptr, 1 << k, k, w, p, int(inverse), stream or None),
+           "cumodp_fft_uni_dev")
+
+
+def select_device(dev: int) -> None:
+    _check(_lib().cumodp_select_device(dev), "cumodp_select_device")
+
+
+def trace_passes(enable: bool) -> None:
+    """Bracket every (non-captured) kernel launch with CUDA events."""
+    _lib().cumodp_trace_passes(int(enable))
+
+
+def trace_report(reset: bool = True) -> dict:
+    """{kernel: (launches, total_ms)} accumulated since the last reset."""
+    n = _lib().cumodp_trace_report(None, 0, 0)
+    buf = C.create_string_buffer(n + 1)
+    _lib().cumodp_trace_report(buf, n + 1, int(reset))
+    out = {}
+    for line in buf.value.decode().splitlines():
+        name, cnt, ms = line.split()
+        out[name] = (int(cnt), float(ms))
+    return out
+
+
+# ------------------------------------------------------ exact products ----
+
+def int128_words_to_ints(w: np.ndarray) -> list:
+    """(lo, hi) int64 word pairs -> Python ints."""
+    lo = w[0::2].astype(np.uint64).astype(object)
+    hi = w[1::2].astype(np.int64).astype(object)
+    return [int(h) * (1 << 64) + int(l) for l, h in zip(lo, hi)]
+
+
+def twoconv_mul(a, b, method: int = 0, raw: bool = False):
+    """Exact product of int64 polynomials (``cumodp_twoconv_mul_i64``).
+
+    Returns the na+nb-1 coefficients as Python ints (or the raw (lo, hi)
+    int64 words when ``raw``).  method 1 forces the two-prime limb split.
+    """
+    a = np.ascontiguousarray(a, dtype=np.int64)
+    b = np.ascontiguousarray(b, dtype=np.int64)
+    c = np.empty(2 * (len(a) + len(b) - 1), dtype=np.int64)
+    _check(_lib().cumodp_twoconv_mul_i64(len(a), a, len(b), b, c, method), "cumodp_twoconv_mul_i64")
+    return c if raw else int128_words_to_ints(c)
+
+
+def twoconv_bit_width(a, b) -> int:
+    a = np.ascontiguousarray(a, dtype=np.int64)
+    b = np.ascontiguousarray(b, dtype=np.int64)
+    return int(_lib().cumodp_twoconv_bit_width(len(a), a, len(b), b))
+
+
+def twoconv_plan(bit_width_a: int, bit_width_b: int, na: int, nb: int, method: int = 0):
+    """(K, M, number of primes) the exact product would use."""
+    K, M, npr = C.c_int(), C.c_int(), C.c_int()
+    _check(_lib().cumodp_twoconv_plan(bit_width_a, bit_width_b, na, nb, method, C.byref(K), C.byref(M),
+                                      C.byref(npr)), "cumodp_twoconv_plan")
+    return K.value, M.value, npr.value
+
+
+# ------------------------------------------------------------- serving ----
+
+class Server:
+    """Continuous-batching request loop (``cumodp_server_*``).
+
+    submit_mod / submit_i64 copy the inputs and return (request id, output
+    array); the output array is filled when wait(id) returns 0.
+    """
+
+    def __init__(self, device: int = 0, memory_budget: int = 0, max_batch: int = 512,
+                 batch_window_us: int = 50, lanes: int = 4, inject_fault_batch: int = 0):
+        cfg = ServerConfig()
+        _lib().cumodp_server_default_config(C.byref(cfg))
+        cfg.device, cfg.memory_budget, cfg.max_batch = device, memory_budget, max_batch
+        cfg.batch_window_us, cfg.lanes, cfg.inject_fault_batch = batch_window_us, lanes, inject_fault_batch
+        self._h = _lib().cumodp_server_create(C.byref(cfg))
+        if not self._h:
+            raise CumodpError(NO_CUDA_DEVICE, "cumodp_server_create")
+        self._outs = {}
+
+    def submit_mod(self, F, G, p: int):
+        f = _as_i32(F)
+        g = _as_i32(G)
+        out = np.empty(len(f) + len(g) - 1, dtype=np.int32)
+        rid = _lib().cumodp_server_submit_mod(self._h, p, len(f) - 1, f.ctypes.data, len(g) - 1, g.ctypes.data,
+                                              out.ctypes.data)
+        if rid < 0:
+            raise CumodpError(ASSUMPTION_ERROR, "cumodp_server_submit_mod")
+        self._outs[rid] = out
+        return rid, out.view(np.uint32)
+
+    def submit_i64(self, a, b):
+        a = np.ascontiguousarray(a, dtype=np.int64)
+        b = np.ascontiguousarray(b, dtype=np.int64)
+        out = np.empty(2 * (len(a) + len(b) - 1), dtype=np.int64)
+        rid = _lib().cumodp_server_submit_i64(self._h, len(a), a.ctypes.data, len(b), b.ctypes.data,
+                                              out.ctypes.data)
+        if rid < 0:
+            raise CumodpError(ASSUMPTION_ERROR, "cumodp_server_submit_i64")
+        self._outs[rid] = out
+        return rid, out
+
+    def poll(self, rid: int) -> int:
+        return int(_lib().cumodp_server_poll(self._h, rid))
+
+    def wait(self, rid: int, timeout_us: int = -1) -> int:
+        st = int(_lib().cumodp_server_wait(self._h, rid, timeout_us))
+        if st != -2:
+            self._outs.pop(rid, None)
+        return st
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        _lib().cumodp_server_get_stats(self._h, C.byref(s))
+        return {k: getattr(s, k) for k, _ in ServerStats._fields_}
+
+    def reset_stats(self) -> None:
+        _lib().cumodp_server_reset_stats(self._h)
+
+    def close(self) -> None:
+        if self._h:
+            _lib().cumodp_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 def device_bytes_in_use() -> int:

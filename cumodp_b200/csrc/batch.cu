@@ -390,6 +390,93 @@ int batch_mul_dev(int count, const sfixn* df, const int64_t* f_off, const u32* F
     return cuda_err(cudaGraphLaunch(P->exec, st));
 }
 
+// ------------------------------------------------------- direct batches ----
+// Products on caller-owned buffers with direct launches (no plan cache, no
+// graph): used where several batches run concurrently on different streams
+// (the serving loop, the exact-product path).  Buffers:
+//   ws     workspace words: direct_ws_words()
+//   djobs  device job-table bytes: direct_job_bytes(); hjobs a pinned host
+//          buffer of the same size that must stay untouched until the stream
+//          has passed this call's work.
+size_t direct_ws_words(int count, const long long* la, const long long* lb) {
+    size_t w = 0;
+    for (int i = 0; i < count; ++i) {
+        const int logn = product_logn(la[i], lb[i]);
+        if (logn > kMaxSmallLog) w += 2ull << logn;
+    }
+    return w;
+}
+
+size_t direct_job_bytes(int count) {
+    return (size_t)count * std::max(sizeof(LargeJob), sizeof(ProdJob)) + 64 * 256;
+}
+
+int direct_batch(int count, const u32* const* a, const long long* la, const u32* const* b, const long long* lb,
+                 u32* const* h, const long long* lh, u32 p, u32* ws, void* djobs, void* hjobs,
+                 cudaStream_t st) {
+    int err = OK;
+    const PrimeCtx* pc = prime_ctx(p, &err);
+    if (!pc) return err;
+    const int dev = current_device();
+    ensure_kernel_attrs();
+    std::map<int, std::vector<int>> cls;
+    for (int i = 0; i < count; ++i) {
+        const int logn = product_logn(la[i], lb[i]);
+        if (logn > pc->info.two_adic || logn > kMaxLog) return FFT_SIZE_TOO_LARGE;
+        cls[logn].push_back(i);
+    }
+    size_t off = 0, wsoff = 0;
+    unsigned char* hj = (unsigned char*)hjobs;
+    struct Launch { int logn; size_t off; int n; int l2; };
+    std::vector<Launch> launches;
+    for (auto& kv : cls) {
+        const int logn = kv.first;
+        const std::vector<int>& mem = kv.second;
+        const bool large = logn > kMaxSmallLog;
+        for (size_t k = 0; k < mem.size(); ++k) {
+            const int i = mem[k];
+            const long long outl = std::min<long long>(lh[i], 1ll << logn);
+            if (!large) {
+                ProdJob j{a[i], b[i], h[i], (int)la[i], (int)lb[i], (int)outl, 0};
+                memcpy(hj + off + k * sizeof(ProdJob), &j, sizeof(j));
+            } else {
+                const size_t n = (size_t)1 << logn;
+                u32* w = ws + wsoff;
+                wsoff += 2 * n;
+                LargeJob j{a[i], b[i], h[i], (int)la[i], (int)lb[i], (int)outl, 0, w, w + n};
+                memcpy(hj + off + k * sizeof(LargeJob), &j, sizeof(j));
+            }
+            if (lh[i] > (1ll << logn)) {
+                cudaError_t e = cudaMemsetAsync(h[i] + (1ll << logn), 0, (size_t)(lh[i] - (1ll << logn)) * 4, st);
+                if (e != cudaSuccess) return cuda_err(e);
+            }
+        }
+        launches.push_back(Launch{logn, off, (int)mem.size(),
+                                  large ? tune_row_log(*pc, logn, (int)mem.size(), dev, st) : 0});
+        off += mem.size() * (large ? sizeof(LargeJob) : sizeof(ProdJob));
+        off = (off + 255) & ~(size_t)255;
+    }
+    cudaError_t ce = cudaMemcpyAsync(djobs, hjobs, off ? off : 256, cudaMemcpyHostToDevice, st);
+    if (ce != cudaSuccess) return cuda_err(ce);
+    for (const Launch& L : launches) {
+        const u32 root = canonical_root(*pc, L.logn);
+        if (L.logn <= kMaxSmallLog) {
+            SmallArgs A;
+            if ((err = small_args(*pc, root, L.logn, dev, &A)) != OK) return err;
+            A.jobs = (const ProdJob*)((char*)djobs + L.off);
+            A.njobs = L.n;
+            launch_small(L.logn, A, L.n, st);
+        } else {
+            LargeArgs A;
+            if ((err = large_args(*pc, root, L.logn, L.l2, dev, &A)) != OK) return err;
+            A.jobs = (const LargeJob*)((char*)djobs + L.off);
+            A.njobs = L.n;
+            launch_large(A, L.n, st);
+        }
+    }
+    return cuda_err(cudaGetLastError());
+}
+
 // Kernel launches one batch issues (for reporting).
 int batch_launch_count(int count, const sfixn* df, const sfixn* dg) {
     std::map<int, int> cls;

@@ -1,6 +1,8 @@
 // C entry points (include/cumodp.h): device queries, the univariate product
 // and the out-of-scope stubs.  Reference interface: src/modpn.cu:47-408.
+#include <algorithm>
 #include <cstdio>
+#include <cstring>
 
 #include "../../include/cumodp.h"
 #include "product.cuh"
@@ -124,6 +126,27 @@ const sfixn* interp_subres_coeff2(sfixn*, void*, sfixn, sfixn) { return nullptr;
 const sfixn* interp_subres_coeff3(sfixn*, sfixn*, void*, sfixn, sfixn) { return nullptr; }
 
 size_t cumodp_device_bytes_in_use(void) { return bytes_in_use(); }
+
+void cumodp_trace_passes(int enable) { pass_timing_enable(enable != 0); }
+
+size_t cumodp_trace_report(char* buf, size_t len, int reset) {
+    const std::string r = pass_timing_report(reset != 0);
+    if (buf && len) {
+        const size_t n = std::min(len - 1, r.size());
+        memcpy(buf, r.data(), n);
+        buf[n] = 0;
+    }
+    return r.size();
+}
+
+cumodp_err cumodp_select_device(int dev) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || dev < 0 || dev >= n) {
+        cudaGetLastError();
+        return n ? CUMODP_ASSUMPTION_ERROR : CUMODP_NO_CUDA_DEVICE;
+    }
+    return cudaSetDevice(dev) == cudaSuccess ? CUMODP_SUCCESS : CUMODP_FAILURE;
+}
 
 const char* cumodp_error_string(cumodp_err e) {
     switch (e) {

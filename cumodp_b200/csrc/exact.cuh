@@ -1,0 +1,28 @@
+// Exact integer products (two-convolution path), shared declarations.
+#pragma once
+#include "product.cuh"
+
+namespace cmb {
+
+struct TwoConvPlan {
+    int K, M, nprimes;
+    int logn;  // y-transform length
+};
+
+// Caller-owned buffers for an exact product (the serving loop runs several
+// at once on different streams); sizes from twoconv_buffer_sizes.
+struct TwoConvBufs {
+    u32* eval;    // evaluations and products
+    u32* ws;      // product workspace
+    void* djobs;  // device job tables
+    void* hjobs;  // pinned host job tables (untouched until the stream passes)
+};
+
+void twoconv_buffer_sizes(long long la, long long lb, size_t* eval_words, size_t* ws_words, size_t* job_bytes);
+int twoconv_plan(int ba, int bb, long long la, long long lb, bool force_two_prime, TwoConvPlan* out);
+// c (lo, hi pairs, la+lb-1 coefficients) = a * b exactly, device pointers;
+// bufs == nullptr uses the library workspace and graph-launched batches.
+int twoconv_mul_dev(const long long* a, long long la, const long long* b, long long lb, long long* c, int ba,
+                    int bb, bool force_two_prime, cudaStream_t st, TwoConvPlan* used, const TwoConvBufs* bufs);
+
+}  // namespace cmb

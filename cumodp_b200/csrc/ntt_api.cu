@@ -267,7 +267,10 @@ int ntt_natural_dev(const u32* x_in, u32* x_out, int k, u32 w, u32 p, bool inver
         A.src = x_in;
         A.dst = x_out;
         A.scale = tw_of(sc, p);
+        cudaEvent_t e0;
+        const bool tr = pass_timing_begin(st, &e0);
         kRowNtt[k](A, 1, st);
+        if (tr) pass_timing_end(st, "ntt_row", e0);
         return cuda_err(cudaGetLastError());
     }
     const int l1 = std::max(5, k - kMaxRowLog), l2 = k - l1;
@@ -276,7 +279,10 @@ int ntt_natural_dev(const u32* x_in, u32* x_out, int k, u32 w, u32 p, bool inver
     if (!ws) return err;
     u32 *w1 = ws, *w2 = ws + n;
     const u32 root_c = powmod_exact(root, 1ull << l2, p), root_r = powmod_exact(root, 1ull << l1, p);
+    cudaEvent_t e0;
+    bool tr = pass_timing_begin(st, &e0);
     if ((err = column_pass(*pc, root_c, l1, l2, x_in, n, w1, dev, st)) != OK) return err;
+    if (tr) pass_timing_end(st, "ntt_col", e0);
     RowNttArgs A;
     memset(&A, 0, sizeof(A));
     const Tw* twr = row_tables(dev, p, root_r, l2, &err);
@@ -292,8 +298,12 @@ int ntt_natural_dev(const u32* x_in, u32* x_out, int k, u32 w, u32 p, bool inver
     A.src = w1;
     A.dst = w2;
     A.scale = tw_of(sc, p);
+    tr = pass_timing_begin(st, &e0);
     kRowNtt[l2](A, 1 << l1, st);
+    if (tr) pass_timing_end(st, "ntt_row", e0);
+    tr = pass_timing_begin(st, &e0);
     k_transpose<<<dim3((1 << l2) / 32, (1 << l1) / 32), dim3(32, 8), 0, st>>>(w2, x_out, 1 << l1, 1 << l2);
+    if (tr) pass_timing_end(st, "ntt_transpose", e0);
     return cuda_err(cudaGetLastError());
 }
 
@@ -394,6 +404,20 @@ cumodp_err host_bivariate(sfixn* X, sfixn em, sfixn wm, sfixn en, sfixn wn, sfix
 }  // namespace
 
 extern "C" {
+
+cumodp_err cumodp_fft_uni_dev(sfixn* X, sfixn n, sfixn k, sfixn w, sfixn p, int inverse, void* stream) {
+    int cnt = 0;
+    if (cudaGetDeviceCount(&cnt) != cudaSuccess || cnt == 0) {
+        cudaGetLastError();
+        return CUMODP_NO_CUDA_DEVICE;
+    }
+    if (!X || k < 0 || k > 30 || n != (sfixn)(1u << k) || p <= 0) return CUMODP_ASSUMPTION_ERROR;
+    std::lock_guard<std::mutex> g(lib_mutex());
+    cudaStream_t st = stream ? (cudaStream_t)stream : lib_stream(current_device());
+    int e = ntt_natural_dev((const u32*)X, (u32*)X, k, (u32)w, (u32)p, inverse != 0, st);
+    if (e == OK && !stream) e = cuda_err(cudaStreamSynchronize(st));
+    return (cumodp_err)e;
+}
 
 cumodp_err cumodp_fft_uni(sfixn* X, sfixn n, sfixn k, sfixn w, sfixn p) { return host_ntt(X, n, k, w, p, false); }
 

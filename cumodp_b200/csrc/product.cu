@@ -167,16 +167,37 @@ int large_args(const PrimeCtx& pc, u32 root_n, int logn, int l2, int dev, LargeA
     return OK;
 }
 
+// Pass-timing names: kernel and the log2 of its transform dimension.
+static const char* kSmallName[15] = {"", "", "", "", "", "small_product_5", "small_product_6",
+    "small_product_7", "small_product_8", "small_product_9", "small_product_10", "small_product_11",
+    "small_product_12", "small_product_13", "small_product_14"};
+static const char* kColFwdName[11] = {"", "col_fwd_1", "col_fwd_2", "col_fwd_3", "col_fwd_4", "col_fwd_5",
+    "col_fwd_6", "col_fwd_7", "col_fwd_8", "col_fwd_9", "col_fwd_10"};
+static const char* kColInvName[11] = {"", "col_inv_1", "col_inv_2", "col_inv_3", "col_inv_4", "col_inv_5",
+    "col_inv_6", "col_inv_7", "col_inv_8", "col_inv_9", "col_inv_10"};
+static const char* kRowName[15] = {"", "", "", "", "", "", "row_fused_6", "row_fused_7", "row_fused_8",
+    "row_fused_9", "row_fused_10", "row_fused_11", "row_fused_12", "row_fused_13", "row_fused_14"};
+
 void launch_small(int logn, const SmallArgs& a, int njobs, cudaStream_t st) {
     const int ppc = small_ppc(logn);
+    cudaEvent_t e0;
+    const bool tr = pass_timing_begin(st, &e0);
     kSmall[logn](a, (njobs + ppc - 1) / ppc, st);
+    if (tr) pass_timing_end(st, kSmallName[logn], e0);
 }
 
 void launch_large(const LargeArgs& a, int njobs, cudaStream_t st) {
     const int n1 = 1 << a.l1, n2 = 1 << a.l2;
+    cudaEvent_t e0;
+    bool tr = pass_timing_begin(st, &e0);
     kColFwd[a.l1](a, dim3(n2 / 32, 2, njobs), st);
+    if (tr) pass_timing_end(st, kColFwdName[a.l1], e0);
+    tr = pass_timing_begin(st, &e0);
     kRow[a.l2](a, dim3(n1, njobs, 1), st);
+    if (tr) pass_timing_end(st, kRowName[a.l2], e0);
+    tr = pass_timing_begin(st, &e0);
     kColInv[a.l1](a, dim3(n2 / 32, 1, njobs), st);
+    if (tr) pass_timing_end(st, kColInvName[a.l1], e0);
 }
 
 int mul_dev(const u32* a, long long la, const u32* b, long long lb, u32* h, long long lh, u32 p,

@@ -29,6 +29,13 @@ void launch_large(const LargeArgs& a, int njobs, cudaStream_t st);
 // before any launch is captured into a graph).
 void ensure_kernel_attrs();
 
+// Batched products on caller-owned buffers, direct launches (batch.cu).
+size_t direct_ws_words(int count, const long long* la, const long long* lb);
+size_t direct_job_bytes(int count);
+int direct_batch(int count, const u32* const* a, const long long* la, const u32* const* b, const long long* lb,
+                 u32* const* h, const long long* lh, u32 p, u32* ws, void* djobs, void* hjobs,
+                 cudaStream_t st);
+
 // h[0..lh) = a[0..la) * b[0..lb) mod p on device pointers, on stream st.
 int mul_dev(const u32* a, long long la, const u32* b, long long lb, u32* h, long long lh, u32 p,
             cudaStream_t st);

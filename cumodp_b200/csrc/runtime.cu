@@ -8,6 +8,7 @@
 // scratch buffers grow once and are reused.
 #include "runtime.cuh"
 
+#include <cstdio>
 #include <cstring>
 
 namespace cmb {
@@ -268,6 +269,86 @@ void account_bytes(long long delta) {
     Caches& C = caches();
     std::lock_guard<std::mutex> g(C.m);
     C.bytes += delta;
+}
+
+namespace {
+struct PassTiming {
+    std::mutex m;
+    bool on = false;
+    std::vector<cudaEvent_t> pool;
+    struct Pending { std::string name; cudaEvent_t e0, e1; };
+    std::vector<Pending> pending;
+    std::map<std::string, std::pair<long long, double>> totals;
+};
+PassTiming& pt() {
+    static PassTiming* t = new PassTiming();
+    return *t;
+}
+cudaEvent_t pt_get_locked(PassTiming& T) {
+    if (!T.pool.empty()) {
+        cudaEvent_t e = T.pool.back();
+        T.pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+void pt_drain_locked(PassTiming& T) {
+    for (auto& p : T.pending) {
+        cudaEventSynchronize(p.e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, p.e0, p.e1);
+        auto& t = T.totals[p.name];
+        t.first += 1;
+        t.second += ms;
+        T.pool.push_back(p.e0);
+        T.pool.push_back(p.e1);
+    }
+    T.pending.clear();
+}
+}  // namespace
+
+bool pass_timing_on() { return pt().on; }
+
+void pass_timing_enable(bool on) {
+    PassTiming& T = pt();
+    std::lock_guard<std::mutex> g(T.m);
+    T.on = on;
+}
+
+bool pass_timing_begin(cudaStream_t st, cudaEvent_t* e0) {
+    PassTiming& T = pt();
+    if (!T.on) return false;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return false;
+    std::lock_guard<std::mutex> g(T.m);
+    if (T.pending.size() > 100000) pt_drain_locked(T);
+    *e0 = pt_get_locked(T);
+    cudaEventRecord(*e0, st);
+    return true;
+}
+
+void pass_timing_end(cudaStream_t st, const char* name, cudaEvent_t e0) {
+    PassTiming& T = pt();
+    std::lock_guard<std::mutex> g(T.m);
+    cudaEvent_t e1 = pt_get_locked(T);
+    cudaEventRecord(e1, st);
+    T.pending.push_back(PassTiming::Pending{name, e0, e1});
+}
+
+std::string pass_timing_report(bool reset) {
+    PassTiming& T = pt();
+    std::lock_guard<std::mutex> g(T.m);
+    pt_drain_locked(T);
+    std::string out;
+    char line[256];
+    for (auto& kv : T.totals) {
+        snprintf(line, sizeof(line), "%s %lld %.6f\n", kv.first.c_str(), kv.second.first, kv.second.second);
+        out += line;
+    }
+    if (reset) T.totals.clear();
+    return out;
 }
 
 int cuda_err(cudaError_t e) {

@@ -77,6 +77,18 @@ size_t bytes_in_use();
 // Records an allocation made outside the caches (plans, server pools).
 void account_bytes(long long delta);
 
+// Per-pass tracing: when enabled, launches that are not being captured into
+// a graph are bracketed by CUDA events on their stream; the totals per
+// kernel name are aggregated on demand (events are read after a sync).
+bool pass_timing_on();
+void pass_timing_enable(bool on);
+// Returns an event pair from the pool, or false when tracing is off or the
+// stream is capturing.
+bool pass_timing_begin(cudaStream_t st, cudaEvent_t* e0);
+void pass_timing_end(cudaStream_t st, const char* name, cudaEvent_t e0);
+// "name launches total_ms" lines for every kernel seen since the last reset.
+std::string pass_timing_report(bool reset);
+
 // Copies the last CUDA error (if any) into a library code.
 int cuda_err(cudaError_t e);
 

@@ -1,0 +1,565 @@
+// Serving loop: continuous batching of multiplication requests.
+//
+// The reference has no server; its entry points are synchronous, one
+// product per call, device 0, with per-call allocation
+// (src/stockham.cu:562-611).  This server keeps a request queue and a few
+// device "lanes" (stream + grow-only device/pinned buffers).  A batcher
+// thread admits requests in arrival order while the device-memory budget
+// allows, groups the admitted ones by (kind, prime) and dispatches each
+// group to a free lane as one batch: one host->device copy of all operands,
+// the batched product kernels (or the exact-product pipeline), one
+// device->host copy, an event.  Requests that arrive while earlier batches
+// are on the GPU are admitted into the next batch at once, so batches from
+// different lanes overlap on the device.  A completion thread waits on lane
+// events, scatters results into the callers' buffers, releases the memory
+// budget and records arrival-to-result latency.
+//
+// Failures are contained per batch: a request that fails validation is
+// completed with its error code; a CUDA error in a batch completes that
+// batch's requests with CUMODP_FFT_ERROR and the lane is re-created.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <thread>
+#include <unordered_map>
+
+#include "../../include/cumodp.h"
+#include "exact.cuh"
+
+namespace cmb {
+
+namespace {
+
+double now_us() {
+    return std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct Req {
+    long long id;
+    int kind;  // 0: modular product, 1: exact int64 product
+    u32 p;
+    long long la, lb;
+    std::vector<u32> A, B;          // kind 0
+    std::vector<long long> A64, B64;  // kind 1
+    int bw = 1;
+    void* out;
+    size_t bytes;
+    double t_submit = 0, t_done = 0;
+    int status = -1;
+    bool done = false;
+};
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    int ensure(size_t want) {
+        if (want <= n) return OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        if (cudaMalloc(&p, std::max<size_t>(want, 1024) * sizeof(T)) != cudaSuccess) {
+            cudaGetLastError();
+            return OUT_OF_MEMORY;
+        }
+        n = std::max<size_t>(want, 1024);
+        return OK;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+template <class T>
+struct PinBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    int ensure(size_t want) {
+        if (want <= n) return OK;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+        if (cudaHostAlloc((void**)&p, std::max<size_t>(want, 1024) * sizeof(T), cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            return OUT_OF_MEMORY;
+        }
+        n = std::max<size_t>(want, 1024);
+        return OK;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+struct Lane {
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev = nullptr;
+    DevBuf<u32> din, dout, ws;
+    DevBuf<unsigned char> djobs;
+    PinBuf<u32> hin, hout;
+    PinBuf<unsigned char> hjobs;
+    std::vector<Req*> reqs;
+    std::vector<size_t> out_off;  // word offset of each request's result in hout
+    int status = OK;
+    bool busy = false;
+    long long seq = 0;
+};
+
+}  // namespace
+
+struct Server {
+    cumodp_server_config cfg;
+    int dev;
+    std::mutex m;
+    std::condition_variable cv_work, cv_done, cv_free;
+    std::deque<Req*> pending;
+    std::unordered_map<long long, Req*> reqs;
+    std::vector<Lane> lanes;
+    std::deque<int> dispatched;  // lane indices in dispatch order
+    size_t inflight = 0;
+    long long next_id = 1, lane_seq = 0;
+    bool stop = false;
+    std::thread batcher, completer;
+    // statistics
+    std::vector<double> lat;
+    long long completed = 0, failed = 0, batches = 0;
+    double t_first = 0, t_last = 0;
+
+    explicit Server(const cumodp_server_config& c) : cfg(c), dev(c.device) {}
+};
+
+namespace {
+
+size_t req_bytes(const Req& r) {
+    const long long lc = r.la + r.lb - 1;
+    if (r.kind == 0) {
+        const int logn = product_logn(r.la, r.lb);
+        const size_t ws = logn > kMaxSmallLog ? (2ull << logn) : 0;
+        return (size_t)(r.la + r.lb + lc + ws) * 4 + 256;
+    }
+    size_t ev, ws, jb;
+    twoconv_buffer_sizes(r.la, r.lb, &ev, &ws, &jb);
+    return (r.la + r.lb + 2 * lc) * 8 + (ev + ws) * 4 + jb;
+}
+
+void finish(Server& S, Req* r, int status) {
+    r->status = status;
+    r->t_done = now_us();
+    r->done = true;
+    if (status == OK) {
+        S.completed++;
+        S.lat.push_back(r->t_done - r->t_submit);
+    } else {
+        S.failed++;
+    }
+    if (!S.t_first) S.t_first = r->t_submit;
+    S.t_last = r->t_done;
+}
+
+// Runs one batch on a lane (lane.reqs share kind and prime).  Called without
+// the server lock; only touches the lane and the requests it owns.
+int run_batch(Server& S, Lane& L) {
+    cudaSetDevice(S.dev);
+    if (S.cfg.inject_fault_batch > 0 && S.batches == S.cfg.inject_fault_batch)
+        return OUT_OF_MEMORY;  // host-side fault injection for tests: nothing is launched
+    const int kind = L.reqs[0]->kind;
+    const u32 p = L.reqs[0]->p;
+    const int cnt = (int)L.reqs.size();
+    int err = OK;
+    if (kind == 0) {
+        std::vector<long long> la(cnt), lb(cnt), lh(cnt);
+        size_t nin = 0, nout = 0;
+        for (int i = 0; i < cnt; ++i) {
+            la[i] = L.reqs[i]->la;
+            lb[i] = L.reqs[i]->lb;
+            lh[i] = la[i] + lb[i] - 1;
+            nin += la[i] + lb[i];
+            nout += lh[i];
+        }
+        if ((err = L.din.ensure(nin)) || (err = L.dout.ensure(nout)) || (err = L.hin.ensure(nin)) ||
+            (err = L.hout.ensure(nout)))
+            return err;
+        const size_t wsw = direct_ws_words(cnt, la.data(), lb.data());
+        const size_t jb = direct_job_bytes(cnt);
+        if ((err = L.ws.ensure(wsw + 1)) || (err = L.djobs.ensure(jb)) || (err = L.hjobs.ensure(jb))) return err;
+        std::vector<const u32*> pa(cnt), pb(cnt);
+        std::vector<u32*> ph(cnt);
+        L.out_off.assign(cnt, 0);
+        size_t o = 0, q = 0;
+        for (int i = 0; i < cnt; ++i) {
+            Req* r = L.reqs[i];
+            memcpy(L.hin.p + o, r->A.data(), r->la * 4);
+            pa[i] = L.din.p + o;
+            o += r->la;
+            memcpy(L.hin.p + o, r->B.data(), r->lb * 4);
+            pb[i] = L.din.p + o;
+            o += r->lb;
+            ph[i] = L.dout.p + q;
+            L.out_off[i] = q;
+            q += lh[i];
+        }
+        cudaError_t ce = cudaMemcpyAsync(L.din.p, L.hin.p, nin * 4, cudaMemcpyHostToDevice, L.st);
+        if (ce != cudaSuccess) return cuda_err(ce);
+        err = direct_batch(cnt, pa.data(), la.data(), pb.data(), lb.data(), ph.data(), lh.data(), p, L.ws.p,
+                           L.djobs.p, L.hjobs.p, L.st);
+        if (err != OK) return err;
+        ce = cudaMemcpyAsync(L.hout.p, L.dout.p, nout * 4, cudaMemcpyDeviceToHost, L.st);
+        if (ce != cudaSuccess) return cuda_err(ce);
+    } else {
+        // exact products, one after another on the lane's stream
+        size_t nin = 0, nout = 0, evw = 0, wsw = 0, jbb = 0;
+        for (Req* r : L.reqs) {
+            nin += r->la + r->lb;
+            nout += 2 * (r->la + r->lb - 1);
+            size_t e, w, j;
+            twoconv_buffer_sizes(r->la, r->lb, &e, &w, &j);
+            evw = std::max(evw, e);
+            wsw = std::max(wsw, w);
+            jbb += j;
+        }
+        // int64 data travels through the u32 buffers (two words per value)
+        if ((err = L.din.ensure(2 * nin)) || (err = L.dout.ensure(2 * nout + evw)) || (err = L.hin.ensure(2 * nin)) ||
+            (err = L.hout.ensure(2 * nout)) || (err = L.ws.ensure(wsw + 1)) || (err = L.djobs.ensure(jbb)) ||
+            (err = L.hjobs.ensure(jbb)))
+            return err;
+        L.out_off.assign(cnt, 0);
+        size_t o = 0, q = 0, jo = 0;
+        u32* eval = L.dout.p + 2 * nout;
+        long long* hin64 = (long long*)L.hin.p;
+        long long* din64 = (long long*)L.din.p;
+        long long* dout64 = (long long*)L.dout.p;
+        for (int i = 0; i < cnt; ++i) {
+            Req* r = L.reqs[i];
+            memcpy(hin64 + o, r->A64.data(), r->la * 8);
+            memcpy(hin64 + o + r->la, r->B64.data(), r->lb * 8);
+            cudaError_t ce = cudaMemcpyAsync(din64 + o, hin64 + o, (r->la + r->lb) * 8, cudaMemcpyHostToDevice, L.st);
+            if (ce != cudaSuccess) return cuda_err(ce);
+            TwoConvBufs B{eval, L.ws.p, L.djobs.p + jo, L.hjobs.p + jo};
+            size_t e, w, j;
+            twoconv_buffer_sizes(r->la, r->lb, &e, &w, &j);
+            err = twoconv_mul_dev(din64 + o, r->la, din64 + o + r->la, r->lb, dout64 + 2 * q, r->bw, r->bw, false,
+                                  L.st, nullptr, &B);
+            if (err != OK) return err;
+            L.out_off[i] = 4 * q;  // (lo, hi) int64 pairs, in u32 words
+            o += r->la + r->lb;
+            q += r->la + r->lb - 1;
+            jo += j;
+        }
+        cudaError_t ce = cudaMemcpyAsync(L.hout.p, L.dout.p, nout * 8, cudaMemcpyDeviceToHost, L.st);
+        if (ce != cudaSuccess) return cuda_err(ce);
+    }
+    return cuda_err(cudaEventRecord(L.ev, L.st));
+}
+
+void recreate_lane(Lane& L) {
+    if (L.st) cudaStreamDestroy(L.st);
+    if (L.ev) cudaEventDestroy(L.ev);
+    cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking);
+    cudaEventCreateWithFlags(&L.ev, cudaEventDisableTiming);
+}
+
+void batcher_loop(Server* Sp) {
+    Server& S = *Sp;
+    cudaSetDevice(S.dev);
+    std::unique_lock<std::mutex> lk(S.m);
+    for (;;) {
+        S.cv_work.wait(lk, [&] { return S.stop || !S.pending.empty(); });
+        if (S.stop) return;
+        // batching window: let a few more requests arrive (continuous
+        // batching: lanes already running are not waited for)
+        if ((int)S.pending.size() < S.cfg.max_batch && S.cfg.batch_window_us > 0) {
+            S.cv_work.wait_for(lk, std::chrono::microseconds(S.cfg.batch_window_us),
+                               [&] { return S.stop || (int)S.pending.size() >= S.cfg.max_batch; });
+            if (S.stop) return;
+        }
+        int li = -1;
+        S.cv_free.wait(lk, [&] {
+            if (S.stop) return true;
+            for (size_t i = 0; i < S.lanes.size(); ++i)
+                if (!S.lanes[i].busy) { li = (int)i; return true; }
+            return false;
+        });
+        if (S.stop) return;
+        // admit in arrival order, same (kind, prime) as the head, within the budget
+        Lane& L = S.lanes[li];
+        L.reqs.clear();
+        Req* head = S.pending.front();
+        const int kind = head->kind;
+        const u32 p = head->p;
+        size_t add = 0;
+        for (auto it = S.pending.begin(); it != S.pending.end() && (int)L.reqs.size() < S.cfg.max_batch;) {
+            Req* r = *it;
+            if (r->kind == kind && r->p == p) {
+                if (S.inflight + add + r->bytes > S.cfg.memory_budget && !(L.reqs.empty() && S.inflight == 0)) break;
+                L.reqs.push_back(r);
+                add += r->bytes;
+                it = S.pending.erase(it);
+            } else {
+                ++it;
+            }
+        }
+        if (L.reqs.empty()) {  // head does not fit yet: wait for a completion
+            S.cv_done.wait(lk);
+            continue;
+        }
+        S.inflight += add;
+        L.busy = true;
+        L.seq = ++S.lane_seq;
+        S.batches++;
+        lk.unlock();
+        L.status = run_batch(S, L);
+        if (L.status != OK) cudaEventRecord(L.ev, L.st);  // completer still waits on the lane
+        lk.lock();
+        S.dispatched.push_back(li);
+        S.cv_done.notify_all();
+    }
+}
+
+void completer_loop(Server* Sp) {
+    Server& S = *Sp;
+    cudaSetDevice(S.dev);
+    std::unique_lock<std::mutex> lk(S.m);
+    for (;;) {
+        S.cv_done.wait(lk, [&] { return S.stop || !S.dispatched.empty(); });
+        if (S.dispatched.empty() && S.stop) return;
+        if (S.dispatched.empty()) continue;
+        const int li = S.dispatched.front();
+        S.dispatched.pop_front();
+        Lane& L = S.lanes[li];
+        lk.unlock();
+        cudaError_t ce = cudaEventSynchronize(L.ev);
+        int st = L.status != OK ? L.status : cuda_err(ce);
+        if (st == OK) st = cuda_err(cudaGetLastError());
+        if (st == OK) {
+            for (size_t i = 0; i < L.reqs.size(); ++i) {
+                Req* r = L.reqs[i];
+                const size_t words = r->kind == 0 ? (size_t)(r->la + r->lb - 1) : (size_t)2 * 2 * (r->la + r->lb - 1);
+                memcpy(r->out, L.hout.p + L.out_off[i], words * 4);
+            }
+        } else {
+            // contain the failure: drain and re-create the lane
+            cudaStreamSynchronize(L.st);
+            cudaGetLastError();
+            recreate_lane(L);
+        }
+        lk.lock();
+        size_t freed = 0;
+        for (Req* r : L.reqs) {
+            freed += r->bytes;
+            finish(S, r, st == FFT_SIZE_TOO_LARGE || st == OK || st == ASSUMPTION_ERROR ||
+                                 st == OUT_OF_MEMORY ? st : FFT_ERROR);
+            r->A.clear(); r->A.shrink_to_fit();
+            r->B.clear(); r->B.shrink_to_fit();
+            r->A64.clear(); r->A64.shrink_to_fit();
+            r->B64.clear(); r->B64.shrink_to_fit();
+        }
+        S.inflight -= std::min(S.inflight, freed);
+        L.reqs.clear();
+        L.busy = false;
+        S.cv_free.notify_all();
+        S.cv_done.notify_all();
+        S.cv_work.notify_all();
+    }
+}
+
+long long submit(Server& S, Req* r) {
+    std::lock_guard<std::mutex> g(S.m);
+    if (S.stop) {
+        delete r;
+        return -1;
+    }
+    r->id = S.next_id++;
+    r->t_submit = now_us();
+    r->bytes = req_bytes(*r);
+    S.reqs[r->id] = r;
+    if (r->status != -1) {  // rejected at submission
+        finish(S, r, r->status);
+        S.cv_done.notify_all();
+        return r->id;
+    }
+    S.pending.push_back(r);
+    S.cv_work.notify_one();
+    return r->id;
+}
+
+}  // namespace
+
+}  // namespace cmb
+
+using namespace cmb;
+
+extern "C" {
+
+void cumodp_server_default_config(cumodp_server_config* c) {
+    if (!c) return;
+    c->device = 0;
+    c->memory_budget = 0;
+    c->max_batch = 512;
+    c->batch_window_us = 50;
+    c->lanes = 4;
+    c->inject_fault_batch = 0;
+}
+
+cumodp_server* cumodp_server_create(const cumodp_server_config* cfg) {
+    cumodp_server_config c;
+    cumodp_server_default_config(&c);
+    if (cfg) c = *cfg;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || c.device < 0 || c.device >= n) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    cudaSetDevice(c.device);
+    if (c.memory_budget == 0) {
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        c.memory_budget = fr / 4;
+    }
+    if (c.max_batch <= 0) c.max_batch = 512;
+    if (c.lanes <= 0) c.lanes = 4;
+    Server* S = new Server(c);
+    S->lanes.resize(c.lanes);
+    for (Lane& L : S->lanes) recreate_lane(L);
+    S->batcher = std::thread(batcher_loop, S);
+    S->completer = std::thread(completer_loop, S);
+    return (cumodp_server*)S;
+}
+
+long long cumodp_server_submit_mod(cumodp_server* h, sfixn p, sfixn df, const sfixn* F, sfixn dg, const sfixn* G,
+                                   sfixn* H) {
+    Server* S = (Server*)h;
+    if (!S || !F || !G || !H || df < 0 || dg < 0) return -1;
+    Req* r = new Req();
+    r->kind = 0;
+    r->p = (u32)p;
+    r->la = (long long)df + 1;
+    r->lb = (long long)dg + 1;
+    r->out = H;
+    int err = OK;
+    const PrimeCtx* pc = prime_ctx((u32)p, &err);
+    if (!pc) r->status = err;
+    else if (product_logn(r->la, r->lb) > std::min(pc->info.two_adic, kMaxLog)) r->status = FFT_SIZE_TOO_LARGE;
+    else {
+        r->A.assign((const u32*)F, (const u32*)F + r->la);
+        r->B.assign((const u32*)G, (const u32*)G + r->lb);
+    }
+    return submit(*S, r);
+}
+
+long long cumodp_server_submit_i64(cumodp_server* h, long long na, const int64_t* a, long long nb, const int64_t* b,
+                                   int64_t* c) {
+    Server* S = (Server*)h;
+    if (!S || !a || !b || !c || na <= 0 || nb <= 0) return -1;
+    Req* r = new Req();
+    r->kind = 1;
+    r->p = 0;
+    r->la = na;
+    r->lb = nb;
+    r->out = c;
+    unsigned long long m = 0;
+    for (long long i = 0; i < na; ++i) m |= a[i] < 0 ? 0ull - (unsigned long long)a[i] : (unsigned long long)a[i];
+    for (long long i = 0; i < nb; ++i) m |= b[i] < 0 ? 0ull - (unsigned long long)b[i] : (unsigned long long)b[i];
+    r->bw = m ? 64 - __builtin_clzll(m) : 1;
+    TwoConvPlan pl;
+    const int e = na + nb - 1 > (1ll << 21) ? FFT_SIZE_TOO_LARGE : twoconv_plan(r->bw, r->bw, na, nb, false, &pl);
+    if (e != OK) r->status = e;
+    else {
+        r->A64.assign((const long long*)a, (const long long*)a + na);
+        r->B64.assign((const long long*)b, (const long long*)b + nb);
+    }
+    return submit(*S, r);
+}
+
+int cumodp_server_poll(cumodp_server* h, long long id) {
+    Server* S = (Server*)h;
+    if (!S) return -1;
+    std::lock_guard<std::mutex> g(S->m);
+    auto it = S->reqs.find(id);
+    if (it == S->reqs.end()) return -1;
+    return it->second->done ? 1 : 0;
+}
+
+int cumodp_server_wait(cumodp_server* h, long long id, long long timeout_us) {
+    Server* S = (Server*)h;
+    if (!S) return -1;
+    std::unique_lock<std::mutex> lk(S->m);
+    auto it = S->reqs.find(id);
+    if (it == S->reqs.end()) return -1;
+    Req* r = it->second;
+    auto pred = [&] { return r->done; };
+    if (timeout_us < 0) S->cv_done.wait(lk, pred);
+    else if (!S->cv_done.wait_for(lk, std::chrono::microseconds(timeout_us), pred)) return -2;
+    const int st = r->status;
+    S->reqs.erase(it);
+    delete r;
+    return st;
+}
+
+void cumodp_server_get_stats(cumodp_server* h, cumodp_server_stats* out) {
+    Server* S = (Server*)h;
+    if (!S || !out) return;
+    std::lock_guard<std::mutex> g(S->m);
+    memset(out, 0, sizeof(*out));
+    out->completed = S->completed;
+    out->failed = S->failed;
+    out->batches = S->batches;
+    out->pending = (long long)S->pending.size();
+    out->inflight_bytes = S->inflight;
+    std::vector<double> l = S->lat;
+    if (!l.empty()) {
+        std::sort(l.begin(), l.end());
+        out->p50_us = l[l.size() / 2];
+        out->p99_us = l[std::min(l.size() - 1, (size_t)(0.99 * l.size()))];
+        out->max_us = l.back();
+    }
+    const double span = (S->t_last - S->t_first) * 1e-6;
+    out->products_per_s = span > 0 ? S->completed / span : 0;
+}
+
+void cumodp_server_reset_stats(cumodp_server* h) {
+    Server* S = (Server*)h;
+    if (!S) return;
+    std::lock_guard<std::mutex> g(S->m);
+    S->lat.clear();
+    S->completed = S->failed = S->batches = 0;
+    S->t_first = S->t_last = 0;
+}
+
+void cumodp_server_destroy(cumodp_server* h) {
+    Server* S = (Server*)h;
+    if (!S) return;
+    {
+        std::unique_lock<std::mutex> lk(S->m);
+        // drain: wait for queued and in-flight work
+        S->cv_done.wait(lk, [&] {
+            bool busy = false;
+            for (auto& L : S->lanes) busy |= L.busy;
+            return S->pending.empty() && !busy && S->dispatched.empty();
+        });
+        S->stop = true;
+    }
+    S->cv_work.notify_all();
+    S->cv_free.notify_all();
+    S->cv_done.notify_all();
+    S->batcher.join();
+    S->completer.join();
+    cudaSetDevice(S->dev);
+    for (Lane& L : S->lanes) {
+        if (L.st) cudaStreamSynchronize(L.st);
+        L.din.release(); L.dout.release(); L.ws.release(); L.djobs.release();
+        L.hin.release(); L.hout.release(); L.hjobs.release();
+        if (L.st) cudaStreamDestroy(L.st);
+        if (L.ev) cudaEventDestroy(L.ev);
+    }
+    for (auto& kv : S->reqs) delete kv.second;
+    delete S;
+}
+
+}  // extern "C"

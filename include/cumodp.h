@@ -150,6 +150,94 @@ cumodp_err cumodp_fftmul_batch(int count, const sfixn *df, const int64_t *f_off,
                                const sfixn *dg, const int64_t *g_off, const sfixn *G,
                                const int64_t *h_off, sfixn *H, sfixn p);
 
+/* Addition.  Exact product of int64-coefficient polynomials: c = a * b in Z[y]
+ * with c written as signed 128-bit integers, two int64 words per
+ * coefficient (low word first), na+nb-1 coefficients.  Counterpart of the
+ * reference's C++ two_convolution_poly_mul (src/two_convolution_poly_mul.cu:
+ * 532-569) for coefficients that fit int64 (the reference takes GMP mpz).
+ * Same algorithm: limb split (K limbs of M bits, sign-magnitude), cyclic and
+ * negacyclic x-convolutions mod Fourier primes 962592769, 950009857,
+ * 940572673, CRT, (u+v)/2 + 2^N (u-v)/2.  method 0 picks the cheapest exact
+ * (K, M, primes); method 1 forces the smallest limb split that needs only
+ * two primes.  Returns CUMODP_ASSUMPTION_ERROR when the exact product does
+ * not fit 127 bits, CUMODP_FFT_SIZE_TOO_LARGE beyond 2^21 coefficients. */
+cumodp_err cumodp_twoconv_mul_i64(long long na, const int64_t *a, long long nb, const int64_t *b, int64_t *c,
+                                  int method);
+/* Addition.  Same on DEVICE pointers, on a caller stream (0 = library stream,
+ * then synchronised); bit_width is max over both inputs of the bit length of
+ * |coefficient| (cumodp_twoconv_bit_width on host data). */
+cumodp_err cumodp_twoconv_mul_i64_dev(long long na, const int64_t *a, long long nb, const int64_t *b, int64_t *c,
+                                      int bit_width, int method, void *stream);
+/* Addition.  Bit width of the largest |coefficient| (0 counts as width 1),
+ * as find_largest_bit_width_of_coefficients (src/two_convolution_poly_mul.cu:
+ * 58-70); -1 on bad arguments. */
+int cumodp_twoconv_bit_width(long long na, const int64_t *a, long long nb, const int64_t *b);
+/* Addition.  The (K, M, number of primes) the product of two inputs of the
+ * given bit widths and lengths uses (determine_bivariate_base,
+ * src/two_convolution_poly_mul.cu:72-82, re-derived from an exactness bound
+ * instead of the reference's fixed table). */
+cumodp_err cumodp_twoconv_plan(int bit_width_a, int bit_width_b, long long na, long long nb, int method, int *K,
+                               int *M, int *nprimes);
+
+/* ---------------------------------------------------- serving (addition) -- */
+/* A request loop with continuous batching.  Requests (modular products, or
+ * exact int64 products) are copied at submission; a batcher thread admits
+ * them in arrival order while the device-memory budget allows, groups them
+ * by (kind, prime) and runs each group as one batch on a free lane (stream
+ * plus device buffers); batches on different lanes overlap on the GPU, and
+ * requests arriving meanwhile join the next batch.  Results are written to
+ * the caller's output buffer, which must stay valid until the request is
+ * waited for.  No counterpart in the reference. */
+typedef struct cumodp_server cumodp_server;
+typedef struct {
+    int device;              /* CUDA device ordinal */
+    size_t memory_budget;    /* device bytes for requests in flight (0: a quarter of free memory) */
+    int max_batch;           /* requests per batch (default 512) */
+    int batch_window_us;     /* wait for more arrivals once work is queued (default 50) */
+    int lanes;               /* batches in flight at once (default 4) */
+    int inject_fault_batch;  /* tests: the n-th batch fails on the host before launching (0 = off) */
+} cumodp_server_config;
+typedef struct {
+    long long completed, failed, batches, pending;
+    size_t inflight_bytes;
+    double p50_us, p99_us, max_us;  /* submission-to-result latency of completed requests */
+    double products_per_s;          /* completed / (last completion - first submission) */
+} cumodp_server_stats;
+void cumodp_server_default_config(cumodp_server_config *cfg);
+cumodp_server *cumodp_server_create(const cumodp_server_config *cfg);
+/* H receives df+dg+1 words.  Returns the request id (> 0), -1 on bad arguments. */
+long long cumodp_server_submit_mod(cumodp_server *s, sfixn p, sfixn df, const sfixn *F, sfixn dg, const sfixn *G,
+                                   sfixn *H);
+/* c receives na+nb-1 signed 128-bit coefficients as (lo, hi) int64 pairs. */
+long long cumodp_server_submit_i64(cumodp_server *s, long long na, const int64_t *a, long long nb, const int64_t *b,
+                                   int64_t *c);
+/* 1 done, 0 pending, -1 unknown id. */
+int cumodp_server_poll(cumodp_server *s, long long id);
+/* Waits (timeout_us < 0: forever) and returns the request's cumodp_err, -2
+ * on timeout, -1 for an unknown id; a waited-for id is forgotten. */
+int cumodp_server_wait(cumodp_server *s, long long id, long long timeout_us);
+void cumodp_server_get_stats(cumodp_server *s, cumodp_server_stats *out);
+void cumodp_server_reset_stats(cumodp_server *s);
+/* Drains queued and in-flight work, then frees everything. */
+void cumodp_server_destroy(cumodp_server *s);
+
+/* Addition.  Device-pointer natural-order transform on a caller stream (0 =
+ * the library's stream, then synchronised): forward as cumodp_fft_uni, or
+ * the inverse of it when `inverse` is nonzero.  X is a DEVICE pointer. */
+cumodp_err cumodp_fft_uni_dev(sfixn *X, sfixn n, sfixn k, sfixn w, sfixn p, int inverse, void *stream);
+
+/* Addition.  Makes `dev` the current device of the calling thread for the
+ * library's own CUDA runtime (one process per GPU). */
+cumodp_err cumodp_select_device(int dev);
+
+/* Addition.  Per-pass tracing: when enabled, every kernel launch that is not
+ * being captured into a graph is bracketed by CUDA events on its stream.
+ * cumodp_trace_report writes "kernel launches total_ms" lines (NUL
+ * terminated, truncated to len) and returns the full report length;
+ * `reset` clears the totals. */
+void cumodp_trace_passes(int enable);
+size_t cumodp_trace_report(char *buf, size_t len, int reset);
+
 /* Addition.  Bytes of device memory the library currently holds (tables,
  * workspace, plans). */
 size_t cumodp_device_bytes_in_use(void);

@@ -1,0 +1,65 @@
+"""Batched products of uneven degree (one graph launch per batch) vs the oracle."""
+import numpy as np
+import pytest
+
+from cumodp_b200.workloads import SplitMix64, seed_for
+
+P0 = 469762049
+pytestmark = pytest.mark.gpu
+
+
+def make_pairs(r, degs, p):
+    return [(r.residues(int(a) + 1, p), r.residues(int(b) + 1, p)) for a, b in degs]
+
+
+def test_mixed_batch_all_classes(cm, oracle_mod):
+    """Every size class from 2^5 to 2^20 in one batch, each checked."""
+    r = SplitMix64(11)
+    degs = [(0, 0), (3, 9), (31, 32), (40, 100), (300, 200), (1000, 1023), (2000, 2047), (4095, 4096),
+            (8191, 8000), (9000, 9000), (16383, 16384), (30000, 40000), (65535, 65535), (200000, 100000),
+            (5, 7), (511, 511), (1, 70000)]
+    pairs = make_pairs(r, degs, P0)
+    outs = cm.fftmul_batch(pairs, P0)
+    for (a, b), h in zip(pairs, outs):
+        assert np.array_equal(h, oracle_mod.polymul(a, b, P0))
+
+
+def test_batch_repeat_uses_cached_plan_and_new_data(cm, oracle_mod):
+    r = SplitMix64(12)
+    degs = [(100, 200), (5000, 5000), (20000, 3)] * 3
+    for rep in range(3):
+        pairs = make_pairs(r, degs, P0)
+        outs = cm.fftmul_batch(pairs, P0)
+        for (a, b), h in zip(pairs, outs):
+            assert np.array_equal(h, oracle_mod.polymul(a, b, P0))
+
+
+def test_c4_shape_sample(cm, oracle_mod):
+    """A 256-pair slice of the C4 workload (degrees log-uniform in [32, 65536])."""
+    r = SplitMix64(seed_for(3))
+    da = r.log_uniform_int(256, 32, 65536)
+    db = r.log_uniform_int(256, 32, 65536)
+    pairs = make_pairs(r, list(zip(da, db)), P0)
+    outs = cm.fftmul_batch(pairs, P0)
+    for (a, b), h in zip(pairs, outs):
+        assert np.array_equal(h, oracle_mod.polymul(a, b, P0))
+
+
+def test_batch_same_result_as_single_calls(cm):
+    r = SplitMix64(13)
+    degs = [(17, 4000), (777, 778), (12000, 30000)]
+    pairs = make_pairs(r, degs, 962592769)
+    outs = cm.fftmul_batch(pairs, 962592769)
+    for (a, b), h in zip(pairs, outs):
+        assert np.array_equal(h, cm.fftmul_uni(a, b, 962592769))
+
+
+def test_empty_batch(cm):
+    assert cm.fftmul_batch([], P0) == []
+
+
+def test_batch_rejects_oversize(cm):
+    a = np.ones(200, np.uint32)
+    with pytest.raises(cm.CumodpError) as e:
+        cm.fftmul_batch([(a, a)], 257)
+    assert e.value.code == cm.FFT_SIZE_TOO_LARGE

@@ -1,0 +1,129 @@
+"""Serving loop: continuous batching gives each request the same result alone and in the mix."""
+import threading
+
+import numpy as np
+import pytest
+
+from cumodp_b200.workloads import SplitMix64
+
+PRIMES = [469762049, 754974721, 962592769]
+pytestmark = pytest.mark.gpu
+
+
+def _mix(r, count, max_log=17):
+    reqs = []
+    kinds = r.uniform01(count)
+    degs_a = r.log_uniform_int(count, 32, 1 << max_log)
+    degs_b = r.log_uniform_int(count, 32, 1 << max_log)
+    pidx = (r.next_u64(count) % np.uint64(3)).astype(int)
+    for i in range(count):
+        if kinds[i] < 0.2:
+            n, m = int(min(degs_a[i], 20000)), int(min(degs_b[i], 20000))
+            reqs.append(("i64", r.int64_in(n + 1, 10**10), r.int64_in(m + 1, 10**10)))
+        else:
+            p = PRIMES[pidx[i]]
+            reqs.append(("mod", p, r.residues(int(degs_a[i]) + 1, p), r.residues(int(degs_b[i]) + 1, p)))
+    return reqs
+
+
+def _submit(srv, req):
+    if req[0] == "mod":
+        return srv.submit_mod(req[2], req[3], req[1])
+    return srv.submit_i64(req[1], req[2])
+
+
+def test_same_result_alone_and_in_the_mix(cm):
+    r = SplitMix64(99)
+    reqs = _mix(r, 120)
+    with cm.Server(max_batch=64, batch_window_us=100) as srv:
+        alone = []
+        for q in reqs:  # one at a time: each request is its own batch
+            rid, out = _submit(srv, q)
+            assert srv.wait(rid) == 0
+            alone.append(out.copy())
+        # the same requests from 4 submitting threads at once, interleaved
+        mixed = [None] * len(reqs)
+
+        def worker(k):
+            ids = []
+            for i in range(k, len(reqs), 4):
+                ids.append((i, _submit(srv, reqs[i])))
+            for i, (rid, out) in ids:
+                assert srv.wait(rid) == 0
+                mixed[i] = out.copy()
+
+        th = [threading.Thread(target=worker, args=(k,)) for k in range(4)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        st = srv.stats()
+    for a, m in zip(alone, mixed):
+        assert np.array_equal(a, m)
+    assert st["completed"] >= 2 * len(reqs) and st["failed"] == 0
+    assert st["batches"] < 2 * len(reqs)  # the mixed phase was batched
+    assert st["p99_us"] >= st["p50_us"] > 0
+
+
+def test_results_match_single_calls(cm, oracle_mod):
+    r = SplitMix64(7)
+    reqs = _mix(r, 40, max_log=15)
+    with cm.Server() as srv:
+        handles = [_submit(srv, q) for q in reqs]
+        for q, (rid, out) in zip(reqs, handles):
+            assert srv.wait(rid) == 0
+            if q[0] == "mod":
+                assert np.array_equal(out, oracle_mod.polymul(q[2], q[3], q[1]))
+            else:
+                assert cm.int128_words_to_ints(out) == oracle_mod.polymul_i128(q[1], q[2])
+
+
+def test_invalid_request_reports_error_and_server_continues(cm):
+    with cm.Server() as srv:
+        rid, _ = srv.submit_mod(np.ones(10, np.uint32), np.ones(10, np.uint32), 1000)  # not prime
+        assert srv.wait(rid) == cm.ASSUMPTION_ERROR
+        big = np.ones(200, np.uint32)
+        rid, _ = srv.submit_mod(big, big, 257)  # beyond 257's 2-adic order
+        assert srv.wait(rid) == cm.FFT_SIZE_TOO_LARGE
+        a = np.arange(1, 100, dtype=np.uint32)
+        rid, out = srv.submit_mod(a, a, 469762049)
+        assert srv.wait(rid) == 0
+        assert np.array_equal(out, cm.fftmul_uni(a, a, 469762049))
+
+
+def test_injected_batch_failure_is_contained(cm):
+    """Host-side fault injection: batch 2 fails before any launch; later batches are exact."""
+    r = SplitMix64(5)
+    p = 469762049
+    with cm.Server(inject_fault_batch=2, batch_window_us=0) as srv:
+        results = []
+        for i in range(4):
+            a, b = r.residues(500 + i, p), r.residues(300, p)
+            rid, out = srv.submit_mod(a, b, p)
+            results.append((srv.wait(rid), a, b, out.copy()))
+        codes = [c for c, *_ in results]
+        assert codes.count(cm.OUT_OF_MEMORY) == 1 and codes[1] == cm.OUT_OF_MEMORY
+        for c, a, b, out in results:
+            if c == 0:
+                assert np.array_equal(out, cm.fftmul_uni(a, b, p))
+        st = srv.stats()
+        assert st["failed"] == 1
+
+
+def test_tight_memory_budget_still_completes(cm):
+    r = SplitMix64(8)
+    p = 469762049
+    with cm.Server(memory_budget=4 << 20, batch_window_us=0) as srv:  # 4 MiB: about one request at a time
+        hs = []
+        for _ in range(12):
+            a, b = r.residues(100000, p), r.residues(90000, p)
+            hs.append((a, b) + srv.submit_mod(a, b, p))
+        for a, b, rid, out in hs:
+            assert srv.wait(rid) == 0
+            assert np.array_equal(out, cm.fftmul_uni(a, b, p))
+
+
+def test_wait_timeout_and_unknown_id(cm):
+    with cm.Server() as srv:
+        assert srv.wait(123456, timeout_us=1000) == -1
+        assert srv.poll(123456) == -1
