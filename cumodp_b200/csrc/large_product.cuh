@@ -79,37 +79,90 @@ __device__ __forceinline__ u32 col_slot_to_k1(u32 s, const LevelPlan& PL, int L1
     return k;
 }
 
-// ------------------------------------------------------------- pass A ----
-// Forward column level LEV on the 32-column tile.  The first level reads the
-// operand from global memory, the last writes the workspace.
+// ------------------------------------------------------ column tiles ----
+// A column CTA owns a tile of 32 adjacent columns x n1 rows, stored row-major
+// in shared memory (128 bytes per row).  The tile is loaded and stored with
+// 16-byte accesses by all threads at once, so every load of the tile is in
+// flight together; the levels then run on shared memory with lane = column
+// (conflict-free, and every twiddle is warp-uniform: a broadcast).
+
+// Bulk-loads rows [0, n1) x columns [c0, c0 + 32) of src (row stride n2),
+// zero beyond `len` elements, reducing every word to [0, 2p) when `reduce`.
+template <int L1, int T>
+__device__ __forceinline__ void tile_load(u32* tile, const u32* __restrict__ src, long long len, int c0, int n2,
+                                          bool reduce, const PrimeK& pk) {
+    constexpr int Q = (1 << L1) * 8;  // 16-byte quads in the tile
+    const bool vec = ((reinterpret_cast<uintptr_t>(src) & 15) == 0);
+#pragma unroll 8
+    for (int idx = threadIdx.x; idx < Q; idx += T) {
+        const int r = idx >> 3, q = idx & 7;
+        const long long gi = (long long)r * n2 + c0 + 4 * q;
+        uint4 v;
+        if (vec && gi + 3 < len) {
+            v = __ldg(reinterpret_cast<const uint4*>(src + gi));
+        } else {
+            v.x = gi < len ? __ldg(src + gi) : 0u;
+            v.y = gi + 1 < len ? __ldg(src + gi + 1) : 0u;
+            v.z = gi + 2 < len ? __ldg(src + gi + 2) : 0u;
+            v.w = gi + 3 < len ? __ldg(src + gi + 3) : 0u;
+        }
+        if (reduce) {
+            v.x = mul_shoup(v.x, 1u, pk.one_q, pk.p);
+            v.y = mul_shoup(v.y, 1u, pk.one_q, pk.p);
+            v.z = mul_shoup(v.z, 1u, pk.one_q, pk.p);
+            v.w = mul_shoup(v.w, 1u, pk.one_q, pk.p);
+        }
+        *reinterpret_cast<uint4*>(tile + r * 32 + 4 * q) = v;
+    }
+}
+
+// Bulk-stores the tile; `final` reduces to [0, p) and stops at `len`.
+template <int L1, int T>
+__device__ __forceinline__ void tile_store(const u32* tile, u32* __restrict__ dst, long long len, int c0, int n2,
+                                           bool final, const PrimeK& pk) {
+    constexpr int Q = (1 << L1) * 8;
+    const bool vec = ((reinterpret_cast<uintptr_t>(dst) & 15) == 0);
+#pragma unroll 8
+    for (int idx = threadIdx.x; idx < Q; idx += T) {
+        const int r = idx >> 3, q = idx & 7;
+        const long long gi = (long long)r * n2 + c0 + 4 * q;
+        uint4 v = *reinterpret_cast<const uint4*>(tile + r * 32 + 4 * q);
+        if (final) {
+            v.x = red1(red2(v.x, pk.p2), pk.p);
+            v.y = red1(red2(v.y, pk.p2), pk.p);
+            v.z = red1(red2(v.z, pk.p2), pk.p);
+            v.w = red1(red2(v.w, pk.p2), pk.p);
+        }
+        if (vec && gi + 3 < len) {
+            *reinterpret_cast<uint4*>(dst + gi) = v;
+        } else {
+            if (gi < len) dst[gi] = v.x;
+            if (gi + 1 < len) dst[gi + 1] = v.y;
+            if (gi + 2 < len) dst[gi + 2] = v.z;
+            if (gi + 3 < len) dst[gi + 3] = v.w;
+        }
+    }
+}
+
+// Forward column level LEV, shared memory to shared memory.
 template <int L1, int LEV, int NW>
-__device__ __forceinline__ void col_fwd_level(u32* tile, const LargeArgs& A, const u32* src, int len,
-                                              u32* dst, int c, int n2) {
+__device__ __forceinline__ void col_fwd_level(u32* tile, const PrimeK& pk, const Tw* __restrict__ twc) {
     using LV = ColLevel<L1, LEV>;
     constexpr LevelPlan PL = col_plan(L1);
     constexpr int R = LV::R, TB = LV::TB, B = LV::B;
-    constexpr bool FIRST = LEV == 0, LAST = LEV + 1 == PL.nlev;
+    constexpr bool LAST = LEV + 1 == PL.nlev;
     constexpr int TASKS = (1 << L1) / R;
-    const u32 p = A.pkc.p, p2 = A.pkc.p2;
+    const u32 p = pk.p, p2 = pk.p2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int id = warp; id < TASKS; id += NW) {
         const int blk = id / TB, o = id % TB;
         const int row0 = blk * B + o;
         u32 x[R];
 #pragma unroll
-        for (int m = 0; m < R; ++m) {
-            const int row = row0 + TB * m;
-            if constexpr (FIRST) {
-                const long long gi = (long long)row * n2 + c;
-                u32 v = gi < len ? __ldg(src + gi) : 0u;
-                x[m] = mul_shoup(v, 1u, A.pkc.one_q, p);
-            } else {
-                x[m] = tile[row * 32 + lane];
-            }
-        }
-        dif_regs<R>(x, A.pkc.rc.f, p, p2);
+        for (int m = 0; m < R; ++m) x[m] = tile[(row0 + TB * m) * 32 + lane];
+        dif_regs<R>(x, pk.rc.f, p, p2);
         if constexpr (!LAST) {
-            const Tw* t = A.twc + LV::TWOFF + o * R;
+            const Tw* t = twc + LV::TWOFF + o * R;
 #pragma unroll
             for (int j = 1; j < R; ++j) {
                 const Tw w = t[j];  // uniform across the warp: broadcast
@@ -117,28 +170,62 @@ __device__ __forceinline__ void col_fwd_level(u32* tile, const LargeArgs& A, con
             }
         }
 #pragma unroll
-        for (int m = 0; m < R; ++m) {
-            const int row = row0 + TB * m;
-            if constexpr (LAST) dst[(size_t)row * n2 + c] = x[m];
-            else tile[row * 32 + lane] = x[m];
-        }
+        for (int m = 0; m < R; ++m) tile[(row0 + TB * m) * 32 + lane] = x[m];
     }
 }
 
 template <int L1, int LEV, int NW>
-__device__ __forceinline__ void col_fwd_levels(u32* tile, const LargeArgs& A, const u32* src, int len,
-                                               u32* dst, int c, int n2) {
+__device__ __forceinline__ void col_fwd_levels(u32* tile, const PrimeK& pk, const Tw* __restrict__ twc) {
     constexpr LevelPlan PL = col_plan(L1);
     if constexpr (LEV < PL.nlev) {
-        col_fwd_level<L1, LEV, NW>(tile, A, src, len, dst, c, n2);
-        if constexpr (LEV + 1 < PL.nlev) __syncthreads();
-        col_fwd_levels<L1, LEV + 1, NW>(tile, A, src, len, dst, c, n2);
+        col_fwd_level<L1, LEV, NW>(tile, pk, twc);
+        __syncthreads();
+        col_fwd_levels<L1, LEV + 1, NW>(tile, pk, twc);
     }
 }
 
-// grid: (n2/32 column tiles, 2 operands, jobs)
+// Inverse column level LEV (pre-twiddle, DIT), shared memory to shared memory.
+template <int L1, int LEV, int NW>
+__device__ __forceinline__ void col_inv_level(u32* tile, const PrimeK& pk, const Tw* __restrict__ twci) {
+    using LV = ColLevel<L1, LEV>;
+    constexpr LevelPlan PL = col_plan(L1);
+    constexpr int R = LV::R, TB = LV::TB, B = LV::B;
+    constexpr bool DEEPEST = LEV + 1 == PL.nlev;
+    constexpr int TASKS = (1 << L1) / R;
+    const u32 p = pk.p, p2 = pk.p2;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int id = warp; id < TASKS; id += NW) {
+        const int blk = id / TB, o = id % TB;
+        const int row0 = blk * B + o;
+        u32 x[R];
+#pragma unroll
+        for (int m = 0; m < R; ++m) x[m] = tile[(row0 + TB * m) * 32 + lane];
+        if constexpr (!DEEPEST) {
+            const Tw* t = twci + LV::TWOFF + o * R;
+#pragma unroll
+            for (int j = 1; j < R; ++j) {
+                const Tw w = t[j];
+                x[j] = mul_shoup(x[j], w.w, w.wq, p);
+            }
+        }
+        dit_regs<R>(x, pk.rc.i, p, p2);
+#pragma unroll
+        for (int m = 0; m < R; ++m) tile[(row0 + TB * m) * 32 + lane] = x[m];
+    }
+}
+
+template <int L1, int LEV, int NW>
+__device__ __forceinline__ void col_inv_levels(u32* tile, const PrimeK& pk, const Tw* __restrict__ twci) {
+    if constexpr (LEV >= 0) {
+        col_inv_level<L1, LEV, NW>(tile, pk, twci);
+        __syncthreads();
+        col_inv_levels<L1, LEV - 1, NW>(tile, pk, twci);
+    }
+}
+
+// pass A, grid: (n2/32 column tiles, operands, jobs)
 template <int L1, int NW>
-__global__ void __launch_bounds__(NW * 32) k_col_fwd(const __grid_constant__ LargeArgs A) {
+__global__ void __launch_bounds__(NW * 32, 1) k_col_fwd(const __grid_constant__ LargeArgs A) {
     extern __shared__ __align__(16) u32 tile[];
     const LargeJob& J = A.jobs ? A.jobs[blockIdx.z] : A.job0;
     const int op = blockIdx.y;
@@ -146,71 +233,24 @@ __global__ void __launch_bounds__(NW * 32) k_col_fwd(const __grid_constant__ Lar
     const int len = op ? J.lb : J.la;
     u32* dst = op ? J.wb : J.wa;
     const int n2 = 1 << A.l2;
-    const int c = blockIdx.x * 32 + (threadIdx.x & 31);
-    col_fwd_levels<L1, 0, NW>(tile, A, src, len, dst, c, n2);
+    const int c0 = blockIdx.x * 32;
+    tile_load<L1, NW * 32>(tile, src, len, c0, n2, true, A.pkc);
+    __syncthreads();
+    col_fwd_levels<L1, 0, NW>(tile, A.pkc, A.twc);
+    tile_store<L1, NW * 32>(tile, dst, 1ll << (L1 + A.l2), c0, n2, false, A.pkc);
 }
 
-// ------------------------------------------------------------- pass C ----
-template <int L1, int LEV, int NW>
-__device__ __forceinline__ void col_inv_level(u32* tile, const LargeArgs& A, const u32* src, u32* h,
-                                              int lh, int c, int n2) {
-    using LV = ColLevel<L1, LEV>;
-    constexpr LevelPlan PL = col_plan(L1);
-    constexpr int R = LV::R, TB = LV::TB, B = LV::B;
-    constexpr bool DEEPEST = LEV + 1 == PL.nlev, OUTER = LEV == 0;
-    constexpr int TASKS = (1 << L1) / R;
-    const u32 p = A.pkc.p, p2 = A.pkc.p2;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int id = warp; id < TASKS; id += NW) {
-        const int blk = id / TB, o = id % TB;
-        const int row0 = blk * B + o;
-        u32 x[R];
-#pragma unroll
-        for (int m = 0; m < R; ++m) {
-            const int row = row0 + TB * m;
-            if constexpr (DEEPEST) x[m] = src[(size_t)row * n2 + c];
-            else x[m] = tile[row * 32 + lane];
-        }
-        if constexpr (!DEEPEST) {
-            const Tw* t = A.twc + A.twc_inv + LV::TWOFF + o * R;
-#pragma unroll
-            for (int j = 1; j < R; ++j) {
-                const Tw w = t[j];
-                x[j] = mul_shoup(x[j], w.w, w.wq, p);
-            }
-        }
-        dit_regs<R>(x, A.pkc.rc.i, p, p2);
-#pragma unroll
-        for (int m = 0; m < R; ++m) {
-            const int row = row0 + TB * m;
-            if constexpr (OUTER) {
-                const long long gi = (long long)row * n2 + c;
-                if (gi < lh) h[gi] = red1(red2(x[m], p2), p);
-            } else {
-                tile[row * 32 + lane] = x[m];
-            }
-        }
-    }
-}
-
-template <int L1, int LEV, int NW>
-__device__ __forceinline__ void col_inv_levels(u32* tile, const LargeArgs& A, const u32* src, u32* h,
-                                               int lh, int c, int n2) {
-    if constexpr (LEV >= 0) {
-        col_inv_level<L1, LEV, NW>(tile, A, src, h, lh, c, n2);
-        if constexpr (LEV > 0) __syncthreads();
-        col_inv_levels<L1, LEV - 1, NW>(tile, A, src, h, lh, c, n2);
-    }
-}
-
-// grid: (n2/32 column tiles, 1, jobs)
+// pass C, grid: (n2/32 column tiles, 1, jobs)
 template <int L1, int NW>
-__global__ void __launch_bounds__(NW * 32) k_col_inv(const __grid_constant__ LargeArgs A) {
+__global__ void __launch_bounds__(NW * 32, 1) k_col_inv(const __grid_constant__ LargeArgs A) {
     extern __shared__ __align__(16) u32 tile[];
     const LargeJob& J = A.jobs ? A.jobs[blockIdx.z] : A.job0;
     const int n2 = 1 << A.l2;
-    const int c = blockIdx.x * 32 + (threadIdx.x & 31);
-    col_inv_levels<L1, col_plan(L1).nlev - 1, NW>(tile, A, J.wa, J.h, J.lh, c, n2);
+    const int c0 = blockIdx.x * 32;
+    tile_load<L1, NW * 32>(tile, J.wa, 1ll << (L1 + A.l2), c0, n2, false, A.pkc);
+    __syncthreads();
+    col_inv_levels<L1, col_plan(L1).nlev - 1, NW>(tile, A.pkc, A.twc + A.twc_inv);
+    tile_store<L1, NW * 32>(tile, J.h, J.lh, c0, n2, true, A.pkc);
 }
 
 // ------------------------------------------------------------- pass B ----
@@ -253,15 +293,25 @@ __global__ void __launch_bounds__(small_threads(L2), 1) k_row_fused(const __grid
     const u32* rowG = J.wb + (size_t)s * n2;
     RowCtx ctx{A.pk, A.twr, A.twr_inv};
 
-    // level 0 forward with the inter-pass twiddle, from global memory
+    // both rows into shared memory with 16-byte loads, all in flight at once
+#pragma unroll 8
+    for (int i = threadIdx.x * 4; i < n2; i += T * 4) {
+        const uint4 f = __ldg(reinterpret_cast<const uint4*>(rowF + i));
+        const uint4 g = __ldg(reinterpret_cast<const uint4*>(rowG + i));
+        *reinterpret_cast<uint4*>(sm + swz(i)) = f;
+        *reinterpret_cast<uint4*>(sm + swz(n2 + i)) = g;
+    }
+    __syncthreads();
+
+    // level 0 forward with the inter-pass twiddle
     for (int o = threadIdx.x; o < TB0; o += T) {
         const u32 mo = seed_mont(A, (k1 * (u32)o) & nmask, false);  // w^(k1 o) * 2^32
         u32 xf[R0], xg[R0];
 #pragma unroll
         for (int m = 0; m < R0; ++m) {
             const u32 cm = mul_shoup(mo, bf[m].w, bf[m].wq, p);  // w^(k1 (o + TB0 m)) * 2^32
-            xf[m] = mul_mont(__ldg(rowF + o + TB0 * m), cm, p, pinv);
-            xg[m] = mul_mont(__ldg(rowG + o + TB0 * m), cm, p, pinv);
+            xf[m] = mul_mont(sm[swz(o + TB0 * m)], cm, p, pinv);
+            xg[m] = mul_mont(sm[swz(n2 + o + TB0 * m)], cm, p, pinv);
         }
         dif_regs<R0>(xf, A.pk.rc.f, p, p2);
         dif_regs<R0>(xg, A.pk.rc.f, p, p2);

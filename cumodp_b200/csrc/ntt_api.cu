@@ -198,10 +198,10 @@ void launch_colfwd1_t(const LargeArgs& a, int tiles, cudaStream_t st) {
     const size_t smem = (size_t)(1 << L1) * 32 * sizeof(u32);
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_col_fwd<L1, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_col_fwd<L1, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    k_col_fwd<L1, 8><<<dim3(tiles, 1, 1), 256, smem, st>>>(a);
+    k_col_fwd<L1, 16><<<dim3(tiles, 1, 1), 512, smem, st>>>(a);
 }
 typedef void (*ColFn)(const LargeArgs&, int, cudaStream_t);
 const ColFn kColFwd1[11] = {nullptr, launch_colfwd1_t<1>, launch_colfwd1_t<2>, launch_colfwd1_t<3>,

@@ -27,7 +27,7 @@ const SmallFn kSmall[15] = {nullptr, nullptr, nullptr, nullptr, nullptr,
                             launch_small_t<11>, launch_small_t<12>, launch_small_t<13>,
                             launch_small_t<14>};
 
-constexpr int kColWarps = 8;
+constexpr int kColWarps = 16;
 
 template <int L1>
 void launch_col_fwd_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {

@@ -84,6 +84,63 @@ std::vector<Tw> build_level_tables(const LevelPlan& pl, int logl, u32 root, u32 
 
 Tw tw_of(u32 w, u32 p) { return Tw{w, shoup_quot(w, p)}; }
 
+size_t level_tables_entries(int kind, int logl) {
+    const LevelPlan pl = kind == 0 ? row_plan(logl) : col_plan(logl);
+    return (size_t)2 * plan_tw_entries(pl, logl) + 2;
+}
+
+int level_tables_into(int kind, u32 p, u32 root, int logl, Tw* out, size_t cap) {
+    const LevelPlan pl = kind == 0 ? row_plan(logl) : col_plan(logl);
+    if (pl.nlev == 0 || level_tables_entries(kind, logl) > cap) return ASSUMPTION_ERROR;
+    const int nf = plan_tw_entries(pl, logl);
+    const u32 rinv = powmod_exact(root, (1ull << logl) - 1, p);
+    int off = 0, lb = logl;
+    for (int i = 0; i + 1 < pl.nlev; ++i) {
+        const int r = pl.logr[i], R = 1 << r, TB = (1 << lb) / R;
+        const u32 wb = powmod_exact(root, 1ull << (logl - lb), p);
+        const u32 wbi = powmod_exact(rinv, 1ull << (logl - lb), p);
+        for (int o = 0; o < TB; ++o)
+            for (int j = 0; j < R; ++j) {
+                u64 e = (u64)o * bitrev((u32)j, r);
+                out[off + o * R + j] = tw_of(powmod_exact(wb, e, p), p);
+                out[nf + off + o * R + j] = tw_of(powmod_exact(wbi, e, p), p);
+            }
+        off += 1 << lb;
+        lb -= r;
+    }
+    return OK;
+}
+
+size_t seed_words(int logn) {
+    const u64 n = 1ull << logn;
+    return 2 * (size_t)(std::min<u64>(n, 4096) + std::max<u64>(1, n / 4096));
+}
+
+int seeds_into(u32 p, u32 root, int logn, u32* s, size_t cap) {
+    if (seed_words(logn) > cap) return ASSUMPTION_ERROR;
+    const u64 n = 1ull << logn;
+    const u32 nlo = (u32)std::min<u64>(n, 4096), nhi = (u32)std::max<u64>(1, n / 4096);
+    const u32 r1 = (u32)((1ull << 32) % p);
+    const u32 rinv = powmod_exact(root, n - 1, p);
+    u32 w = 1, wi = 1;
+    for (u32 t = 0; t < nlo; ++t) {
+        s[t] = mulmod_exact(w, r1, p);
+        s[nlo + nhi + t] = mulmod_exact(wi, r1, p);
+        w = mulmod_exact(w, root, p);
+        wi = mulmod_exact(wi, rinv, p);
+    }
+    const u32 step = powmod_exact(root, 4096, p), stepi = powmod_exact(rinv, 4096, p);
+    w = 1;
+    wi = 1;
+    for (u32 t = 0; t < nhi; ++t) {
+        s[nlo + t] = mulmod_exact(w, r1, p);
+        s[2 * nlo + nhi + t] = mulmod_exact(wi, r1, p);
+        w = mulmod_exact(w, step, p);
+        wi = mulmod_exact(wi, stepi, p);
+    }
+    return OK;
+}
+
 PrimeK make_prime_k(const PrimeInfo& pi, u32 w32) {
     PrimeK k;
     k.p = pi.p;

@@ -60,6 +60,13 @@ const Tw* col_tables(int dev, u32 p, u32 root, int logl, int* err);
 // of two entries yields w^(lo+hi) * 2^32.
 const u32* seed_tables(int dev, u32 p, u32 root, int logn, int* err);
 
+// The same tables written into caller storage (no allocation):
+// level_tables_entries / seed_words give the sizes.
+size_t level_tables_entries(int kind, int logl);  // kind 0: row plan, 1: column plan
+int level_tables_into(int kind, u32 p, u32 root, int logl, Tw* out, size_t cap);
+size_t seed_words(int logn);
+int seeds_into(u32 p, u32 root, int logn, u32* out, size_t cap);
+
 // Per-device scratch that grows on demand (never shrinks while the process
 // lives).  Each call site names a slot so concurrent users do not collide.
 void* workspace(int dev, int slot, size_t bytes, int* err);
