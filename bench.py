@@ -333,6 +333,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     if rank == 0 and not args.no_extras:
         extras["ntt_2_24"] = ntt_2_24(cm, torch, dev, stream, hbm_peak)
         extras["batched_c4"] = batched_c4(cm, torch, dev, stream)
+        extras["c1_4095x4095"] = c1_latency(cm, torch, dev, stream)
     cpu = None
     if rank == 0 and world == 1 and not args.no_extras:
         cpu = cpu_baseline()
@@ -441,6 +442,59 @@ def batched_c4(cm, torch, dev, stream):
     return {"pairs": cnt, "ms_batched": round(t_batch, 4), "products_per_s_batched": round(cnt / (t_batch / 1000), 1),
             "ms_one_call_per_pair": round(t_single, 4), "ms_one_call_per_pair_wall": round(t_single_wall, 4),
             "speedup_vs_one_call": round(t_single / t_batch, 2), "batched_equals_single": same}
+
+
+def c1_latency(cm, torch, dev, stream):
+    """Config 1: one 4095 x 4095 product mod 469762049 (transform 8192): latency and batched copies."""
+    from cumodp_b200.workloads import SplitMix64, seed_for
+    r = SplitMix64(seed_for(0))
+    a, b = r.residues(4096, P), r.residues(4096, P)
+    dA = torch.from_numpy(a.view(np.int32)).to(dev)
+    dB = torch.from_numpy(b.view(np.int32)).to(dev)
+    dH = torch.empty(8191, dtype=torch.int32, device=dev)
+    sp = stream.cuda_stream
+    for _ in range(5):
+        cm.fftmul_uni_dev(dH.data_ptr(), 8191, dA.data_ptr(), 4095, dB.data_ptr(), 4095, P, sp)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    reps = 200
+    e0.record(stream)
+    for _ in range(reps):
+        cm.fftmul_uni_dev(dH.data_ptr(), 8191, dA.data_ptr(), 4095, dB.data_ptr(), 4095, P, sp)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    dev_us = e0.elapsed_time(e1) * 1000 / reps
+    # host entry point, pageable numpy buffers, one product per call
+    for _ in range(5):
+        cm.fftmul_uni(a, b, P)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        h = cm.fftmul_uni(a, b, P)
+    host_us = (time.perf_counter() - t0) * 1e6 / reps
+    ok = product_check(a, b, h)
+    # R = 4096 independent copies in one batched call (device buffers)
+    R = 4096
+    F = dA.repeat(R)
+    G = dB.repeat(R)
+    H = torch.empty(R * 8191, dtype=torch.int32, device=dev)
+    df = np.full(R, 4095, np.int32)
+    offs = np.arange(R, dtype=np.int64) * 4096
+    hoff = np.arange(R, dtype=np.int64) * 8191
+    for _ in range(3):
+        cm.fftmul_batch_dev(df, offs, F.data_ptr(), df, offs, G.data_ptr(), hoff, H.data_ptr(), P, sp)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(5):
+        cm.fftmul_batch_dev(df, offs, F.data_ptr(), df, offs, G.data_ptr(), hoff, H.data_ptr(), P, sp)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    batch_ms = e0.elapsed_time(e1) / 5
+    same = bool(torch.equal(H[:8191], dH))
+    return {"device_us_per_call": round(dev_us, 2), "host_us_per_call": round(host_us, 2),
+            "eval_point_identity": ok, "batched_copies": R, "batched_ms": round(batch_ms, 4),
+            "batched_products_per_s": round(R / (batch_ms / 1000), 1),
+            "batched_mulmods_per_s": round(R * 167936 / (batch_ms / 1000), 1), "batched_equals_single": same}
 
 
 def cpu_baseline():
