@@ -96,6 +96,9 @@ def _lib():
         L.cumodp_fftmul_batch_dev.restype = C.c_int
         L.cumodp_fftmul_batch_dev.argtypes = [C.c_int, _i32p, _i64p, C.c_void_p, _i32p, _i64p, C.c_void_p,
                                               _i64p, C.c_void_p, C.c_int32, C.c_void_p]
+        L.cumodp_fftmul_uni_dev_noalloc.restype = C.c_int
+        L.cumodp_fftmul_uni_dev_noalloc.argtypes = [C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32,
+                                                    C.c_void_p, C.c_int32, C.c_void_p]
         L.cumodp_fft_uni_dev.restype = C.c_int
         L.cumodp_fft_uni_dev.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int,
                                          C.c_void_p]
@@ -193,6 +196,20 @@ def fftmul_uni_dev(h_ptr: int, lh: int, f_ptr: int, df: int, g_ptr: int, dg: int
     """Device-pointer product: lh words of H = F * G mod p (``cumodp_fftmul_uni_dev``)."""
     _check(_lib().cumodp_fftmul_uni_dev(lh, h_ptr, df, f_ptr, dg, g_ptr, p, stream or None),
            "cumodp_fftmul_uni_dev")
+
+
+def fftmul_uni_dev_noalloc(h_ptr: int, lh: int, f_ptr: int, df: int, g_ptr: int, dg: int, p: int,
+                           stream: int = 0) -> None:
+    """Device-pointer product that allocates no device memory (``cumodp_fftmul_uni_dev_noalloc``).
+
+    For callers that may not allocate device memory (work captured into
+    someone else's CUDA graph, pool-owned device memory, plugins in a host
+    that partitioned device memory).  Scratch is a fixed ~8.4 MiB array in
+    the library's device data segment; products up to df + dg + 1 <= 2^20;
+    calls that overlap on the GPU race on that array.
+    """
+    _check(_lib().cumodp_fftmul_uni_dev_noalloc(lh, h_ptr, df, f_ptr, dg, g_ptr, p, stream or None),
+           "cumodp_fftmul_uni_dev_noalloc")
 
 
 # ----------------------------------------------------------- transforms ----

@@ -133,6 +133,22 @@ const sfixn *interp_subres_coeff3(sfixn *nx, sfixn *ny, void *scb, sfixn i, sfix
 cumodp_err cumodp_fftmul_uni_dev(sfixn lh, sfixn *H, sfixn df, const sfixn *F,
                                  sfixn dg, const sfixn *G, sfixn p, void *stream);
 
+/* Addition (no counterpart in the reference).  The device-pointer product of
+ * cumodp_fftmul_uni_dev for callers that cannot allocate device memory --
+ * code running while another component captures the device's work into a
+ * CUDA graph, services whose device memory belongs to their own pool
+ * allocator, plugins loaded after the host partitioned all device memory.
+ * It calls no cudaMalloc/cudaFree and no allocating library routine: its
+ * scratch (workspace and twiddle tables) is one fixed ~8.4 MiB array in the
+ * library's device data segment, held by every GPU that loads the library
+ * until exit.  Limit: df + dg + 1 <= 2^20 (CUMODP_FFT_SIZE_TOO_LARGE
+ * beyond).  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the array: calls whose GPU work overlaps race.  stream 0
+ * runs on the default stream and synchronises before returning. */
+cumodp_err cumodp_fftmul_uni_dev_noalloc(sfixn lh, sfixn *H, sfixn df, const sfixn *F,
+                                         sfixn dg, const sfixn *G, sfixn p, void *stream);
+
 /* Addition.  Batched products mod one prime, all on the device: product i is
  * H_i = F_i * G_i with F_i = F + f_off[i] (df[i]+1 words), G_i = G + g_off[i]
  * (dg[i]+1 words), H_i = H + h_off[i] (df[i]+dg[i]+1 words).  f_off, g_off,
