@@ -304,7 +304,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     product_gbs = prod_alg / (ms / args.steps / 1000.0) / 1e9 / world
 
     # e2e through the host C entry point, pinned host buffers
-    L = cm.lib()
+    L = ctypes.CDLL(cm.LIB_PATH)  # own function objects: the binding's prototypes stay untouched
     hA = torch.from_numpy(ops[0][0].view(np.int32)).pin_memory()
     hB = torch.from_numpy(ops[0][1].view(np.int32)).pin_memory()
     hH = torch.empty(n - 1, dtype=torch.int32).pin_memory()
@@ -334,6 +334,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         extras["ntt_2_24"] = ntt_2_24(cm, torch, dev, stream, hbm_peak)
         extras["batched_c4"] = batched_c4(cm, torch, dev, stream)
         extras["c1_4095x4095"] = c1_latency(cm, torch, dev, stream)
+        extras["serving_c5"] = serving_c5(cm)
     cpu = None
     if rank == 0 and world == 1 and not args.no_extras:
         cpu = cpu_baseline()
@@ -495,6 +496,61 @@ def c1_latency(cm, torch, dev, stream):
             "eval_point_identity": ok, "batched_copies": R, "batched_ms": round(batch_ms, 4),
             "batched_products_per_s": round(R / (batch_ms / 1000), 1),
             "batched_mulmods_per_s": round(R * 167936 / (batch_ms / 1000), 1), "batched_equals_single": same}
+
+
+def serving_c5(cm, rates=(1000, 10000, 100000), max_requests=3000, max_seconds=1.5):
+    """Config 5: Poisson arrivals of mixed requests into the continuous-batching server.
+
+    Degrees log-uniform in [2^5, 2^20]; prime uniform over {469762049,
+    754974721, 962592769}; 20% exact int64 products (|c| <= 10^10, degrees
+    capped at 2^14 so the 127-bit bound holds).  Requests whose product
+    exceeds the prime's 2-adic order (962592769 supports 2^21 points) are
+    answered with CUMODP_FFT_SIZE_TOO_LARGE and counted as rejected.
+    Latency = submission to result on the host.
+    """
+    from cumodp_b200.workloads import SplitMix64, seed_for
+    primes = (469762049, 754974721, 962592769)
+    r = SplitMix64(seed_for(4))
+    pool_u = r.residues(1 << 21, 469762049)        # operand slices come from these pools
+    pool_i = r.int64_in(1 << 15, 10**10)
+    out = {}
+    for rate in rates:
+        n = max_requests
+        gaps = -np.log(1.0 - r.uniform01(n)) / rate
+        da = r.log_uniform_int(n, 32, 1 << 20)
+        db = r.log_uniform_int(n, 32, 1 << 20)
+        kind = r.uniform01(n)
+        pidx = (r.next_u64(n) % np.uint64(3)).astype(int)
+        offs = (r.next_u64(2 * n) % np.uint64(1 << 20)).astype(np.int64)
+        with cm.Server(max_batch=256, batch_window_us=50, lanes=4) as srv:
+            ids = []
+            t0 = time.perf_counter()
+            t_next = t0
+            for i in range(n):
+                t_next += gaps[i]
+                while time.perf_counter() < t_next:
+                    pass
+                if kind[i] < 0.2:
+                    a = pool_i[offs[i] % (1 << 14):][: min(int(da[i]), 1 << 14) + 1]
+                    b = pool_i[offs[n + i] % (1 << 14):][: min(int(db[i]), 1 << 14) + 1]
+                    ids.append(srv.submit_i64(a, b)[0])
+                else:
+                    a = pool_u[offs[i]:offs[i] + int(da[i]) + 1]
+                    b = pool_u[offs[n + i]:offs[n + i] + int(db[i]) + 1]
+                    ids.append(srv.submit_mod(a, b, primes[pidx[i]])[0])
+                if time.perf_counter() - t0 > max_seconds:
+                    break
+            codes = [srv.wait(rid) for rid in ids]
+            span = time.perf_counter() - t0
+            st = srv.stats()
+        ok = sum(1 for c in codes if c == 0)
+        out[str(rate)] = {"submitted": len(ids), "completed": ok,
+                          "rejected_size": sum(1 for c in codes if c == cm.FFT_SIZE_TOO_LARGE),
+                          "failed_other": sum(1 for c in codes if c not in (0, cm.FFT_SIZE_TOO_LARGE)),
+                          "p50_ms": round(st["p50_us"] / 1000, 3), "p99_ms": round(st["p99_us"] / 1000, 3),
+                          "products_per_s": round(ok / span, 1), "batches": st["batches"],
+                          "offered_per_s": round(len(ids) / span, 1)}
+    return out
 
 
 def cpu_baseline():

@@ -155,9 +155,12 @@ def _check(code: int, what: str) -> None:
 
 
 def _as_i32(x) -> np.ndarray:
+    """32-bit words of x as an int32 view (no copy for contiguous int32/uint32 input)."""
     a = np.asarray(x)
     if a.dtype == np.int32:
         return np.ascontiguousarray(a)
+    if a.dtype == np.uint32:
+        return np.ascontiguousarray(a).view(np.int32)
     return np.ascontiguousarray(a.astype(np.uint32).view(np.int32))
 
 

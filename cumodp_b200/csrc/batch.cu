@@ -76,7 +76,7 @@ std::vector<int> legal_row_logs(int logn) {
     return v;
 }
 
-int tune_row_log(const PrimeCtx& pc, int logn, int njobs, int dev, cudaStream_t st) {
+int tune_row_log(const PrimeCtx& pc, int logn, int njobs, int dev, cudaStream_t st, bool allow_tuning) {
     const char* off = getenv("CUMODP_AUTOTUNE");
     if (off && off[0] == '0') return default_row_log(logn);
     const TuneKey key{dev, logn, job_bucket(njobs)};
@@ -86,6 +86,7 @@ int tune_row_log(const PrimeCtx& pc, int logn, int njobs, int dev, cudaStream_t 
         auto it = g_tune.find(key);
         if (it != g_tune.end()) return it->second;
     }
+    if (!allow_tuning) return default_row_log(logn);
     const std::vector<int> cands = legal_row_logs(logn);
     if (cands.size() <= 1) return cands.empty() ? default_row_log(logn) : cands[0];
     // synthetic class: `jobs` products of two length-n/2 operands
@@ -221,7 +222,7 @@ int build_plan(BatchPlan& P, const PrimeCtx& pc, cudaStream_t st) {
         jb += c.members.size() * (c.large ? sizeof(LargeJob) : sizeof(ProdJob));
         jb = (jb + 255) & ~(size_t)255;
         if (c.large) {
-            c.l2 = tune_row_log(pc, c.logn, (int)c.members.size(), P.dev, st);
+            c.l2 = tune_row_log(pc, c.logn, (int)c.members.size(), P.dev, st, true);
             c.ws_off = ws;
             ws += c.members.size() * (2ull << c.logn);
         }
@@ -413,7 +414,7 @@ size_t direct_job_bytes(int count) {
 
 int direct_batch(int count, const u32* const* a, const long long* la, const u32* const* b, const long long* lb,
                  u32* const* h, const long long* lh, u32 p, u32* ws, void* djobs, void* hjobs,
-                 cudaStream_t st) {
+                 cudaStream_t st, bool allow_tuning) {
     int err = OK;
     const PrimeCtx* pc = prime_ctx(p, &err);
     if (!pc) return err;
@@ -452,7 +453,7 @@ int direct_batch(int count, const u32* const* a, const long long* la, const u32*
             }
         }
         launches.push_back(Launch{logn, off, (int)mem.size(),
-                                  large ? tune_row_log(*pc, logn, (int)mem.size(), dev, st) : 0});
+                                  large ? tune_row_log(*pc, logn, (int)mem.size(), dev, st, allow_tuning) : 0});
         off += mem.size() * (large ? sizeof(LargeJob) : sizeof(ProdJob));
         off = (off + 255) & ~(size_t)255;
     }

@@ -88,24 +88,23 @@ __device__ __forceinline__ u32 col_slot_to_k1(u32 s, const LevelPlan& PL, int L1
 
 // Bulk-loads rows [0, n1) x columns [c0, c0 + 32) of src (row stride n2),
 // zero beyond `len` elements, reducing every word to [0, 2p) when `reduce`.
+// Rows entirely inside `len` take a branch-free 16-byte path when src is
+// 16-byte aligned; only the boundary row checks elements one by one, and
+// rows entirely past `len` are zero-filled without loads.
 template <int L1, int T>
 __device__ __forceinline__ void tile_load(u32* tile, const u32* __restrict__ src, long long len, int c0, int n2,
                                           bool reduce, const PrimeK& pk) {
-    constexpr int Q = (1 << L1) * 8;  // 16-byte quads in the tile
+    constexpr int n1 = 1 << L1;
+    constexpr int Q = n1 * 8;  // 16-byte quads in the tile
     const bool vec = ((reinterpret_cast<uintptr_t>(src) & 15) == 0);
-#pragma unroll 8
-    for (int idx = threadIdx.x; idx < Q; idx += T) {
+    // rows [0, rf) lie fully below len; rows [re, n1) fully at or above it
+    const long long lc = len - c0;
+    const int rf = vec ? (int)(lc >= 32 ? min((long long)n1, (lc - 32) / n2 + 1) : 0) : 0;
+    const int re = (int)(lc > 0 ? min((long long)n1, (lc - 1) / n2 + 1) : 0);
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < rf * 8; idx += T) {
         const int r = idx >> 3, q = idx & 7;
-        const long long gi = (long long)r * n2 + c0 + 4 * q;
-        uint4 v;
-        if (vec && gi + 3 < len) {
-            v = __ldg(reinterpret_cast<const uint4*>(src + gi));
-        } else {
-            v.x = gi < len ? __ldg(src + gi) : 0u;
-            v.y = gi + 1 < len ? __ldg(src + gi + 1) : 0u;
-            v.z = gi + 2 < len ? __ldg(src + gi + 2) : 0u;
-            v.w = gi + 3 < len ? __ldg(src + gi + 3) : 0u;
-        }
+        uint4 v = __ldg(reinterpret_cast<const uint4*>(src + (long long)r * n2 + c0 + 4 * q));
         if (reduce) {
             v.x = mul_shoup(v.x, 1u, pk.one_q, pk.p);
             v.y = mul_shoup(v.y, 1u, pk.one_q, pk.p);
@@ -114,16 +113,48 @@ __device__ __forceinline__ void tile_load(u32* tile, const u32* __restrict__ src
         }
         *reinterpret_cast<uint4*>(tile + r * 32 + 4 * q) = v;
     }
+    for (int idx = rf * 8 + threadIdx.x; idx < re * 8; idx += T) {
+        const int r = idx >> 3, q = idx & 7;
+        const long long gi = (long long)r * n2 + c0 + 4 * q;
+        uint4 v;
+        v.x = gi < len ? __ldg(src + gi) : 0u;
+        v.y = gi + 1 < len ? __ldg(src + gi + 1) : 0u;
+        v.z = gi + 2 < len ? __ldg(src + gi + 2) : 0u;
+        v.w = gi + 3 < len ? __ldg(src + gi + 3) : 0u;
+        if (reduce) {
+            v.x = mul_shoup(v.x, 1u, pk.one_q, pk.p);
+            v.y = mul_shoup(v.y, 1u, pk.one_q, pk.p);
+            v.z = mul_shoup(v.z, 1u, pk.one_q, pk.p);
+            v.w = mul_shoup(v.w, 1u, pk.one_q, pk.p);
+        }
+        *reinterpret_cast<uint4*>(tile + r * 32 + 4 * q) = v;
+    }
+    for (int idx = re * 8 + threadIdx.x; idx < Q; idx += T)
+        *reinterpret_cast<uint4*>(tile + (idx >> 3) * 32 + 4 * (idx & 7)) = make_uint4(0u, 0u, 0u, 0u);
 }
 
 // Bulk-stores the tile; `final` reduces to [0, p) and stops at `len`.
 template <int L1, int T>
 __device__ __forceinline__ void tile_store(const u32* tile, u32* __restrict__ dst, long long len, int c0, int n2,
                                            bool final, const PrimeK& pk) {
-    constexpr int Q = (1 << L1) * 8;
+    constexpr int n1 = 1 << L1;
     const bool vec = ((reinterpret_cast<uintptr_t>(dst) & 15) == 0);
-#pragma unroll 8
-    for (int idx = threadIdx.x; idx < Q; idx += T) {
+    const long long lc = len - c0;
+    const int rf = vec ? (int)(lc >= 32 ? min((long long)n1, (lc - 32) / n2 + 1) : 0) : 0;
+    const int re = (int)(lc > 0 ? min((long long)n1, (lc - 1) / n2 + 1) : 0);
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < rf * 8; idx += T) {
+        const int r = idx >> 3, q = idx & 7;
+        uint4 v = *reinterpret_cast<const uint4*>(tile + r * 32 + 4 * q);
+        if (final) {
+            v.x = red1(red2(v.x, pk.p2), pk.p);
+            v.y = red1(red2(v.y, pk.p2), pk.p);
+            v.z = red1(red2(v.z, pk.p2), pk.p);
+            v.w = red1(red2(v.w, pk.p2), pk.p);
+        }
+        *reinterpret_cast<uint4*>(dst + (long long)r * n2 + c0 + 4 * q) = v;
+    }
+    for (int idx = rf * 8 + threadIdx.x; idx < re * 8; idx += T) {
         const int r = idx >> 3, q = idx & 7;
         const long long gi = (long long)r * n2 + c0 + 4 * q;
         uint4 v = *reinterpret_cast<const uint4*>(tile + r * 32 + 4 * q);
@@ -133,14 +164,10 @@ __device__ __forceinline__ void tile_store(const u32* tile, u32* __restrict__ ds
             v.z = red1(red2(v.z, pk.p2), pk.p);
             v.w = red1(red2(v.w, pk.p2), pk.p);
         }
-        if (vec && gi + 3 < len) {
-            *reinterpret_cast<uint4*>(dst + gi) = v;
-        } else {
-            if (gi < len) dst[gi] = v.x;
-            if (gi + 1 < len) dst[gi + 1] = v.y;
-            if (gi + 2 < len) dst[gi + 2] = v.z;
-            if (gi + 3 < len) dst[gi + 3] = v.w;
-        }
+        if (gi < len) dst[gi] = v.x;
+        if (gi + 1 < len) dst[gi + 1] = v.y;
+        if (gi + 2 < len) dst[gi + 2] = v.z;
+        if (gi + 3 < len) dst[gi + 3] = v.w;
     }
 }
 
@@ -160,7 +187,7 @@ __device__ __forceinline__ void col_fwd_level(u32* tile, const PrimeK& pk, const
         u32 x[R];
 #pragma unroll
         for (int m = 0; m < R; ++m) x[m] = tile[(row0 + TB * m) * 32 + lane];
-        dif_regs<R>(x, pk.rc.f, p, p2);
+        dif_regs<R, !LAST>(x, pk.rc.f, p, p2);
         if constexpr (!LAST) {
             const Tw* t = twc + LV::TWOFF + o * R;
 #pragma unroll
@@ -208,7 +235,7 @@ __device__ __forceinline__ void col_inv_level(u32* tile, const PrimeK& pk, const
                 x[j] = mul_shoup(x[j], w.w, w.wq, p);
             }
         }
-        dit_regs<R>(x, pk.rc.i, p, p2);
+        dit_regs<R, !DEEPEST>(x, pk.rc.i, p, p2);
 #pragma unroll
         for (int m = 0; m < R; ++m) tile[(row0 + TB * m) * 32 + lane] = x[m];
     }
@@ -261,9 +288,9 @@ __device__ __forceinline__ u32 seed_mont(const LargeArgs& A, u32 e, bool inv) {
 }
 
 template <int L2>
-__global__ void __launch_bounds__(small_threads(L2), 1) k_row_fused(const __grid_constant__ LargeArgs A) {
+__global__ void __launch_bounds__(row_threads(L2), 1) k_row_fused(const __grid_constant__ LargeArgs A) {
     constexpr int n2 = 1 << L2;
-    constexpr int T = small_threads(L2);
+    constexpr int T = row_threads(L2);
     constexpr LevelPlan PL = row_plan(L2);
     static_assert(PL.nlev >= 2, "row pass needs at least two levels");
     using LV0 = SmallLevel<L2, 0>;
@@ -313,8 +340,8 @@ __global__ void __launch_bounds__(small_threads(L2), 1) k_row_fused(const __grid
             xf[m] = mul_mont(sm[swz(o + TB0 * m)], cm, p, pinv);
             xg[m] = mul_mont(sm[swz(n2 + o + TB0 * m)], cm, p, pinv);
         }
-        dif_regs<R0>(xf, A.pk.rc.f, p, p2);
-        dif_regs<R0>(xg, A.pk.rc.f, p, p2);
+        dif_regs<R0, true>(xf, A.pk.rc.f, p, p2);
+        dif_regs<R0, true>(xg, A.pk.rc.f, p, p2);
         Tw t[R0];
         load_tw<R0>(t, A.twr + o * R0);
 #pragma unroll
@@ -331,18 +358,29 @@ __global__ void __launch_bounds__(small_threads(L2), 1) k_row_fused(const __grid
     __syncthreads();
     small_fwd_levels<L2, 1, T, 1>(sm, ctx);
 
-    // last level: forward both, pointwise (Montgomery; the 2^-32 is undone by
-    // the inverse twiddle), inverse
+    // last level: forward DIF of every 32-word row of both operands, then
+    // per row the pointwise product (Montgomery; its 2^-32 is undone by the
+    // inverse twiddle) and the inverse DIT of that level
+    for (int row = threadIdx.x; row < n2 / 16; row += T) {
+        u32 x[32];
+        load_row32(x, sm, row * 32);  // rows [0, n2/32): F, then G
+        dif_regs<32>(x, A.pk.rc.f, p, p2);
+        store_row32(sm, row * 32, x);
+    }
+    __syncthreads();
     for (int row = threadIdx.x; row < n2 / 32; row += T) {
-        u32 xf[32], xg[32];
-        load_row32(xf, sm, row * 32);
-        load_row32(xg, sm, n2 + row * 32);
-        dif_regs<32>(xf, A.pk.rc.f, p, p2);
-        dif_regs<32>(xg, A.pk.rc.f, p, p2);
+        u32 x[32];
+        load_row32(x, sm, row * 32);
 #pragma unroll
-        for (int j = 0; j < 32; ++j) xf[j] = mul_mont(xf[j], xg[j], p, pinv);
-        dit_regs<32>(xf, A.pk.rc.i, p, p2);
-        store_row32(sm, row * 32, xf);
+        for (int c = 0; c < 8; ++c) {
+            const uint4 g = *reinterpret_cast<const uint4*>(sm + swz(n2 + row * 32 + 4 * c));
+            x[4 * c] = mul_mont(x[4 * c], g.x, p, pinv);
+            x[4 * c + 1] = mul_mont(x[4 * c + 1], g.y, p, pinv);
+            x[4 * c + 2] = mul_mont(x[4 * c + 2], g.z, p, pinv);
+            x[4 * c + 3] = mul_mont(x[4 * c + 3], g.w, p, pinv);
+        }
+        dit_regs<32>(x, A.pk.rc.i, p, p2);
+        store_row32(sm, row * 32, x);
     }
     __syncthreads();
     small_inv_levels<L2, PL.nlev - 2, T, 1, 1>(sm, ctx);
@@ -357,7 +395,7 @@ __global__ void __launch_bounds__(small_threads(L2), 1) k_row_fused(const __grid
         load_tw<R0>(t, A.twr + A.twr_inv + o * R0);
 #pragma unroll
         for (int j = 1; j < R0; ++j) x[j] = mul_shoup(x[j], t[j].w, t[j].wq, p);
-        dit_regs<R0>(x, A.pk.rc.i, p, p2);
+        dit_regs<R0, true>(x, A.pk.rc.i, p, p2);
         const u32 mo = seed_mont(A, (k1 * (u32)o) & nmask, true);  // w^-(k1 o) * 2^32
 #pragma unroll
         for (int m = 0; m < R0; ++m) {

@@ -67,7 +67,7 @@ __device__ __forceinline__ void fwd1_level(u32* sm, const PrimeK& pk, const Tw* 
         u32 x[R];
 #pragma unroll
         for (int m = 0; m < R; ++m) x[m] = sm[swz(base + TB * m)];
-        dif_regs<R>(x, pk.rc.f, p, p2);
+        dif_regs<R, true>(x, pk.rc.f, p, p2);
         Tw t[R];
         load_tw<R>(t, tw + LV::TWOFF + o * R);
 #pragma unroll
@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(small_threads(L2), 1) k_row_ntt(const __grid_c
             if (twid) x[m] = mul_mont(v, mul_shoup(mo, bf[m].w, bf[m].wq, p), p, pinv);
             else x[m] = mul_shoup(v, 1u, A.pk.one_q, p);
         }
-        dif_regs<R0>(x, A.pk.rc.f, p, p2);
+        dif_regs<R0, true>(x, A.pk.rc.f, p, p2);
         Tw t[R0];
         load_tw<R0>(t, A.twr + o * R0);
 #pragma unroll
@@ -198,10 +198,10 @@ void launch_colfwd1_t(const LargeArgs& a, int tiles, cudaStream_t st) {
     const size_t smem = (size_t)(1 << L1) * 32 * sizeof(u32);
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_col_fwd<L1, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_col_fwd<L1, (L1 == 10 ? 32 : 16)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    k_col_fwd<L1, 16><<<dim3(tiles, 1, 1), 512, smem, st>>>(a);
+    k_col_fwd<L1, (L1 == 10 ? 32 : 16)><<<dim3(tiles, 1, 1), (L1 == 10 ? 32 : 16) * 32, smem, st>>>(a);
 }
 typedef void (*ColFn)(const LargeArgs&, int, cudaStream_t);
 const ColFn kColFwd1[11] = {nullptr, launch_colfwd1_t<1>, launch_colfwd1_t<2>, launch_colfwd1_t<3>,

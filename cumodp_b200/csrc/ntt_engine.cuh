@@ -44,8 +44,10 @@ struct PrimeK {
 __device__ __forceinline__ int swz(int i) { return i ^ (((i >> 5) & 7) << 2); }
 
 // Forward R-point DIF on registers; x[j] ends holding X[bitrev_r(j)].
-// Inputs and outputs in [0, 2p).
-template <int R>
+// Inputs in [0, 2p).  Outputs in [0, 2p), except that with TW (the caller
+// multiplies every output j >= 1 by a Shoup twiddle next, which accepts any
+// 32-bit input) the last stage leaves outputs j >= 1 in [0, 4p).
+template <int R, bool TW = false>
 __device__ __forceinline__ void dif_regs(u32 (&x)[R], const Tw* __restrict__ c, u32 p, u32 p2) {
 #pragma unroll
     for (int half = R / 2; half >= 1; half >>= 1) {
@@ -54,19 +56,22 @@ __device__ __forceinline__ void dif_regs(u32 (&x)[R], const Tw* __restrict__ c, 
 #pragma unroll
             for (int j = 0; j < half; ++j) {
                 const int e = j * (32 / (2 * half));  // w_{2half}^j = w_32^e
+                const bool lazy = TW && half == 1;
                 u32 a = x[g + j], b = x[g + j + half];
                 u32 s = a + b;
                 u32 d = a - b + p2;
-                x[g + j] = red2(s, p2);
-                x[g + j + half] = (e == 0) ? red2(d, p2) : mul_shoup(d, c[e].w, c[e].wq, p);
+                x[g + j] = (lazy && g + j != 0) ? s : red2(s, p2);
+                x[g + j + half] = (e == 0) ? (lazy ? d : red2(d, p2)) : mul_shoup(d, c[e].w, c[e].wq, p);
             }
         }
     }
 }
 
 // Inverse R-point DIT on registers (roots c = w_32^-j); x[j] holds Y[bitrev(j)]
-// on entry and R * y[j] on exit.  Inputs and outputs in [0, 4p).
-template <int R>
+// on entry and R * y[j] on exit.  Inputs and outputs in [0, 4p).  With PRE
+// (the caller multiplied every input j >= 1 by a Shoup twiddle, so those are
+// already in [0, 2p)) the first stage skips their reductions.
+template <int R, bool PRE = false>
 __device__ __forceinline__ void dit_regs(u32 (&x)[R], const Tw* __restrict__ c, u32 p, u32 p2) {
 #pragma unroll
     for (int half = 1; half < R; half <<= 1) {
@@ -75,9 +80,10 @@ __device__ __forceinline__ void dit_regs(u32 (&x)[R], const Tw* __restrict__ c, 
 #pragma unroll
             for (int j = 0; j < half; ++j) {
                 const int e = j * (32 / (2 * half));
-                u32 a = red2(x[g + j], p2);
+                const bool small_in = PRE && half == 1;
+                u32 a = (small_in && g + j != 0) ? x[g + j] : red2(x[g + j], p2);
                 u32 b = x[g + j + half];
-                u32 t = (e == 0) ? red2(b, p2) : mul_shoup(b, c[e].w, c[e].wq, p);
+                u32 t = (e == 0) ? (small_in ? b : red2(b, p2)) : mul_shoup(b, c[e].w, c[e].wq, p);
                 x[g + j] = a + t;
                 x[g + j + half] = a - t + p2;
             }

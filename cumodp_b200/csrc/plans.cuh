@@ -21,7 +21,7 @@ __host__ __device__ constexpr LevelPlan row_plan(int logl) {
         case 11: return LevelPlan{3, {3, 3, 5}};
         case 12: return LevelPlan{3, {3, 4, 5}};
         case 13: return LevelPlan{3, {4, 4, 5}};
-        case 14: return LevelPlan{4, {2, 3, 4, 5}};
+        case 14: return LevelPlan{4, {3, 3, 3, 5}};
         default: return LevelPlan{0, {0}};
     }
 }
@@ -46,8 +46,14 @@ __host__ __device__ constexpr LevelPlan col_plan(int logl) {
     }
 }
 
+// Threads of the three-pass row kernel: 2^14-word rows use 1024 threads with
+// at most 64 registers each (32 warps per SM; the plan's twiddled levels
+// have radix <= 8 so both operands fit), shorter rows the single-CTA count.
+__host__ __device__ constexpr int row_threads(int logl);
+
 // Threads and products per CTA for the fused single-CTA product of length L.
 __host__ __device__ constexpr int small_threads(int logl) { return logl >= 12 ? (1 << (logl - 5)) : 128; }
 __host__ __device__ constexpr int small_ppc(int logl) { return logl >= 12 ? 1 : (1 << (12 - logl)); }
+__host__ __device__ constexpr int row_threads(int logl) { return logl == 14 ? 1024 : small_threads(logl); }
 
 }  // namespace cmb

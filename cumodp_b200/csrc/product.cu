@@ -27,27 +27,29 @@ const SmallFn kSmall[15] = {nullptr, nullptr, nullptr, nullptr, nullptr,
                             launch_small_t<11>, launch_small_t<12>, launch_small_t<13>,
                             launch_small_t<14>};
 
-constexpr int kColWarps = 16;
+// 16-warp column CTAs; 32 for the 2^10-row tile (1 CTA per SM, <= 64 registers)
+template <int L1>
+constexpr int col_warps() { return L1 == 10 ? 32 : 16; }
 
 template <int L1>
 void launch_col_fwd_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
     const size_t smem = (size_t)(1 << L1) * 32 * sizeof(u32);
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_col_fwd<L1, kColWarps>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_col_fwd<L1, col_warps<L1>()>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    k_col_fwd<L1, kColWarps><<<grid, kColWarps * 32, smem, st>>>(a);
+    k_col_fwd<L1, col_warps<L1>()><<<grid, col_warps<L1>() * 32, smem, st>>>(a);
 }
 template <int L1>
 void launch_col_inv_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
     const size_t smem = (size_t)(1 << L1) * 32 * sizeof(u32);
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_col_inv<L1, kColWarps>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_col_inv<L1, col_warps<L1>()>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    k_col_inv<L1, kColWarps><<<grid, kColWarps * 32, smem, st>>>(a);
+    k_col_inv<L1, col_warps<L1>()><<<grid, col_warps<L1>() * 32, smem, st>>>(a);
 }
 template <int L2>
 void launch_row_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
@@ -57,7 +59,7 @@ void launch_row_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
         cudaFuncSetAttribute(k_row_fused<L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    k_row_fused<L2><<<grid, small_threads(L2), smem, st>>>(a);
+    k_row_fused<L2><<<grid, row_threads(L2), smem, st>>>(a);
 }
 
 typedef void (*PassFn)(const LargeArgs&, dim3, cudaStream_t);
@@ -82,8 +84,8 @@ void attr_small() {
 template <int L1>
 void attr_col() {
     const int smem = (1 << L1) * 32 * (int)sizeof(u32);
-    cudaFuncSetAttribute(k_col_fwd<L1, kColWarps>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(k_col_inv<L1, kColWarps>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_col_fwd<L1, col_warps<L1>()>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_col_inv<L1, col_warps<L1>()>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
 template <int L2>
 void attr_row() {

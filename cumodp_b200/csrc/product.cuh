@@ -32,9 +32,11 @@ void ensure_kernel_attrs();
 // Batched products on caller-owned buffers, direct launches (batch.cu).
 size_t direct_ws_words(int count, const long long* la, const long long* lb);
 size_t direct_job_bytes(int count);
+// allow_tuning: a size class seen for the first time may be autotuned
+// (synchronous timing runs); otherwise cached choices or the default split.
 int direct_batch(int count, const u32* const* a, const long long* la, const u32* const* b, const long long* lb,
                  u32* const* h, const long long* lh, u32 p, u32* ws, void* djobs, void* hjobs,
-                 cudaStream_t st);
+                 cudaStream_t st, bool allow_tuning);
 
 // h[0..lh) = a[0..la) * b[0..lb) mod p on device pointers, on stream st.
 int mul_dev(const u32* a, long long la, const u32* b, long long lb, u32* h, long long lh, u32 p,

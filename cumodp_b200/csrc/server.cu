@@ -207,8 +207,9 @@ int run_batch(Server& S, Lane& L) {
         }
         cudaError_t ce = cudaMemcpyAsync(L.din.p, L.hin.p, nin * 4, cudaMemcpyHostToDevice, L.st);
         if (ce != cudaSuccess) return cuda_err(ce);
+        // no autotuning on the serving path: cached or default splits only
         err = direct_batch(cnt, pa.data(), la.data(), pb.data(), lb.data(), ph.data(), lh.data(), p, L.ws.p,
-                           L.djobs.p, L.hjobs.p, L.st);
+                           L.djobs.p, L.hjobs.p, L.st, false);
         if (err != OK) return err;
         ce = cudaMemcpyAsync(L.hout.p, L.dout.p, nout * 4, cudaMemcpyDeviceToHost, L.st);
         if (ce != cudaSuccess) return cuda_err(ce);

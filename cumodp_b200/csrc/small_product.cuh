@@ -81,8 +81,8 @@ __device__ __forceinline__ void small_fwd_level(u32* sm, const Ctx& A) {
             xf[m] = sm[swz(base + TB * m)];
             xg[m] = sm[swz(base + L + TB * m)];
         }
-        dif_regs<R>(xf, A.pk.rc.f, p, p2);
-        dif_regs<R>(xg, A.pk.rc.f, p, p2);
+        dif_regs<R, true>(xf, A.pk.rc.f, p, p2);
+        dif_regs<R, true>(xg, A.pk.rc.f, p, p2);
         Tw t[R];
         load_tw<R>(t, A.tw + LV::TWOFF + o * R);
 #pragma unroll
@@ -117,7 +117,7 @@ __device__ __forceinline__ void small_inv_level(u32* sm, const Ctx& A) {
         load_tw<R>(t, A.tw + A.tw_inv_off + LV::TWOFF + o * R);
 #pragma unroll
         for (int j = 1; j < R; ++j) x[j] = mul_shoup(x[j], t[j].w, t[j].wq, p);
-        dit_regs<R>(x, A.pk.rc.i, p, p2);
+        dit_regs<R, true>(x, A.pk.rc.i, p, p2);
 #pragma unroll
         for (int m = 0; m < R; ++m) sm[swz(base + TB * m)] = x[m];
     }

@@ -301,7 +301,7 @@ int twoconv_mul_dev(const long long* a, long long la, const long long* b, long l
             }
             err = direct_batch(npts, pa.data(), LA.data(), pb.data(), LB.data(), ph.data(), LH.data(),
                                kTwoConvPrimes[r], bufs->ws + r * wsw, (char*)bufs->djobs + r * jb,
-                               (char*)bufs->hjobs + r * jb, st);
+                               (char*)bufs->hjobs + r * jb, st, false);
             if (err != OK) return err;
         }
     }

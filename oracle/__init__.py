@@ -23,6 +23,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libmodpn_ref.so")
+MODPN_GPU_SO = os.path.join(HERE, "_ref", "libmodpn_gpu.so")
 
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
@@ -31,10 +32,11 @@ _u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
 
 
 def build(ref: bool = False) -> None:
-    """Compile liboracle.so (and the modpn reference when ``ref``)."""
+    """Compile liboracle.so (and, when ``ref``, the modpn reference builds)."""
     subprocess.check_call(["make", "-s", "-C", HERE, "oracle"])
     if ref:
         subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
+        subprocess.check_call(["make", "-s", "-C", HERE, "modpn_gpu"])
 
 
 _lib = None
@@ -215,6 +217,33 @@ def ref_polymul(a: np.ndarray, b: np.ndarray, p: int) -> np.ndarray:
     h = np.empty(len(a) + len(b) - 1, dtype=np.int32)
     if L.ref_fftmul(len(a) - 1, a, len(b) - 1, b, h, p) != 0:
         raise RuntimeError("modpn product failed")
+    return h.view(np.uint32)
+
+
+def modpn_gpu_available() -> bool:
+    return os.path.exists(MODPN_GPU_SO)
+
+
+_mg = None
+
+
+def modpn_gpu_polymul(a: np.ndarray, b: np.ndarray, p: int) -> np.ndarray:
+    """modpn's in-place product with its GPU dispatch compiled in, linked to libcumodp.so.
+
+    For transform sizes >= 2^16 modpn itself calls can_call_fftmul_uni and
+    cumodp_fftmul_uni (modpn/src/FMUL.c:1943-1957); below that it multiplies
+    on the CPU.  Used to show the library is a drop-in for modpn.
+    """
+    global _mg
+    if _mg is None:
+        _mg = C.CDLL(MODPN_GPU_SO)
+        _mg.modpn_gpu_fftmul.restype = C.c_int
+        _mg.modpn_gpu_fftmul.argtypes = [C.c_int32, _i32p, C.c_int32, _i32p, _i32p, C.c_int32]
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.uint32).view(np.int32))
+    b = np.ascontiguousarray(np.asarray(b, dtype=np.uint32).view(np.int32))
+    h = np.empty(len(a) + len(b) - 1, dtype=np.int32)
+    if _mg.modpn_gpu_fftmul(len(a) - 1, a, len(b) - 1, b, h, p) != 0:
+        raise RuntimeError("modpn prime error")
     return h.view(np.uint32)
 
 

@@ -47,3 +47,15 @@ def test_queries_without_gpu_do_not_crash():
     n = cm.num_of_cuda_devices()
     assert n >= 0
     assert cm.is_cuda_enabled() == (n > 0)
+
+
+def test_modpn_links_against_this_library():
+    """modpn with its GPU dispatch links unchanged against libcumodp.so (no GPU call)."""
+    import oracle
+    if not oracle.modpn_gpu_available():
+        pytest.skip("modpn GPU-dispatch build absent (needs the reference sources)")
+    import subprocess
+    out = subprocess.run(["ldd", oracle.MODPN_GPU_SO], capture_output=True, text=True).stdout
+    assert "libcumodp.so" in out
+    lib = ctypes.CDLL(oracle.MODPN_GPU_SO)  # resolves cumodp_fftmul_uni / can_call_fftmul_uni
+    assert hasattr(lib, "modpn_gpu_fftmul")
