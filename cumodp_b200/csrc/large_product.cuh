@@ -41,6 +41,7 @@ struct LargeArgs {
     const LargeJob* __restrict__ jobs;  // device job table, or nullptr: use job0
     int njobs;
     LevelPlan colpl;             // column plan (row slot -> k1 map)
+    int row_fused;               // 1: one fused row kernel; 0: the split pair
     LargeJob job0;
 };
 
@@ -261,9 +262,13 @@ __global__ void __launch_bounds__(NW * 32, 1) k_col_fwd(const __grid_constant__ 
     u32* dst = op ? J.wb : J.wa;
     const int n2 = 1 << A.l2;
     const int c0 = blockIdx.x * 32;
+    // the plan's twiddles (warp-uniform reads) next to the tile
+    constexpr int NTW = col_tw_entries(L1);
+    Tw* tws = reinterpret_cast<Tw*>(tile + (32 << L1));
+    for (int i = threadIdx.x; i < NTW; i += NW * 32) tws[i] = A.twc[i];
     tile_load<L1, NW * 32>(tile, src, len, c0, n2, true, A.pkc);
     __syncthreads();
-    col_fwd_levels<L1, 0, NW>(tile, A.pkc, A.twc);
+    col_fwd_levels<L1, 0, NW>(tile, A.pkc, tws);
     tile_store<L1, NW * 32>(tile, dst, 1ll << (L1 + A.l2), c0, n2, false, A.pkc);
 }
 
@@ -274,9 +279,12 @@ __global__ void __launch_bounds__(NW * 32, 1) k_col_inv(const __grid_constant__ 
     const LargeJob& J = A.jobs ? A.jobs[blockIdx.z] : A.job0;
     const int n2 = 1 << A.l2;
     const int c0 = blockIdx.x * 32;
+    constexpr int NTW = col_tw_entries(L1);
+    Tw* tws = reinterpret_cast<Tw*>(tile + (32 << L1));
+    for (int i = threadIdx.x; i < NTW; i += NW * 32) tws[i] = A.twc[A.twc_inv + i];
     tile_load<L1, NW * 32>(tile, J.wa, 1ll << (L1 + A.l2), c0, n2, false, A.pkc);
     __syncthreads();
-    col_inv_levels<L1, col_plan(L1).nlev - 1, NW>(tile, A.pkc, A.twc + A.twc_inv);
+    col_inv_levels<L1, col_plan(L1).nlev - 1, NW>(tile, A.pkc, tws);
     tile_store<L1, NW * 32>(tile, J.h, J.lh, c0, n2, true, A.pkc);
 }
 
@@ -401,6 +409,158 @@ __global__ void __launch_bounds__(row_threads(L2), 1) k_row_fused(const __grid_c
         for (int m = 0; m < R0; ++m) {
             const u32 d = mul_shoup(mo, bi[m].w, bi[m].wq, p);  // w^-(k1 c) * 2^64 / n
             rowH[o + TB0 * m] = mul_mont(red2(x[m], p2), d, p, pinv);
+        }
+    }
+}
+
+
+// ------------------------------------------------------------ pass B' ----
+// The row pass as two kernels of one operand each, so a CTA needs half the
+// shared memory (one 2^14-word row = 64 KiB) and two CTAs share an SM:
+//   k_row_fwd_g   row DFT of G' (inter-pass twiddle, all forward levels),
+//                 result written over G' in digit-reversed row order;
+//   k_row_mul_f   row DFT of F', pointwise product with that row of G^
+//                 read from global memory in the same order, inverse row
+//                 DFT, inverse twiddle with 2^64/n, result over F'.
+// Costs one extra n-word write and read of HBM against the fused pass.
+
+template <int L2>
+__device__ __forceinline__ void row_slot_factors(const LargeArgs& A, u32 k1, Tw* bf, Tw* bi) {
+    using LV0 = SmallLevel<L2, 0>;
+    constexpr int R0 = LV0::R, TB0 = LV0::TB;
+    const u32 nmask = (1u << (A.l1 + L2)) - 1;
+    const u32 p = A.pk.p, pinv = A.pk.pinv_neg;
+    if (threadIdx.x < 2 * R0) {
+        const bool inv = threadIdx.x >= R0;
+        if (inv && !bi) return;
+        const u32 m = threadIdx.x % R0;
+        const u32 e = (k1 * (u32)TB0 * m) & nmask;
+        u32 v = red1(mul_mont(seed_mont(A, e, inv), 1u, p, pinv), p);  // plain w^(+-e)
+        if (inv) v = (u32)(((u64)v * A.scale_rn) % p);
+        const Tw t{v, (u32)(((u64)v << 32) / p)};
+        if (inv) bi[m] = t; else bf[m] = t;
+    }
+}
+
+// Loads one row into swizzled shared memory with 16-byte loads.
+template <int L2, int T>
+__device__ __forceinline__ void row_load(u32* sm, const u32* __restrict__ row) {
+    constexpr int n2 = 1 << L2;
+#pragma unroll 8
+    for (int i = threadIdx.x * 4; i < n2; i += T * 4)
+        *reinterpret_cast<uint4*>(sm + swz(i)) = __ldg(reinterpret_cast<const uint4*>(row + i));
+}
+
+// Level 0 forward of one operand with the inter-pass twiddle w_n^(k1 c).
+template <int L2, int T>
+__device__ __forceinline__ void row_level0_fwd(u32* sm, const LargeArgs& A, u32 k1, const Tw* bf) {
+    using LV0 = SmallLevel<L2, 0>;
+    constexpr int R0 = LV0::R, TB0 = LV0::TB;
+    const u32 nmask = (1u << (A.l1 + L2)) - 1;
+    const u32 p = A.pk.p, p2 = A.pk.p2, pinv = A.pk.pinv_neg;
+    for (int o = threadIdx.x; o < TB0; o += T) {
+        Tw t[R0];
+        load_tw<R0>(t, A.twr + o * R0);
+        const u32 mo = seed_mont(A, (k1 * (u32)o) & nmask, false);  // w^(k1 o) * 2^32
+        u32 x[R0];
+#pragma unroll
+        for (int m = 0; m < R0; ++m)
+            x[m] = mul_mont(sm[swz(o + TB0 * m)], mul_shoup(mo, bf[m].w, bf[m].wq, p), p, pinv);
+        dif_regs<R0, true>(x, A.pk.rc.f, p, p2);
+#pragma unroll
+        for (int j = 1; j < R0; ++j) x[j] = mul_shoup(x[j], t[j].w, t[j].wq, p);
+#pragma unroll
+        for (int m = 0; m < R0; ++m) sm[swz(o + TB0 * m)] = x[m];
+    }
+}
+
+template <int L2>
+__global__ void __launch_bounds__(rowsplit_threads(L2), 2) k_row_fwd_g(const __grid_constant__ LargeArgs A) {
+    constexpr int n2 = 1 << L2;
+    constexpr int T = rowsplit_threads(L2);
+    constexpr LevelPlan PL = row_plan(L2);
+    static_assert(PL.nlev >= 2, "row pass needs at least two levels");
+    constexpr int R0 = SmallLevel<L2, 0>::R;
+    extern __shared__ __align__(16) u32 sm[];
+    __shared__ Tw bf[R0];
+    const LargeJob& J = A.jobs ? A.jobs[blockIdx.y] : A.job0;
+    const u32 s = blockIdx.x;
+    const u32 k1 = col_slot_to_k1(s, A.colpl, A.l1);
+    const u32 p = A.pk.p, p2 = A.pk.p2;
+    u32* row = J.wb + (size_t)s * n2;
+    row_slot_factors<L2>(A, k1, bf, nullptr);
+    row_load<L2, T>(sm, row);
+    __syncthreads();
+    row_level0_fwd<L2, T>(sm, A, k1, bf);
+    __syncthreads();
+    fwd1_levels<L2, 1, T>(sm, A.pk, A.twr);
+    for (int r = threadIdx.x; r < n2 / 32; r += T) {
+        u32 x[32];
+        load_row32(x, sm, r * 32);
+        dif_regs<32>(x, A.pk.rc.f, p, p2);
+        // store this 32-word row of the spectrum straight to global memory
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+            *reinterpret_cast<uint4*>(row + r * 32 + 4 * c) =
+                make_uint4(x[4 * c], x[4 * c + 1], x[4 * c + 2], x[4 * c + 3]);
+    }
+}
+
+template <int L2>
+__global__ void __launch_bounds__(rowsplit_threads(L2), 2) k_row_mul_f(const __grid_constant__ LargeArgs A) {
+    constexpr int n2 = 1 << L2;
+    constexpr int T = rowsplit_threads(L2);
+    constexpr LevelPlan PL = row_plan(L2);
+    static_assert(PL.nlev >= 2, "row pass needs at least two levels");
+    using LV0 = SmallLevel<L2, 0>;
+    constexpr int R0 = LV0::R, TB0 = LV0::TB;
+    extern __shared__ __align__(16) u32 sm[];
+    __shared__ Tw bf[R0], bi[R0];
+    const LargeJob& J = A.jobs ? A.jobs[blockIdx.y] : A.job0;
+    const u32 s = blockIdx.x;
+    const u32 k1 = col_slot_to_k1(s, A.colpl, A.l1);
+    const u32 nmask = (1u << (A.l1 + L2)) - 1;
+    const u32 p = A.pk.p, p2 = A.pk.p2, pinv = A.pk.pinv_neg;
+    u32* rowF = J.wa + (size_t)s * n2;
+    const u32* rowG = J.wb + (size_t)s * n2;
+    RowCtx ctx{A.pk, A.twr, A.twr_inv};
+    row_slot_factors<L2>(A, k1, bf, bi);
+    row_load<L2, T>(sm, rowF);
+    __syncthreads();
+    row_level0_fwd<L2, T>(sm, A, k1, bf);
+    __syncthreads();
+    fwd1_levels<L2, 1, T>(sm, A.pk, A.twr);
+    for (int r = threadIdx.x; r < n2 / 32; r += T) {
+        u32 x[32];
+        load_row32(x, sm, r * 32);
+        dif_regs<32>(x, A.pk.rc.f, p, p2);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const uint4 g = __ldg(reinterpret_cast<const uint4*>(rowG + r * 32 + 4 * c));
+            x[4 * c] = mul_mont(x[4 * c], g.x, p, pinv);
+            x[4 * c + 1] = mul_mont(x[4 * c + 1], g.y, p, pinv);
+            x[4 * c + 2] = mul_mont(x[4 * c + 2], g.z, p, pinv);
+            x[4 * c + 3] = mul_mont(x[4 * c + 3], g.w, p, pinv);
+        }
+        dit_regs<32>(x, A.pk.rc.i, p, p2);
+        store_row32(sm, r * 32, x);
+    }
+    __syncthreads();
+    small_inv_levels<L2, PL.nlev - 2, T, 1, 1>(sm, ctx);
+    for (int o = threadIdx.x; o < TB0; o += T) {
+        u32 x[R0];
+#pragma unroll
+        for (int m = 0; m < R0; ++m) x[m] = sm[swz(o + TB0 * m)];
+        Tw t[R0];
+        load_tw<R0>(t, A.twr + A.twr_inv + o * R0);
+#pragma unroll
+        for (int j = 1; j < R0; ++j) x[j] = mul_shoup(x[j], t[j].w, t[j].wq, p);
+        dit_regs<R0, true>(x, A.pk.rc.i, p, p2);
+        const u32 mo = seed_mont(A, (k1 * (u32)o) & nmask, true);  // w^-(k1 o) * 2^32
+#pragma unroll
+        for (int m = 0; m < R0; ++m) {
+            const u32 d = mul_shoup(mo, bi[m].w, bi[m].wq, p);  // w^-(k1 c) * 2^64 / n
+            rowF[o + TB0 * m] = mul_mont(red2(x[m], p2), d, p, pinv);
         }
     }
 }

@@ -55,38 +55,6 @@ __device__ __forceinline__ u32 row_pos_to_freq(u32 P) {
     return f;
 }
 
-// Single-operand forward level LEV (not the last) on a row in shared memory.
-template <int LOGL, int LEV, int T>
-__device__ __forceinline__ void fwd1_level(u32* sm, const PrimeK& pk, const Tw* __restrict__ tw) {
-    using LV = SmallLevel<LOGL, LEV>;
-    constexpr int L = 1 << LOGL, R = LV::R, TB = LV::TB, B = LV::B;
-    const u32 p = pk.p, p2 = pk.p2;
-    for (int id = threadIdx.x; id < L / R; id += T) {
-        const int blk = id / TB, o = id % TB;
-        const int base = blk * B + o;
-        u32 x[R];
-#pragma unroll
-        for (int m = 0; m < R; ++m) x[m] = sm[swz(base + TB * m)];
-        dif_regs<R, true>(x, pk.rc.f, p, p2);
-        Tw t[R];
-        load_tw<R>(t, tw + LV::TWOFF + o * R);
-#pragma unroll
-        for (int j = 1; j < R; ++j) x[j] = mul_shoup(x[j], t[j].w, t[j].wq, p);
-#pragma unroll
-        for (int m = 0; m < R; ++m) sm[swz(base + TB * m)] = x[m];
-    }
-}
-
-template <int LOGL, int LEV, int T>
-__device__ __forceinline__ void fwd1_levels(u32* sm, const PrimeK& pk, const Tw* __restrict__ tw) {
-    constexpr LevelPlan PL = row_plan(LOGL);
-    if constexpr (LEV + 1 < PL.nlev) {
-        fwd1_level<LOGL, LEV, T>(sm, pk, tw);
-        __syncthreads();
-        fwd1_levels<LOGL, LEV + 1, T>(sm, pk, tw);
-    }
-}
-
 template <int L2>
 __global__ void __launch_bounds__(small_threads(L2), 1) k_row_ntt(const __grid_constant__ RowNttArgs A) {
     constexpr int n2 = 1 << L2;
@@ -195,7 +163,7 @@ const RowNttFn kRowNtt[15] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullp
 // Forward-column launchers shared with the product path (single operand).
 template <int L1>
 void launch_colfwd1_t(const LargeArgs& a, int tiles, cudaStream_t st) {
-    const size_t smem = (size_t)(1 << L1) * 32 * sizeof(u32);
+    const size_t smem = col_smem_bytes(L1);
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_col_fwd<L1, (L1 == 10 ? 32 : 16)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

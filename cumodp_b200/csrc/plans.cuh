@@ -46,6 +46,16 @@ __host__ __device__ constexpr LevelPlan col_plan(int logl) {
     }
 }
 
+// Twiddle entries (one direction) of the column plan of length 2^logl.
+__host__ __device__ constexpr int col_tw_entries(int logl) {
+    int n = 0, lb = logl;
+    const LevelPlan pl = col_plan(logl);
+    for (int i = 0; i + 1 < pl.nlev; ++i) { n += 1 << lb; lb -= pl.logr[i]; }
+    return n;
+}
+// Dynamic shared memory of a column CTA: the 32-column tile and its twiddles.
+__host__ __device__ constexpr int col_smem_bytes(int logl) { return (32 << logl) * 4 + col_tw_entries(logl) * 8; }
+
 // Threads of the three-pass row kernel: 2^14-word rows use 1024 threads with
 // at most 64 registers each (32 warps per SM; the plan's twiddled levels
 // have radix <= 8 so both operands fit), shorter rows the single-CTA count.
@@ -55,5 +65,8 @@ __host__ __device__ constexpr int row_threads(int logl);
 __host__ __device__ constexpr int small_threads(int logl) { return logl >= 12 ? (1 << (logl - 5)) : 128; }
 __host__ __device__ constexpr int small_ppc(int logl) { return logl >= 12 ? 1 : (1 << (12 - logl)); }
 __host__ __device__ constexpr int row_threads(int logl) { return logl == 14 ? 1024 : small_threads(logl); }
+// Threads of the split row kernels (one operand row per CTA, two CTAs per
+// SM): one per 32-word row of the last level.
+__host__ __device__ constexpr int rowsplit_threads(int logl) { return logl >= 10 ? (1 << (logl - 5)) : 32; }
 
 }  // namespace cmb

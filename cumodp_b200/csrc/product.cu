@@ -2,6 +2,7 @@
 #include "product.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 
 namespace cmb {
@@ -33,7 +34,7 @@ constexpr int col_warps() { return L1 == 10 ? 32 : 16; }
 
 template <int L1>
 void launch_col_fwd_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
-    const size_t smem = (size_t)(1 << L1) * 32 * sizeof(u32);
+    const size_t smem = col_smem_bytes(L1);
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_col_fwd<L1, col_warps<L1>()>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -43,7 +44,7 @@ void launch_col_fwd_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
 }
 template <int L1>
 void launch_col_inv_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
-    const size_t smem = (size_t)(1 << L1) * 32 * sizeof(u32);
+    const size_t smem = col_smem_bytes(L1);
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_col_inv<L1, col_warps<L1>()>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -60,6 +61,15 @@ void launch_row_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
         attr = true;
     }
     k_row_fused<L2><<<grid, row_threads(L2), smem, st>>>(a);
+}
+
+template <int L2>
+void launch_row_g_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
+    k_row_fwd_g<L2><<<grid, rowsplit_threads(L2), (size_t)(1 << L2) * sizeof(u32), st>>>(a);
+}
+template <int L2>
+void launch_row_f_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
+    k_row_mul_f<L2><<<grid, rowsplit_threads(L2), (size_t)(1 << L2) * sizeof(u32), st>>>(a);
 }
 
 typedef void (*PassFn)(const LargeArgs&, dim3, cudaStream_t);
@@ -83,7 +93,7 @@ void attr_small() {
 }
 template <int L1>
 void attr_col() {
-    const int smem = (1 << L1) * 32 * (int)sizeof(u32);
+    const int smem = col_smem_bytes(L1);
     cudaFuncSetAttribute(k_col_fwd<L1, col_warps<L1>()>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     cudaFuncSetAttribute(k_col_inv<L1, col_warps<L1>()>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
@@ -92,6 +102,22 @@ void attr_row() {
     cudaFuncSetAttribute(k_row_fused<L2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          2 * (1 << L2) * (int)sizeof(u32));
 }
+
+template <int L2>
+void attr_rowsplit() {
+    const int smem = (1 << L2) * (int)sizeof(u32);
+    cudaFuncSetAttribute(k_row_fwd_g<L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_row_mul_f<L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+}
+
+const PassFn kRowG[15] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                          launch_row_g_t<6>, launch_row_g_t<7>, launch_row_g_t<8>, launch_row_g_t<9>,
+                          launch_row_g_t<10>, launch_row_g_t<11>, launch_row_g_t<12>, launch_row_g_t<13>,
+                          launch_row_g_t<14>};
+const PassFn kRowF[15] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                          launch_row_f_t<6>, launch_row_f_t<7>, launch_row_f_t<8>, launch_row_f_t<9>,
+                          launch_row_f_t<10>, launch_row_f_t<11>, launch_row_f_t<12>, launch_row_f_t<13>,
+                          launch_row_f_t<14>};
 
 int ceil_log2(long long s) {
     int k = 0;
@@ -110,6 +136,8 @@ void ensure_kernel_attrs() {
         attr_col<6>(); attr_col<7>(); attr_col<8>(); attr_col<9>(); attr_col<10>();
         attr_row<6>(); attr_row<7>(); attr_row<8>(); attr_row<9>(); attr_row<10>();
         attr_row<11>(); attr_row<12>(); attr_row<13>(); attr_row<14>();
+        attr_rowsplit<6>(); attr_rowsplit<7>(); attr_rowsplit<8>(); attr_rowsplit<9>(); attr_rowsplit<10>();
+        attr_rowsplit<11>(); attr_rowsplit<12>(); attr_rowsplit<13>(); attr_rowsplit<14>();
     });
 }
 
@@ -166,6 +194,8 @@ int large_args(const PrimeCtx& pc, u32 root_n, int logn, int l2, int dev, LargeA
     a->l1 = l1;
     a->l2 = l2;
     a->colpl = col_plan(l1);
+    const char* rf = getenv("CUMODP_ROW_FUSED");
+    a->row_fused = rf && rf[0] == '1';
     return OK;
 }
 
@@ -177,6 +207,10 @@ static const char* kColFwdName[11] = {"", "col_fwd_1", "col_fwd_2", "col_fwd_3",
     "col_fwd_6", "col_fwd_7", "col_fwd_8", "col_fwd_9", "col_fwd_10"};
 static const char* kColInvName[11] = {"", "col_inv_1", "col_inv_2", "col_inv_3", "col_inv_4", "col_inv_5",
     "col_inv_6", "col_inv_7", "col_inv_8", "col_inv_9", "col_inv_10"};
+static const char* kRowGName[15] = {"", "", "", "", "", "", "row_fwd_g_6", "row_fwd_g_7", "row_fwd_g_8",
+    "row_fwd_g_9", "row_fwd_g_10", "row_fwd_g_11", "row_fwd_g_12", "row_fwd_g_13", "row_fwd_g_14"};
+static const char* kRowFName[15] = {"", "", "", "", "", "", "row_mul_f_6", "row_mul_f_7", "row_mul_f_8",
+    "row_mul_f_9", "row_mul_f_10", "row_mul_f_11", "row_mul_f_12", "row_mul_f_13", "row_mul_f_14"};
 static const char* kRowName[15] = {"", "", "", "", "", "", "row_fused_6", "row_fused_7", "row_fused_8",
     "row_fused_9", "row_fused_10", "row_fused_11", "row_fused_12", "row_fused_13", "row_fused_14"};
 
@@ -194,9 +228,18 @@ void launch_large(const LargeArgs& a, int njobs, cudaStream_t st) {
     bool tr = pass_timing_begin(st, &e0);
     kColFwd[a.l1](a, dim3(n2 / 32, 2, njobs), st);
     if (tr) pass_timing_end(st, kColFwdName[a.l1], e0);
-    tr = pass_timing_begin(st, &e0);
-    kRow[a.l2](a, dim3(n1, njobs, 1), st);
-    if (tr) pass_timing_end(st, kRowName[a.l2], e0);
+    if (a.row_fused) {
+        tr = pass_timing_begin(st, &e0);
+        kRow[a.l2](a, dim3(n1, njobs, 1), st);
+        if (tr) pass_timing_end(st, kRowName[a.l2], e0);
+    } else {
+        tr = pass_timing_begin(st, &e0);
+        kRowG[a.l2](a, dim3(n1, njobs, 1), st);
+        if (tr) pass_timing_end(st, kRowGName[a.l2], e0);
+        tr = pass_timing_begin(st, &e0);
+        kRowF[a.l2](a, dim3(n1, njobs, 1), st);
+        if (tr) pass_timing_end(st, kRowFName[a.l2], e0);
+    }
     tr = pass_timing_begin(st, &e0);
     kColInv[a.l1](a, dim3(n2 / 32, 1, njobs), st);
     if (tr) pass_timing_end(st, kColInvName[a.l1], e0);

@@ -144,6 +144,38 @@ __device__ __forceinline__ void small_inv_levels(u32* sm, const Ctx& A) {
     }
 }
 
+// Single-operand forward level LEV (not the last) on a row in shared memory.
+template <int LOGL, int LEV, int T>
+__device__ __forceinline__ void fwd1_level(u32* sm, const PrimeK& pk, const Tw* __restrict__ tw) {
+    using LV = SmallLevel<LOGL, LEV>;
+    constexpr int L = 1 << LOGL, R = LV::R, TB = LV::TB, B = LV::B;
+    const u32 p = pk.p, p2 = pk.p2;
+    for (int id = threadIdx.x; id < L / R; id += T) {
+        const int blk = id / TB, o = id % TB;
+        const int base = blk * B + o;
+        u32 x[R];
+#pragma unroll
+        for (int m = 0; m < R; ++m) x[m] = sm[swz(base + TB * m)];
+        dif_regs<R, true>(x, pk.rc.f, p, p2);
+        Tw t[R];
+        load_tw<R>(t, tw + LV::TWOFF + o * R);
+#pragma unroll
+        for (int j = 1; j < R; ++j) x[j] = mul_shoup(x[j], t[j].w, t[j].wq, p);
+#pragma unroll
+        for (int m = 0; m < R; ++m) sm[swz(base + TB * m)] = x[m];
+    }
+}
+
+template <int LOGL, int LEV, int T>
+__device__ __forceinline__ void fwd1_levels(u32* sm, const PrimeK& pk, const Tw* __restrict__ tw) {
+    constexpr LevelPlan PL = row_plan(LOGL);
+    if constexpr (LEV + 1 < PL.nlev) {
+        fwd1_level<LOGL, LEV, T>(sm, pk, tw);
+        __syncthreads();
+        fwd1_levels<LOGL, LEV + 1, T>(sm, pk, tw);
+    }
+}
+
 __device__ __forceinline__ void load_row32(u32 (&x)[32], const u32* sm, int base) {
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
