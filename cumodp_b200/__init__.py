@@ -31,7 +31,7 @@ FFT_SIZE_TOO_LARGE = 0x202
 FFT_SIZE_TOO_SMALL = 0x203
 OUT_OF_MEMORY = 0x401
 
-# Fourier primes used by the reference (two-convolution).
+# Fourier primes used by the reference (its benchmark configurations, two-convolution).
 P_469762049 = 469762049   # 7 * 2^26 + 1
 P_754974721 = 754974721   # 45 * 2^24 + 1
 TWOCONV_PRIMES = (962592769, 950009857, 940572673)
@@ -102,6 +102,9 @@ def _lib():
         L.cumodp_fft_uni_dev.restype = C.c_int
         L.cumodp_fft_uni_dev.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int,
                                          C.c_void_p]
+        L.cumodp_list_fft_dev.restype = C.c_int
+        L.cumodp_list_fft_dev.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int,
+                                          C.c_void_p]
         L.cumodp_select_device.restype = C.c_int
         L.cumodp_select_device.argtypes = [C.c_int]
         L.cumodp_trace_passes.restype = None
@@ -287,6 +290,11 @@ def fft_uni_dev(x_ptr: int, k: int, w: int, p: int, inverse: bool = False, strea
     """In-place natural-order transform of 2^k device words (``cumodp_fft_uni_dev``)."""
     _check(_lib().cumodp_fft_uni_dev(x_ptr, 1 << k, k, w, p, int(inverse), stream or None),
            "cumodp_fft_uni_dev")
+
+
+def list_fft_dev(x_ptr: int, m: int, k: int, w: int, p: int, inverse: bool = False, stream: int = 0) -> None:
+    """m natural-order transforms of 2^k device words each, in place (``cumodp_list_fft_dev``)."""
+    _check(_lib().cumodp_list_fft_dev(x_ptr, m, k, w, p, int(inverse), stream or None), "cumodp_list_fft_dev")
 
 
 def select_device(dev: int) -> None:

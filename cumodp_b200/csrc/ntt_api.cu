@@ -32,6 +32,7 @@ struct RowNttArgs {
     const u32* src;                 // row slot s at src + s * n2
     u32* dst;                       // natural row k1 at dst + k1 * n2
     Tw scale;                       // applied to every output
+    int rows_in_place;              // 1: independent rows, row s written to dst row s
 };
 
 __device__ __forceinline__ u32 seed_mont_at(const u32* __restrict__ seeds, int nlo, u32 e, u32 p, u32 pinv) {
@@ -68,6 +69,7 @@ __global__ void __launch_bounds__(small_threads(L2), 1) k_row_ntt(const __grid_c
 
     const u32 s = blockIdx.x;
     const u32 k1 = A.l1 ? col_slot_to_k1(s, A.colpl, A.l1) : 0u;
+    const u32 out_row = A.rows_in_place ? s : k1;
     const bool twid = A.seeds != nullptr;
     const u32 nmask = (1u << (A.l1 + L2)) - 1;
     const u32 p = A.pk.p, p2 = A.pk.p2, pinv = A.pk.pinv_neg;
@@ -110,7 +112,7 @@ __global__ void __launch_bounds__(small_threads(L2), 1) k_row_ntt(const __grid_c
         }
     }
     __syncthreads();
-    u32* out = A.dst + (size_t)k1 * n2;
+    u32* out = A.dst + (size_t)out_row * n2;
     for (int i = threadIdx.x * 4; i < n2; i += T * 4) {
         uint4 v = *reinterpret_cast<const uint4*>(sm + n2 + swz(i));
         *reinterpret_cast<uint4*>(out + i) = v;
@@ -128,10 +130,13 @@ __global__ void k_transpose(const u32* __restrict__ in, u32* __restrict__ out, i
         out[(size_t)(c0 + y) * rows + r0 + threadIdx.x] = t[threadIdx.x][y];
 }
 
-// Direct DFT for n <= 32 (one CTA of n threads): out[j] = scale * sum x_i w^(ij).
+// Direct DFT for n <= 32, one CTA of n threads per vector (vector b at
+// offset b * n): out[j] = scale * sum x_i w^(ij).
 __global__ void k_tiny_dft(const u32* __restrict__ x, u32* __restrict__ y, int n, u32 w, u32 p, u32 scale) {
     __shared__ u32 xs[32], pw[32];
     const int j = threadIdx.x;
+    x += (size_t)blockIdx.x * n;
+    y += (size_t)blockIdx.x * n;
     xs[j] = x[j] % p;
     u32 t = 1;
     for (int i = 0; i < j; ++i) t = (u32)(((u64)t * w) % p);
@@ -275,6 +280,47 @@ int ntt_natural_dev(const u32* x_in, u32* x_out, int k, u32 w, u32 p, bool inver
     return cuda_err(cudaGetLastError());
 }
 
+// m independent natural-order transforms of length 2^k (row i at x + i 2^k),
+// in place: the list transform I_m (x) DFT_n.
+int list_ntt_dev(u32* x, long long m, int k, u32 w, u32 p, bool inverse, cudaStream_t st) {
+    int err = OK;
+    const PrimeCtx* pc = prime_ctx(p, &err);
+    if (!pc) return err;
+    if (m < 0 || k < 0) return ASSUMPTION_ERROR;
+    if (m == 0) return OK;
+    if (k > pc->info.two_adic) return FFT_SIZE_TOO_LARGE;
+    if (!root_has_order(w, k, p)) return ASSUMPTION_ERROR;
+    const u32 root = inverse ? inv_of(w, p) : w;
+    const u32 sc = inverse ? inv_of((u32)((1ull << k) % p), p) : 1u;
+    if (k <= 5) {
+        for (long long r0 = 0; r0 < m; r0 += 65535) {
+            const unsigned nb = (unsigned)std::min<long long>(65535, m - r0);
+            k_tiny_dft<<<nb, 1 << k, 0, st>>>(x + (r0 << k), x + (r0 << k), 1 << k, root, p, sc);
+        }
+        return cuda_err(cudaGetLastError());
+    }
+    if (k <= kMaxSmallLog) {
+        const int dev = current_device();
+        const Tw* twr = row_tables(dev, p, root, k, &err);
+        if (!twr) return err;
+        RowNttArgs A;
+        memset(&A, 0, sizeof(A));
+        A.pk = make_prime_k_for(pc->info, root, k);
+        A.twr = twr;
+        A.scale = tw_of(sc, p);
+        A.rows_in_place = 1;
+        for (long long r0 = 0; r0 < m; r0 += (1ll << 30)) {
+            A.src = x + (r0 << k);
+            A.dst = x + (r0 << k);
+            kRowNtt[k](A, (int)std::min<long long>(1ll << 30, m - r0), st);
+        }
+        return cuda_err(cudaGetLastError());
+    }
+    for (long long r = 0; r < m; ++r)
+        if ((err = ntt_natural_dev(x + (r << k), x + (r << k), k, w, p, inverse, st)) != OK) return err;
+    return OK;
+}
+
 // 2-D DFT of a row-major 2^em x 2^en array, in place.
 int bivariate_dev(u32* x, int em, u32 wm, int en, u32 wn, u32 p, bool inverse, cudaStream_t st) {
     int err = OK;
@@ -383,6 +429,20 @@ cumodp_err cumodp_fft_uni_dev(sfixn* X, sfixn n, sfixn k, sfixn w, sfixn p, int 
     std::lock_guard<std::mutex> g(lib_mutex());
     cudaStream_t st = stream ? (cudaStream_t)stream : lib_stream(current_device());
     int e = ntt_natural_dev((const u32*)X, (u32*)X, k, (u32)w, (u32)p, inverse != 0, st);
+    if (e == OK && !stream) e = cuda_err(cudaStreamSynchronize(st));
+    return (cumodp_err)e;
+}
+
+cumodp_err cumodp_list_fft_dev(sfixn* X, sfixn m, sfixn k, sfixn w, sfixn p, int inverse, void* stream) {
+    int cnt = 0;
+    if (cudaGetDeviceCount(&cnt) != cudaSuccess || cnt == 0) {
+        cudaGetLastError();
+        return CUMODP_NO_CUDA_DEVICE;
+    }
+    if (!X || m < 0 || k < 0 || k > 30 || p <= 0) return CUMODP_ASSUMPTION_ERROR;
+    std::lock_guard<std::mutex> g(lib_mutex());
+    cudaStream_t st = stream ? (cudaStream_t)stream : lib_stream(current_device());
+    int e = list_ntt_dev((u32*)X, m, k, (u32)w, (u32)p, inverse != 0, st);
     if (e == OK && !stream) e = cuda_err(cudaStreamSynchronize(st));
     return (cumodp_err)e;
 }

@@ -6,9 +6,12 @@
 // device "lanes" (stream + grow-only device/pinned buffers).  A batcher
 // thread admits requests in arrival order while the device-memory budget
 // allows, groups the admitted ones by (kind, prime) and dispatches each
-// group to a free lane as one batch: one host->device copy of all operands,
-// the batched product kernels (or the exact-product pipeline), one
-// device->host copy, an event.  Requests that arrive while earlier batches
+// group to a free lane as one batch: asynchronous host->device copies of
+// the operands (each request's operands were copied once, by the submitting
+// thread, into a pinned slab), the batched product kernels (or the
+// exact-product pipeline), asynchronous device->host copies into each
+// request's pinned result slab, an event.  The waiting thread copies its
+// result out of the slab.  Requests that arrive while earlier batches
 // are on the GPU are admitted into the next batch at once, so batches from
 // different lanes overlap on the device.  A completion thread waits on lane
 // events, scatters results into the callers' buffers, releases the memory
@@ -37,13 +40,74 @@ double now_us() {
     return std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+// Pinned host slabs in power-of-two size classes, recycled: allocating pinned
+// memory is slow, so slabs outlive requests.
+struct PinnedPool {
+    std::mutex m;
+    std::vector<std::vector<void*>> free_by_class = std::vector<std::vector<void*>>(40);
+    size_t held = 0;
+    static int cls(size_t bytes) {
+        int c = 12;
+        while (((size_t)1 << c) < bytes) ++c;
+        return c;
+    }
+    void* get(size_t bytes) {
+        const int c = cls(bytes);
+        {
+            std::lock_guard<std::mutex> g(m);
+            if (!free_by_class[c].empty()) {
+                void* p = free_by_class[c].back();
+                free_by_class[c].pop_back();
+                return p;
+            }
+        }
+        void* p = nullptr;
+        if (cudaHostAlloc(&p, (size_t)1 << c, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        std::lock_guard<std::mutex> g(m);
+        held += (size_t)1 << c;
+        return p;
+    }
+    // Allocates `count` slabs of each class in [lo, hi] up front so that
+    // serving does not call cudaHostAlloc (slow, and it synchronises with
+    // the device) on its hot path.
+    void warm(int lo, int hi, size_t budget) {
+        for (int c = lo; c <= hi; ++c) {
+            const int count = c <= 18 ? 16 : (c <= 21 ? 8 : 4);
+            for (int k = 0; k < count && ((size_t)1 << c) <= budget; ++k) {
+                void* p = nullptr;
+                if (cudaHostAlloc(&p, (size_t)1 << c, cudaHostAllocDefault) != cudaSuccess) {
+                    cudaGetLastError();
+                    return;
+                }
+                std::lock_guard<std::mutex> g(m);
+                free_by_class[c].push_back(p);
+                held += (size_t)1 << c;
+                budget -= (size_t)1 << c;
+            }
+        }
+    }
+    void put(void* p, size_t bytes) {
+        if (!p) return;
+        std::lock_guard<std::mutex> g(m);
+        free_by_class[cls(bytes)].push_back(p);
+    }
+    ~PinnedPool() {
+        for (auto& v : free_by_class)
+            for (void* p : v) cudaFreeHost(p);
+    }
+};
+
 struct Req {
     long long id;
     int kind;  // 0: modular product, 1: exact int64 product
     u32 p;
     long long la, lb;
-    std::vector<u32> A, B;          // kind 0
-    std::vector<long long> A64, B64;  // kind 1
+    void* in = nullptr;   // pinned: operands (kind 0: u32 A then B; kind 1: int64 A then B)
+    void* res = nullptr;  // pinned: result (kind 0: la+lb-1 u32; kind 1: 2(la+lb-1) int64)
+    size_t in_bytes = 0, res_bytes = 0;
     int bw = 1;
     void* out;
     size_t bytes;
@@ -103,10 +167,8 @@ struct Lane {
     cudaEvent_t ev = nullptr;
     DevBuf<u32> din, dout, ws;
     DevBuf<unsigned char> djobs;
-    PinBuf<u32> hin, hout;
     PinBuf<unsigned char> hjobs;
     std::vector<Req*> reqs;
-    std::vector<size_t> out_off;  // word offset of each request's result in hout
     int status = OK;
     bool busy = false;
     long long seq = 0;
@@ -122,6 +184,7 @@ struct Server {
     std::deque<Req*> pending;
     std::unordered_map<long long, Req*> reqs;
     std::vector<Lane> lanes;
+    PinnedPool pool;
     std::deque<int> dispatched;  // lane indices in dispatch order
     size_t inflight = 0;
     long long next_id = 1, lane_seq = 0;
@@ -183,36 +246,31 @@ int run_batch(Server& S, Lane& L) {
             nin += la[i] + lb[i];
             nout += lh[i];
         }
-        if ((err = L.din.ensure(nin)) || (err = L.dout.ensure(nout)) || (err = L.hin.ensure(nin)) ||
-            (err = L.hout.ensure(nout)))
-            return err;
+        if ((err = L.din.ensure(nin)) || (err = L.dout.ensure(nout))) return err;
         const size_t wsw = direct_ws_words(cnt, la.data(), lb.data());
         const size_t jb = direct_job_bytes(cnt);
         if ((err = L.ws.ensure(wsw + 1)) || (err = L.djobs.ensure(jb)) || (err = L.hjobs.ensure(jb))) return err;
         std::vector<const u32*> pa(cnt), pb(cnt);
         std::vector<u32*> ph(cnt);
-        L.out_off.assign(cnt, 0);
         size_t o = 0, q = 0;
         for (int i = 0; i < cnt; ++i) {
             Req* r = L.reqs[i];
-            memcpy(L.hin.p + o, r->A.data(), r->la * 4);
+            cudaError_t ce = cudaMemcpyAsync(L.din.p + o, r->in, (r->la + r->lb) * 4, cudaMemcpyHostToDevice, L.st);
+            if (ce != cudaSuccess) return cuda_err(ce);
             pa[i] = L.din.p + o;
-            o += r->la;
-            memcpy(L.hin.p + o, r->B.data(), r->lb * 4);
-            pb[i] = L.din.p + o;
-            o += r->lb;
+            pb[i] = L.din.p + o + r->la;
+            o += r->la + r->lb;
             ph[i] = L.dout.p + q;
-            L.out_off[i] = q;
             q += lh[i];
         }
-        cudaError_t ce = cudaMemcpyAsync(L.din.p, L.hin.p, nin * 4, cudaMemcpyHostToDevice, L.st);
-        if (ce != cudaSuccess) return cuda_err(ce);
         // no autotuning on the serving path: cached or default splits only
         err = direct_batch(cnt, pa.data(), la.data(), pb.data(), lb.data(), ph.data(), lh.data(), p, L.ws.p,
                            L.djobs.p, L.hjobs.p, L.st, false);
         if (err != OK) return err;
-        ce = cudaMemcpyAsync(L.hout.p, L.dout.p, nout * 4, cudaMemcpyDeviceToHost, L.st);
-        if (ce != cudaSuccess) return cuda_err(ce);
+        for (int i = 0; i < cnt; ++i) {
+            cudaError_t ce = cudaMemcpyAsync(L.reqs[i]->res, ph[i], lh[i] * 4, cudaMemcpyDeviceToHost, L.st);
+            if (ce != cudaSuccess) return cuda_err(ce);
+        }
     } else {
         // exact products, one after another on the lane's stream
         size_t nin = 0, nout = 0, evw = 0, wsw = 0, jbb = 0;
@@ -226,21 +284,16 @@ int run_batch(Server& S, Lane& L) {
             jbb += j;
         }
         // int64 data travels through the u32 buffers (two words per value)
-        if ((err = L.din.ensure(2 * nin)) || (err = L.dout.ensure(2 * nout + evw)) || (err = L.hin.ensure(2 * nin)) ||
-            (err = L.hout.ensure(2 * nout)) || (err = L.ws.ensure(wsw + 1)) || (err = L.djobs.ensure(jbb)) ||
-            (err = L.hjobs.ensure(jbb)))
+        if ((err = L.din.ensure(2 * nin)) || (err = L.dout.ensure(2 * nout + evw)) || (err = L.ws.ensure(wsw + 1)) ||
+            (err = L.djobs.ensure(jbb)) || (err = L.hjobs.ensure(jbb)))
             return err;
-        L.out_off.assign(cnt, 0);
         size_t o = 0, q = 0, jo = 0;
         u32* eval = L.dout.p + 2 * nout;
-        long long* hin64 = (long long*)L.hin.p;
         long long* din64 = (long long*)L.din.p;
         long long* dout64 = (long long*)L.dout.p;
         for (int i = 0; i < cnt; ++i) {
             Req* r = L.reqs[i];
-            memcpy(hin64 + o, r->A64.data(), r->la * 8);
-            memcpy(hin64 + o + r->la, r->B64.data(), r->lb * 8);
-            cudaError_t ce = cudaMemcpyAsync(din64 + o, hin64 + o, (r->la + r->lb) * 8, cudaMemcpyHostToDevice, L.st);
+            cudaError_t ce = cudaMemcpyAsync(din64 + o, r->in, (r->la + r->lb) * 8, cudaMemcpyHostToDevice, L.st);
             if (ce != cudaSuccess) return cuda_err(ce);
             TwoConvBufs B{eval, L.ws.p, L.djobs.p + jo, L.hjobs.p + jo};
             size_t e, w, j;
@@ -248,13 +301,12 @@ int run_batch(Server& S, Lane& L) {
             err = twoconv_mul_dev(din64 + o, r->la, din64 + o + r->la, r->lb, dout64 + 2 * q, r->bw, r->bw, false,
                                   L.st, nullptr, &B);
             if (err != OK) return err;
-            L.out_off[i] = 4 * q;  // (lo, hi) int64 pairs, in u32 words
+            ce = cudaMemcpyAsync(r->res, dout64 + 2 * q, (r->la + r->lb - 1) * 16, cudaMemcpyDeviceToHost, L.st);
+            if (ce != cudaSuccess) return cuda_err(ce);
             o += r->la + r->lb;
             q += r->la + r->lb - 1;
             jo += j;
         }
-        cudaError_t ce = cudaMemcpyAsync(L.hout.p, L.dout.p, nout * 8, cudaMemcpyDeviceToHost, L.st);
-        if (ce != cudaSuccess) return cuda_err(ce);
     }
     return cuda_err(cudaEventRecord(L.ev, L.st));
 }
@@ -338,13 +390,7 @@ void completer_loop(Server* Sp) {
         cudaError_t ce = cudaEventSynchronize(L.ev);
         int st = L.status != OK ? L.status : cuda_err(ce);
         if (st == OK) st = cuda_err(cudaGetLastError());
-        if (st == OK) {
-            for (size_t i = 0; i < L.reqs.size(); ++i) {
-                Req* r = L.reqs[i];
-                const size_t words = r->kind == 0 ? (size_t)(r->la + r->lb - 1) : (size_t)2 * 2 * (r->la + r->lb - 1);
-                memcpy(r->out, L.hout.p + L.out_off[i], words * 4);
-            }
-        } else {
+        if (st != OK) {
             // contain the failure: drain and re-create the lane
             cudaStreamSynchronize(L.st);
             cudaGetLastError();
@@ -356,10 +402,8 @@ void completer_loop(Server* Sp) {
             freed += r->bytes;
             finish(S, r, st == FFT_SIZE_TOO_LARGE || st == OK || st == ASSUMPTION_ERROR ||
                                  st == OUT_OF_MEMORY ? st : FFT_ERROR);
-            r->A.clear(); r->A.shrink_to_fit();
-            r->B.clear(); r->B.shrink_to_fit();
-            r->A64.clear(); r->A64.shrink_to_fit();
-            r->B64.clear(); r->B64.shrink_to_fit();
+            S.pool.put(r->in, r->in_bytes);  // the operands' copy has completed
+            r->in = nullptr;
         }
         S.inflight -= std::min(S.inflight, freed);
         L.reqs.clear();
@@ -428,6 +472,8 @@ cumodp_server* cumodp_server_create(const cumodp_server_config* cfg) {
     Server* S = new Server(c);
     S->lanes.resize(c.lanes);
     for (Lane& L : S->lanes) recreate_lane(L);
+    // pinned slabs for operands and results of up to 2^21 words, at most 1 GiB
+    S->pool.warm(12, 23, 1ull << 30);
     S->batcher = std::thread(batcher_loop, S);
     S->completer = std::thread(completer_loop, S);
     return (cumodp_server*)S;
@@ -448,8 +494,16 @@ long long cumodp_server_submit_mod(cumodp_server* h, sfixn p, sfixn df, const sf
     if (!pc) r->status = err;
     else if (product_logn(r->la, r->lb) > std::min(pc->info.two_adic, kMaxLog)) r->status = FFT_SIZE_TOO_LARGE;
     else {
-        r->A.assign((const u32*)F, (const u32*)F + r->la);
-        r->B.assign((const u32*)G, (const u32*)G + r->lb);
+        r->in_bytes = (size_t)(r->la + r->lb) * 4;
+        r->res_bytes = (size_t)(r->la + r->lb - 1) * 4;
+        r->in = S->pool.get(r->in_bytes);
+        r->res = S->pool.get(r->res_bytes);
+        if (!r->in || !r->res) {
+            r->status = OUT_OF_MEMORY;
+        } else {
+            memcpy(r->in, F, (size_t)r->la * 4);
+            memcpy((u32*)r->in + r->la, G, (size_t)r->lb * 4);
+        }
     }
     return submit(*S, r);
 }
@@ -472,8 +526,16 @@ long long cumodp_server_submit_i64(cumodp_server* h, long long na, const int64_t
     const int e = na + nb - 1 > (1ll << 21) ? FFT_SIZE_TOO_LARGE : twoconv_plan(r->bw, r->bw, na, nb, false, &pl);
     if (e != OK) r->status = e;
     else {
-        r->A64.assign((const long long*)a, (const long long*)a + na);
-        r->B64.assign((const long long*)b, (const long long*)b + nb);
+        r->in_bytes = (size_t)(na + nb) * 8;
+        r->res_bytes = (size_t)(na + nb - 1) * 16;
+        r->in = S->pool.get(r->in_bytes);
+        r->res = S->pool.get(r->res_bytes);
+        if (!r->in || !r->res) {
+            r->status = OUT_OF_MEMORY;
+        } else {
+            memcpy(r->in, a, (size_t)na * 8);
+            memcpy((long long*)r->in + na, b, (size_t)nb * 8);
+        }
     }
     return submit(*S, r);
 }
@@ -499,6 +561,10 @@ int cumodp_server_wait(cumodp_server* h, long long id, long long timeout_us) {
     else if (!S->cv_done.wait_for(lk, std::chrono::microseconds(timeout_us), pred)) return -2;
     const int st = r->status;
     S->reqs.erase(it);
+    lk.unlock();
+    if (st == OK) memcpy(r->out, r->res, r->res_bytes);
+    S->pool.put(r->in, r->in_bytes);
+    S->pool.put(r->res, r->res_bytes);
     delete r;
     return st;
 }
@@ -555,11 +621,15 @@ void cumodp_server_destroy(cumodp_server* h) {
     for (Lane& L : S->lanes) {
         if (L.st) cudaStreamSynchronize(L.st);
         L.din.release(); L.dout.release(); L.ws.release(); L.djobs.release();
-        L.hin.release(); L.hout.release(); L.hjobs.release();
+        L.hjobs.release();
         if (L.st) cudaStreamDestroy(L.st);
         if (L.ev) cudaEventDestroy(L.ev);
     }
-    for (auto& kv : S->reqs) delete kv.second;
+    for (auto& kv : S->reqs) {
+        S->pool.put(kv.second->in, kv.second->in_bytes);
+        S->pool.put(kv.second->res, kv.second->res_bytes);
+        delete kv.second;
+    }
     delete S;
 }
 

@@ -201,9 +201,11 @@ cumodp_err cumodp_twoconv_plan(int bit_width_a, int bit_width_b, long long na, l
  * them in arrival order while the device-memory budget allows, groups them
  * by (kind, prime) and runs each group as one batch on a free lane (stream
  * plus device buffers); batches on different lanes overlap on the GPU, and
- * requests arriving meanwhile join the next batch.  Results are written to
- * the caller's output buffer, which must stay valid until the request is
- * waited for.  No counterpart in the reference. */
+ * requests arriving meanwhile join the next batch.  Operands are copied at
+ * submission into pinned memory owned by the server; the result is copied
+ * into the caller's output buffer by cumodp_server_wait, which must be
+ * called once per request (the buffer must stay valid until then).  No
+ * counterpart in the reference. */
 typedef struct cumodp_server cumodp_server;
 typedef struct {
     int device;              /* CUDA device ordinal */
@@ -241,6 +243,16 @@ void cumodp_server_destroy(cumodp_server *s);
  * the library's stream, then synchronised): forward as cumodp_fft_uni, or
  * the inverse of it when `inverse` is nonzero.  X is a DEVICE pointer. */
 cumodp_err cumodp_fft_uni_dev(sfixn *X, sfixn n, sfixn k, sfixn w, sfixn p, int inverse, void *stream);
+
+/* Addition.  The list transform I_m (x) DFT_n: m independent natural-order
+ * transforms of length n = 2^k of the DEVICE array X (row i at X + i n), in
+ * place, root w (inverse: w^-1 and scaling by n^-1).  Counterpart of the
+ * reference's C++ list_stockham_dev (src/list_stockham.cu:595-665, declared
+ * in include/list_stockham.h:48-49; include/list_stockham_b200.h here gives
+ * the same C++ signatures) without its grid bug for m * n / 128 > 2^15 and
+ * without its __constant__ globals.  stream: 0 = library stream, then
+ * synchronised. */
+cumodp_err cumodp_list_fft_dev(sfixn *X, sfixn m, sfixn k, sfixn w, sfixn p, int inverse, void *stream);
 
 /* Addition.  Makes `dev` the current device of the calling thread for the
  * library's own CUDA runtime (one process per GPU). */

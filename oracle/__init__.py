@@ -24,6 +24,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libmodpn_ref.so")
 MODPN_GPU_SO = os.path.join(HERE, "_ref", "libmodpn_gpu.so")
+REF_GPU_SO = os.path.join(HERE, "_ref", "libcumodp_refgpu.so")
 
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
@@ -37,6 +38,7 @@ def build(ref: bool = False) -> None:
     if ref:
         subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
         subprocess.check_call(["make", "-s", "-C", HERE, "modpn_gpu"])
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref_gpu"])
 
 
 _lib = None
@@ -244,6 +246,36 @@ def modpn_gpu_polymul(a: np.ndarray, b: np.ndarray, p: int) -> np.ndarray:
     h = np.empty(len(a) + len(b) - 1, dtype=np.int32)
     if _mg.modpn_gpu_fftmul(len(a) - 1, a, len(b) - 1, b, h, p) != 0:
         raise RuntimeError("modpn prime error")
+    return h.view(np.uint32)
+
+
+def ref_gpu_available() -> bool:
+    return os.path.exists(REF_GPU_SO)
+
+
+_rg = None
+
+
+def ref_gpu_polymul(a: np.ndarray, b: np.ndarray, p: int) -> np.ndarray:
+    """The reference's own GPU product (stockham_poly_mul_host, src/stockham.cu:562-611).
+
+    Runs the reference as shipped (radix-2 Stockham, synchronised launches,
+    per-call allocation).  Transform sizes below 256 are refused by the
+    reference itself (it returns with H untouched), so callers keep to
+    len(a) + len(b) - 1 > 128.
+    """
+    global _rg
+    if _rg is None:
+        _rg = C.CDLL(REF_GPU_SO)
+        _rg.ref_gpu_fftmul.restype = C.c_int
+        _rg.ref_gpu_fftmul.argtypes = [C.c_int, _i32p, C.c_int, _i32p, C.c_int, _i32p, C.c_int]
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.uint32).view(np.int32))
+    b = np.ascontiguousarray(np.asarray(b, dtype=np.uint32).view(np.int32))
+    dh = len(a) + len(b) - 2
+    h = np.zeros(dh + 1, dtype=np.int32)
+    rc = _rg.ref_gpu_fftmul(dh, h, len(a) - 1, a, len(b) - 1, b, p)
+    if rc != 0:
+        raise RuntimeError(f"reference GPU product failed: CUDA error {rc}")
     return h.view(np.uint32)
 
 

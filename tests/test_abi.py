@@ -19,8 +19,10 @@ def declared_functions():
             name = m.group(1)
             prefix = src[max(0, m.start() - 80):m.start()]
             # a declaration: the name follows a type at the start of a statement
+            stmt = re.split(r"[;{}]", prefix)[-1]
+            # inline C++ forwarders (list_stockham_b200.h) are not exports
             if re.search(r"(^|[;}\n])\s*(const\s+)?[A-Za-z_][A-Za-z0-9_ ]*[\s\*]+$", prefix) and \
-                    name not in ("if", "defined", "sizeof"):
+                    name not in ("if", "defined", "sizeof") and not re.search(r"\binline\b", stmt):
                 names.add(name)
     return sorted(names)
 
@@ -59,3 +61,26 @@ def test_modpn_links_against_this_library():
     assert "libcumodp.so" in out
     lib = ctypes.CDLL(oracle.MODPN_GPU_SO)  # resolves cumodp_fftmul_uni / can_call_fftmul_uni
     assert hasattr(lib, "modpn_gpu_fftmul")
+
+
+def test_cpp_forwarding_header_compiles():
+    """include/list_stockham_b200.h gives the reference's C++ list_stockham_dev overloads."""
+    import shutil
+    import subprocess
+    import tempfile
+    gxx = shutil.which("g++")
+    cuda_inc = "/usr/local/cuda/include"
+    if not gxx or not os.path.isdir(cuda_inc):
+        pytest.skip("g++ or CUDA headers absent")
+    src = (
+        '#include "list_stockham_b200.h"\n'
+        "void use(sfixn* X, const sfixn* W) {\n"
+        "  cumodp_err a = list_stockham_dev(X, 4, 10, 3, 469762049);\n"
+        "  cumodp_err b = list_stockham_dev(X, 4, 10, W, 469762049);\n"
+        "  (void)a; (void)b;\n}\n")
+    with tempfile.TemporaryDirectory() as d:
+        f = os.path.join(d, "use.cpp")
+        open(f, "w").write(src)
+        r = subprocess.run([gxx, "-fsyntax-only", "-I", os.path.join(ROOT, "include"), "-I", cuda_inc, f],
+                           capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr

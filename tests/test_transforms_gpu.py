@@ -29,7 +29,7 @@ def test_fft_uni_matches_dft(cm, oracle_mod, k, p):
 
 
 def test_fft_uni_2_24_round_trip(cm, oracle_mod):
-    """The BASELINE-size transform: 2^24 points, forward vs oracle, then inverse round trip."""
+    """The headline-size transform: 2^24 points, forward vs oracle, then inverse round trip."""
     k = 24
     r = SplitMix64(0xC0DA0001)
     x = r.residues(1 << k, P0)
