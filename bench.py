@@ -509,74 +509,66 @@ def c1_latency(cm, torch, dev, stream):
             "batched_mulmods_per_s": round(R * 167936 / (batch_ms / 1000), 1), "batched_equals_single": same}
 
 
-def serving_c5(cm, rates=(1000, 10000, 100000), max_requests=4000, max_seconds=1.5, submitters=3):
+def serving_c5(cm, rates=(1000, 3000, 10000, 30000, 100000), max_requests=20000, max_seconds=2.0, threads=4):
     """Config 5: Poisson arrivals of mixed requests into the continuous-batching server.
 
     Degrees log-uniform in [2^5, 2^20]; prime uniform over {469762049,
     754974721, 962592769}; 20% exact int64 products (|c| <= 10^10, degrees
-    capped at 2^14 so the 127-bit bound holds).  `submitters` threads each
-    replay a Poisson stream of rate/submitters (the binding releases the GIL
-    inside the C calls, so submissions and waits run in parallel).  Requests
-    whose product exceeds the prime's 2-adic order (962592769 supports 2^21
-    points) are answered with CUMODP_FFT_SIZE_TOO_LARGE and counted as
-    rejected.  Latency = submission to result in the caller's buffer.
+    capped at 2^14 so the 127-bit bound holds).  The trace is replayed
+    open-loop by the library's native replay threads (cumodp_server_replay):
+    request i is submitted at its arrival time whatever happened before, and
+    its latency runs from the scheduled arrival to the result in a host
+    buffer.  Each rate replays min(max_requests, rate * max_seconds)
+    requests.  Requests whose product exceeds the prime's 2-adic order
+    (962592769 supports 2^21 points) are answered with
+    CUMODP_FFT_SIZE_TOO_LARGE and counted as rejected; requests shed by the
+    server's pinned host budget are counted as shed.
     """
-    import threading
-
     from cumodp_b200.workloads import SplitMix64, seed_for
     primes = (469762049, 754974721, 962592769)
     r = SplitMix64(seed_for(4))
     pool_u = r.residues(1 << 21, 469762049)        # operand slices come from these pools
     pool_i = r.int64_in(1 << 15, 10**10)
     out = {}
-    for rate in rates:
-        n = max_requests
-        gaps = -np.log(1.0 - r.uniform01(n)) / (rate / submitters)
-        da = r.log_uniform_int(n, 32, 1 << 20)
-        db = r.log_uniform_int(n, 32, 1 << 20)
-        kind = r.uniform01(n)
-        pidx = (r.next_u64(n) % np.uint64(3)).astype(int)
-        offs = (r.next_u64(2 * n) % np.uint64(1 << 20)).astype(np.int64)
-        codes = []
-        lock = threading.Lock()
-        with cm.Server(max_batch=256, batch_window_us=50, lanes=4) as srv:
-            t0 = time.perf_counter()
-
-            def submitter(k):
-                ids = []
-                t_next = t0
-                for i in range(k, n, submitters):
-                    t_next += gaps[i]
-                    while time.perf_counter() < t_next:
-                        pass
-                    if time.perf_counter() - t0 > max_seconds:
-                        break
-                    if kind[i] < 0.2:
-                        a = pool_i[offs[i] % (1 << 14):][: min(int(da[i]), 1 << 14) + 1]
-                        b = pool_i[offs[n + i] % (1 << 14):][: min(int(db[i]), 1 << 14) + 1]
-                        ids.append(srv.submit_i64(a, b)[0])
-                    else:
-                        a = pool_u[offs[i]:offs[i] + int(da[i]) + 1]
-                        b = pool_u[offs[n + i]:offs[n + i] + int(db[i]) + 1]
-                        ids.append(srv.submit_mod(a, b, primes[pidx[i]])[0])
-                got = [srv.wait(rid) for rid in ids]
-                with lock:
-                    codes.extend(got)
-
-            th = [threading.Thread(target=submitter, args=(k,)) for k in range(submitters)]
-            for t in th:
-                t.start()
-            for t in th:
-                t.join()
-            span = time.perf_counter() - t0
-            st = srv.stats()
-        ok = sum(1 for c in codes if c == 0)
-        out[str(rate)] = {"submitted": len(codes), "completed": ok,
-                          "rejected_size": sum(1 for c in codes if c == cm.FFT_SIZE_TOO_LARGE),
-                          "failed_other": sum(1 for c in codes if c not in (0, cm.FFT_SIZE_TOO_LARGE)),
-                          "p50_ms": round(st["p50_us"] / 1000, 3), "p99_ms": round(st["p99_us"] / 1000, 3),
-                          "products_per_s": round(ok / span, 1), "batches": st["batches"],
-                          "offered_per_s": round(len(codes) / span, 1), "submitter_threads": submitters}
+    with cm.Server(max_batch=256, batch_window_us=50, lanes=4) as srv:
+        # warm-up: tables for every prime and size class, lane buffers
+        warm = [(pool_u[:(1 << k) + 1], pool_u[:(1 << k) + 1], p) for p in primes for k in range(5, 21, 3)]
+        warm += [(pool_i[:(1 << k) + 1], pool_i[:(1 << k) + 1], None) for k in range(5, 15, 3)]
+        srv.replay(np.zeros(len(warm)), warm, threads=threads)
+        for rate in rates:
+            n = int(min(max_requests, rate * max_seconds))
+            arrival = np.cumsum(-np.log(1.0 - r.uniform01(n)) / rate) * 1e6
+            da = r.log_uniform_int(n, 32, 1 << 20)
+            db = r.log_uniform_int(n, 32, 1 << 20)
+            kind = r.uniform01(n)
+            pidx = (r.next_u64(n) % np.uint64(3)).astype(int)
+            offs = (r.next_u64(2 * n) % np.uint64(1 << 20)).astype(np.int64)
+            reqs = []
+            for i in range(n):
+                if kind[i] < 0.2:
+                    a = pool_i[offs[i] % (1 << 14):][: min(int(da[i]), 1 << 14) + 1]
+                    b = pool_i[offs[n + i] % (1 << 14):][: min(int(db[i]), 1 << 14) + 1]
+                    reqs.append((a, b, None))
+                else:
+                    reqs.append((pool_u[offs[i]:offs[i] + int(da[i]) + 1],
+                                 pool_u[offs[n + i]:offs[n + i] + int(db[i]) + 1], primes[pidx[i]]))
+            srv.reset_stats()
+            st, lat, span_us = srv.replay(arrival, reqs, threads=threads)
+            ok = st == 0
+            lat_ok = np.sort(lat[ok]) / 1000.0
+            pct = (lambda q: round(float(lat_ok[min(len(lat_ok) - 1, int(q * len(lat_ok)))]), 3)) \
+                if len(lat_ok) else (lambda q: None)
+            in_bytes = sum(a.nbytes + b.nbytes for a, b, _ in reqs)
+            out[str(rate)] = {"requests": n, "completed": int(ok.sum()),
+                              "rejected_size": int((st == cm.FFT_SIZE_TOO_LARGE).sum()),
+                              "shed": int((st == cm.OUT_OF_MEMORY).sum()),
+                              "failed_other": int((~ok & (st != cm.FFT_SIZE_TOO_LARGE) &
+                                                   (st != cm.OUT_OF_MEMORY)).sum()),
+                              "p50_ms": pct(0.5), "p99_ms": pct(0.99), "max_ms": pct(1.0),
+                              "products_per_s": round(ok.sum() / (span_us * 1e-6), 1),
+                              "offered_per_s": round(n / (arrival[-1] * 1e-6), 1),
+                              "operand_gb_per_s": round(in_bytes / (span_us * 1e3), 2),
+                              "batches": srv.stats()["batches"], "replay_threads": threads}
     return out
 
 

@@ -49,7 +49,8 @@ _LIB = None
 
 class ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int), ("memory_budget", C.c_size_t), ("max_batch", C.c_int),
-                ("batch_window_us", C.c_int), ("lanes", C.c_int), ("inject_fault_batch", C.c_int)]
+                ("batch_window_us", C.c_int), ("lanes", C.c_int), ("inject_fault_batch", C.c_int),
+                ("host_budget", C.c_size_t)]
 
 
 class ServerStats(C.Structure):
@@ -135,6 +136,10 @@ def _lib():
         L.cumodp_server_poll.argtypes = [C.c_void_p, C.c_longlong]
         L.cumodp_server_wait.restype = C.c_int
         L.cumodp_server_wait.argtypes = [C.c_void_p, C.c_longlong, C.c_longlong]
+        L.cumodp_server_replay.restype = C.c_int
+        L.cumodp_server_replay.argtypes = [C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                           C.c_void_p, C.POINTER(C.c_double)]
         L.cumodp_server_get_stats.restype = None
         L.cumodp_server_get_stats.argtypes = [C.c_void_p, C.POINTER(ServerStats)]
         L.cumodp_server_reset_stats.restype = None
@@ -364,11 +369,12 @@ class Server:
     """
 
     def __init__(self, device: int = 0, memory_budget: int = 0, max_batch: int = 512,
-                 batch_window_us: int = 50, lanes: int = 4, inject_fault_batch: int = 0):
+                 batch_window_us: int = 50, lanes: int = 4, inject_fault_batch: int = 0, host_budget: int = 0):
         cfg = ServerConfig()
         _lib().cumodp_server_default_config(C.byref(cfg))
         cfg.device, cfg.memory_budget, cfg.max_batch = device, memory_budget, max_batch
         cfg.batch_window_us, cfg.lanes, cfg.inject_fault_batch = batch_window_us, lanes, inject_fault_batch
+        cfg.host_budget = host_budget
         self._h = _lib().cumodp_server_create(C.byref(cfg))
         if not self._h:
             raise CumodpError(NO_CUDA_DEVICE, "cumodp_server_create")
@@ -395,6 +401,48 @@ class Server:
             raise CumodpError(ASSUMPTION_ERROR, "cumodp_server_submit_i64")
         self._outs[rid] = out
         return rid, out
+
+    def replay(self, arrival_us, requests, threads: int = 4, outputs=None):
+        """Open-loop replay of a timed trace by native threads (``cumodp_server_replay``).
+
+        requests[i] = (a, b, p): p = None for an exact int64 product, else the
+        prime of a product mod p (a, b residue arrays).  outputs[i] (optional)
+        receives the result; without it results are dropped.  Returns
+        (status array, latency array in microseconds from the scheduled
+        arrival to the result, span in microseconds).
+        """
+        n = len(requests)
+        arr = np.ascontiguousarray(arrival_us, dtype=np.float64)
+        assert len(arr) == n
+        kind = np.empty(n, np.int32)
+        pr = np.zeros(n, np.int32)
+        la = np.empty(n, np.int64)
+        lb = np.empty(n, np.int64)
+        keep = []
+        pa = (C.c_void_p * max(n, 1))()
+        pb = (C.c_void_p * max(n, 1))()
+        for i, (a, b, p) in enumerate(requests):
+            if p is None:
+                a = np.ascontiguousarray(a, dtype=np.int64)
+                b = np.ascontiguousarray(b, dtype=np.int64)
+                kind[i] = 1
+            else:
+                a, b = _as_i32(a), _as_i32(b)
+                kind[i], pr[i] = 0, p
+            keep += [a, b]
+            la[i], lb[i] = len(a), len(b)
+            pa[i], pb[i] = a.ctypes.data, b.ctypes.data
+        ph = None
+        if outputs is not None:
+            ph = (C.c_void_p * max(n, 1))(*[o.ctypes.data for o in outputs])
+        lat = np.zeros(n, np.float64)
+        st = np.zeros(n, np.int32)
+        span = C.c_double(0)
+        _check(_lib().cumodp_server_replay(self._h, n, arr.ctypes.data, kind.ctypes.data, pr.ctypes.data,
+                                           la.ctypes.data, lb.ctypes.data, pa, pb, ph, threads,
+                                           lat.ctypes.data, st.ctypes.data, C.byref(span)),
+               "cumodp_server_replay")
+        return st, lat, span.value
 
     def poll(self, rid: int) -> int:
         return int(_lib().cumodp_server_poll(self._h, rid))

@@ -475,7 +475,7 @@ __device__ __forceinline__ void row_level0_fwd(u32* sm, const LargeArgs& A, u32 
 }
 
 template <int L2>
-__global__ void __launch_bounds__(rowsplit_threads(L2), 2) k_row_fwd_g(const __grid_constant__ LargeArgs A) {
+__global__ void __launch_bounds__(rowsplit_threads(L2), rowsplit_ctas(L2)) k_row_fwd_g(const __grid_constant__ LargeArgs A) {
     constexpr int n2 = 1 << L2;
     constexpr int T = rowsplit_threads(L2);
     constexpr LevelPlan PL = row_plan(L2);
@@ -507,7 +507,7 @@ __global__ void __launch_bounds__(rowsplit_threads(L2), 2) k_row_fwd_g(const __g
 }
 
 template <int L2>
-__global__ void __launch_bounds__(rowsplit_threads(L2), 2) k_row_mul_f(const __grid_constant__ LargeArgs A) {
+__global__ void __launch_bounds__(rowsplit_threads(L2), rowsplit_ctas(L2)) k_row_mul_f(const __grid_constant__ LargeArgs A) {
     constexpr int n2 = 1 << L2;
     constexpr int T = rowsplit_threads(L2);
     constexpr LevelPlan PL = row_plan(L2);

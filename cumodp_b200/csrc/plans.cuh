@@ -68,5 +68,7 @@ __host__ __device__ constexpr int row_threads(int logl) { return logl == 14 ? 10
 // Threads of the split row kernels (one operand row per CTA, two CTAs per
 // SM): one per 32-word row of the last level.
 __host__ __device__ constexpr int rowsplit_threads(int logl) { return logl >= 10 ? (1 << (logl - 5)) : 32; }
+// Resident CTAs per SM the split row kernels are compiled for.
+__host__ __device__ constexpr int rowsplit_ctas(int logl) { return 2; }
 
 }  // namespace cmb

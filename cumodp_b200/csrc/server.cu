@@ -46,6 +46,8 @@ struct PinnedPool {
     std::mutex m;
     std::vector<std::vector<void*>> free_by_class = std::vector<std::vector<void*>>(40);
     size_t held = 0;
+    size_t in_use = 0;             // bytes of slabs handed out and not yet returned
+    size_t limit = ~(size_t)0;     // get() fails beyond this (load shedding)
     static int cls(size_t bytes) {
         int c = 12;
         while (((size_t)1 << c) < bytes) ++c;
@@ -53,8 +55,11 @@ struct PinnedPool {
     }
     void* get(size_t bytes) {
         const int c = cls(bytes);
+        const size_t sz = (size_t)1 << c;
         {
             std::lock_guard<std::mutex> g(m);
+            if (in_use + sz > limit) return nullptr;
+            in_use += sz;
             if (!free_by_class[c].empty()) {
                 void* p = free_by_class[c].back();
                 free_by_class[c].pop_back();
@@ -62,12 +67,14 @@ struct PinnedPool {
             }
         }
         void* p = nullptr;
-        if (cudaHostAlloc(&p, (size_t)1 << c, cudaHostAllocDefault) != cudaSuccess) {
+        if (cudaHostAlloc(&p, sz, cudaHostAllocDefault) != cudaSuccess) {
             cudaGetLastError();
+            std::lock_guard<std::mutex> g(m);
+            in_use -= sz;
             return nullptr;
         }
         std::lock_guard<std::mutex> g(m);
-        held += (size_t)1 << c;
+        held += sz;
         return p;
     }
     // Allocates `count` slabs of each class in [lo, hi] up front so that
@@ -93,6 +100,7 @@ struct PinnedPool {
         if (!p) return;
         std::lock_guard<std::mutex> g(m);
         free_by_class[cls(bytes)].push_back(p);
+        in_use -= (size_t)1 << cls(bytes);
     }
     ~PinnedPool() {
         for (auto& v : free_by_class)
@@ -116,20 +124,25 @@ struct Req {
     bool done = false;
 };
 
+// Lane buffers grow geometrically (at least 1.5x), so that a stream of
+// growing batches reallocates a logarithmic number of times.
+size_t grow_to(size_t have, size_t want) { return std::max<size_t>({want, have + have / 2, 1024}); }
+
 template <class T>
 struct DevBuf {
     T* p = nullptr;
     size_t n = 0;
     int ensure(size_t want) {
         if (want <= n) return OK;
-        if (p) cudaFree(p);
+        if (p) cudaFree(p);  // synchronises the device: grow rarely
         p = nullptr;
+        const size_t cap = grow_to(n, want);
         n = 0;
-        if (cudaMalloc(&p, std::max<size_t>(want, 1024) * sizeof(T)) != cudaSuccess) {
+        if (cudaMalloc(&p, cap * sizeof(T)) != cudaSuccess) {
             cudaGetLastError();
             return OUT_OF_MEMORY;
         }
-        n = std::max<size_t>(want, 1024);
+        n = cap;
         return OK;
     }
     void release() {
@@ -147,12 +160,13 @@ struct PinBuf {
         if (want <= n) return OK;
         if (p) cudaFreeHost(p);
         p = nullptr;
+        const size_t cap = grow_to(n, want);
         n = 0;
-        if (cudaHostAlloc((void**)&p, std::max<size_t>(want, 1024) * sizeof(T), cudaHostAllocDefault) != cudaSuccess) {
+        if (cudaHostAlloc((void**)&p, cap * sizeof(T), cudaHostAllocDefault) != cudaSuccess) {
             cudaGetLastError();
             return OUT_OF_MEMORY;
         }
-        n = std::max<size_t>(want, 1024);
+        n = cap;
         return OK;
     }
     void release() {
@@ -434,6 +448,138 @@ long long submit(Server& S, Req* r) {
     return r->id;
 }
 
+// Waits for request `id`, copies its result into the caller's buffer and
+// releases it.  *t_ready (optional) receives the time at which the result
+// reached the caller's buffer, as if a thread had been waiting for exactly
+// this request: completion time plus the copy's duration.
+int wait_request(Server* S, long long id, long long timeout_us, double* t_ready) {
+    if (!S) return -1;
+    std::unique_lock<std::mutex> lk(S->m);
+    auto it = S->reqs.find(id);
+    if (it == S->reqs.end()) return -1;
+    Req* r = it->second;
+    auto pred = [&] { return r->done; };
+    if (timeout_us < 0) S->cv_done.wait(lk, pred);
+    else if (!S->cv_done.wait_for(lk, std::chrono::microseconds(timeout_us), pred)) return -2;
+    const int st = r->status;
+    const double t_done = r->t_done;
+    S->reqs.erase(it);
+    lk.unlock();
+    const double c0 = now_us();
+    if (st == OK) memcpy(r->out, r->res, r->res_bytes);
+    if (t_ready) *t_ready = t_done + (now_us() - c0);
+    S->pool.put(r->in, r->in_bytes);
+    S->pool.put(r->res, r->res_bytes);
+    delete r;
+    return st;
+}
+
+// Replay of a timed trace (cumodp_server_replay): `threads` submitters, each
+// with a collector thread that waits for its requests in submission order.
+struct Replay {
+    Server* S;
+    long long count;
+    const double* arrival;
+    const int* kind;
+    const sfixn* p;
+    const long long *la, *lb;
+    const void* const* a;
+    const void* const* b;
+    void* const* h;
+    double* lat;
+    int* status;
+    double t0;
+};
+
+// Result buffers for requests whose caller gave none, recycled.
+struct ScratchPool {
+    std::mutex m;
+    std::vector<std::pair<size_t, void*>> free_list;
+    void* get(size_t bytes) {
+        std::lock_guard<std::mutex> g(m);
+        for (size_t i = 0; i < free_list.size(); ++i)
+            if (free_list[i].first >= bytes) {
+                void* q = free_list[i].second;
+                free_list.erase(free_list.begin() + i);
+                return q;
+            }
+        return malloc(bytes);
+    }
+    void put(void* q, size_t bytes) {
+        std::lock_guard<std::mutex> g(m);
+        free_list.emplace_back(bytes, q);
+    }
+    ~ScratchPool() {
+        for (auto& e : free_list) free(e.second);
+    }
+};
+
+void replay_thread(const Replay& R, int t, int threads) {
+    struct Item {
+        long long i, id;
+        void* scratch;
+        size_t bytes;
+    };
+    std::mutex qm;
+    std::condition_variable qcv;
+    std::deque<Item> q;
+    bool done = false;
+    ScratchPool scratch;
+    std::thread collector([&] {
+        for (;;) {
+            Item it;
+            {
+                std::unique_lock<std::mutex> lk(qm);
+                qcv.wait(lk, [&] { return done || !q.empty(); });
+                if (q.empty()) return;
+                it = q.front();
+                q.pop_front();
+            }
+            if (it.id < 0) {
+                R.status[it.i] = -1;
+                R.lat[it.i] = 0;
+            } else {
+                double t_ready = 0;
+                R.status[it.i] = wait_request(R.S, it.id, -1, &t_ready);
+                R.lat[it.i] = t_ready - (R.t0 + R.arrival[it.i]);
+            }
+            if (it.scratch) scratch.put(it.scratch, it.bytes);
+        }
+    });
+    for (long long i = t; i < R.count; i += threads) {
+        const double target = R.t0 + R.arrival[i];
+        for (;;) {
+            const double d = target - now_us();
+            if (d <= 0) break;
+            if (d > 200) std::this_thread::sleep_for(std::chrono::microseconds((long long)(d - 100)));
+            else std::this_thread::yield();
+        }
+        const long long n = R.la[i] + R.lb[i] - 1;
+        const size_t bytes = (size_t)std::max<long long>(n, 1) * (R.kind[i] ? 16 : 4);
+        void* out = R.h ? R.h[i] : nullptr;
+        void* scr = nullptr;
+        if (!out) out = scr = scratch.get(bytes);
+        long long id;
+        if (R.kind[i] == 0)
+            id = cumodp_server_submit_mod((cumodp_server*)R.S, R.p[i], (sfixn)(R.la[i] - 1), (const sfixn*)R.a[i],
+                                          (sfixn)(R.lb[i] - 1), (const sfixn*)R.b[i], (sfixn*)out);
+        else
+            id = cumodp_server_submit_i64((cumodp_server*)R.S, R.la[i], (const int64_t*)R.a[i], R.lb[i],
+                                          (const int64_t*)R.b[i], (int64_t*)out);
+        {
+            std::lock_guard<std::mutex> g(qm);
+            q.push_back(Item{i, id, scr, bytes});
+        }
+        qcv.notify_one();
+    }
+    {
+        std::lock_guard<std::mutex> g(qm);
+        done = true;
+    }
+    qcv.notify_one();
+    collector.join();
+}
+
 }  // namespace
 
 }  // namespace cmb
@@ -450,6 +596,7 @@ void cumodp_server_default_config(cumodp_server_config* c) {
     c->batch_window_us = 50;
     c->lanes = 4;
     c->inject_fault_batch = 0;
+    c->host_budget = 0;
 }
 
 cumodp_server* cumodp_server_create(const cumodp_server_config* cfg) {
@@ -474,6 +621,7 @@ cumodp_server* cumodp_server_create(const cumodp_server_config* cfg) {
     for (Lane& L : S->lanes) recreate_lane(L);
     // pinned slabs for operands and results of up to 2^21 words, at most 1 GiB
     S->pool.warm(12, 23, 1ull << 30);
+    S->pool.limit = c.host_budget ? c.host_budget : (8ull << 30);
     S->batcher = std::thread(batcher_loop, S);
     S->completer = std::thread(completer_loop, S);
     return (cumodp_server*)S;
@@ -497,8 +645,11 @@ long long cumodp_server_submit_mod(cumodp_server* h, sfixn p, sfixn df, const sf
         r->in_bytes = (size_t)(r->la + r->lb) * 4;
         r->res_bytes = (size_t)(r->la + r->lb - 1) * 4;
         r->in = S->pool.get(r->in_bytes);
-        r->res = S->pool.get(r->res_bytes);
+        r->res = r->in ? S->pool.get(r->res_bytes) : nullptr;
         if (!r->in || !r->res) {
+            // pinned budget exhausted: shed the request
+            S->pool.put(r->in, r->in_bytes);
+            r->in = nullptr;
             r->status = OUT_OF_MEMORY;
         } else {
             memcpy(r->in, F, (size_t)r->la * 4);
@@ -529,8 +680,10 @@ long long cumodp_server_submit_i64(cumodp_server* h, long long na, const int64_t
         r->in_bytes = (size_t)(na + nb) * 8;
         r->res_bytes = (size_t)(na + nb - 1) * 16;
         r->in = S->pool.get(r->in_bytes);
-        r->res = S->pool.get(r->res_bytes);
+        r->res = r->in ? S->pool.get(r->res_bytes) : nullptr;
         if (!r->in || !r->res) {
+            S->pool.put(r->in, r->in_bytes);
+            r->in = nullptr;
             r->status = OUT_OF_MEMORY;
         } else {
             memcpy(r->in, a, (size_t)na * 8);
@@ -550,23 +703,30 @@ int cumodp_server_poll(cumodp_server* h, long long id) {
 }
 
 int cumodp_server_wait(cumodp_server* h, long long id, long long timeout_us) {
-    Server* S = (Server*)h;
-    if (!S) return -1;
-    std::unique_lock<std::mutex> lk(S->m);
-    auto it = S->reqs.find(id);
-    if (it == S->reqs.end()) return -1;
-    Req* r = it->second;
-    auto pred = [&] { return r->done; };
-    if (timeout_us < 0) S->cv_done.wait(lk, pred);
-    else if (!S->cv_done.wait_for(lk, std::chrono::microseconds(timeout_us), pred)) return -2;
-    const int st = r->status;
-    S->reqs.erase(it);
-    lk.unlock();
-    if (st == OK) memcpy(r->out, r->res, r->res_bytes);
-    S->pool.put(r->in, r->in_bytes);
-    S->pool.put(r->res, r->res_bytes);
-    delete r;
-    return st;
+    return wait_request((Server*)h, id, timeout_us, nullptr);
+}
+
+cumodp_err cumodp_server_replay(cumodp_server* s, long long count, const double* arrival_us, const int* kind,
+                                const sfixn* p, const long long* la, const long long* lb, const void* const* a,
+                                const void* const* b, void* const* h, int threads, double* lat_us, int* status,
+                                double* span_us) {
+    Server* S = (Server*)s;
+    if (!S || count < 0 || threads <= 0 || (count > 0 && (!arrival_us || !kind || !p || !la || !lb || !a || !b ||
+                                                          !lat_us || !status)))
+        return CUMODP_ASSUMPTION_ERROR;
+    for (long long i = 0; i < count; ++i)
+        if (la[i] <= 0 || lb[i] <= 0 || !a[i] || !b[i] || (kind[i] != 0 && kind[i] != 1) ||
+            (kind[i] == 0 && (la[i] > INT32_MAX || lb[i] > INT32_MAX)))
+            return CUMODP_ASSUMPTION_ERROR;
+    Replay R{S, count, arrival_us, kind, p, la, lb, a, b, h, lat_us, status, now_us()};
+    std::vector<std::thread> th;
+    for (int t = 0; t < threads; ++t) th.emplace_back(replay_thread, std::cref(R), t, threads);
+    for (auto& x : th) x.join();
+    double last = R.t0;
+    for (long long i = 0; i < count; ++i)
+        if (status[i] != -1) last = std::max(last, R.t0 + arrival_us[i] + lat_us[i]);
+    if (span_us) *span_us = last - R.t0;
+    return CUMODP_SUCCESS;
 }
 
 void cumodp_server_get_stats(cumodp_server* h, cumodp_server_stats* out) {

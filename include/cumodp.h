@@ -214,6 +214,9 @@ typedef struct {
     int batch_window_us;     /* wait for more arrivals once work is queued (default 50) */
     int lanes;               /* batches in flight at once (default 4) */
     int inject_fault_batch;  /* tests: the n-th batch fails on the host before launching (0 = off) */
+    size_t host_budget;      /* pinned host bytes held by unfinished requests (operand and result
+                                slabs in power-of-two classes); a submission beyond it completes at
+                                once with CUMODP_OUT_OF_MEMORY (load shedding).  0 = 8 GiB */
 } cumodp_server_config;
 typedef struct {
     long long completed, failed, batches, pending;
@@ -234,6 +237,22 @@ int cumodp_server_poll(cumodp_server *s, long long id);
 /* Waits (timeout_us < 0: forever) and returns the request's cumodp_err, -2
  * on timeout, -1 for an unknown id; a waited-for id is forgotten. */
 int cumodp_server_wait(cumodp_server *s, long long id, long long timeout_us);
+/* Addition.  Open-loop replay of a timed request trace against a server,
+ * driven by native threads (a load generator for capacity planning).
+ * Request i is submitted arrival_us[i] microseconds after the call starts
+ * (a submitter that falls behind submits at once): kind[i] = 0 is the
+ * product mod p[i] of la[i] and lb[i] sfixn coefficients a[i], b[i] into
+ * h[i] (la+lb-1 words); kind[i] = 1 the exact product of int64 operands into
+ * h[i] (2(la+lb-1) int64 words).  h may be NULL (results are then written to
+ * recycled scratch buffers and dropped).  `threads` submitters share the
+ * trace round-robin, each with a collector thread.  On return status[i] is
+ * the request's cumodp_err (-1: refused by the server), lat_us[i] the time
+ * from the scheduled arrival to the result in the output buffer, and
+ * *span_us the time from the start to the last result. */
+cumodp_err cumodp_server_replay(cumodp_server *s, long long count, const double *arrival_us, const int *kind,
+                                const sfixn *p, const long long *la, const long long *lb, const void *const *a,
+                                const void *const *b, void *const *h, int threads, double *lat_us, int *status,
+                                double *span_us);
 void cumodp_server_get_stats(cumodp_server *s, cumodp_server_stats *out);
 void cumodp_server_reset_stats(cumodp_server *s);
 /* Drains queued and in-flight work, then frees everything. */

@@ -127,3 +127,43 @@ def test_wait_timeout_and_unknown_id(cm):
     with cm.Server() as srv:
         assert srv.wait(123456, timeout_us=1000) == -1
         assert srv.poll(123456) == -1
+
+
+def test_replay_trace_results_and_latency(cm, oracle_mod):
+    """Native open-loop replay: every result equals the oracle's, latencies are positive."""
+    r = SplitMix64(0xC0DA0105)
+    reqs = _mix(r, 60, max_log=14)
+    arrival = np.cumsum(-np.log(1.0 - r.uniform01(len(reqs))) / 2000.0) * 1e6
+    trace, outs = [], []
+    for q in reqs:
+        if q[0] == "mod":
+            trace.append((q[2], q[3], q[1]))
+            outs.append(np.zeros(len(q[2]) + len(q[3]) - 1, np.uint32))
+        else:
+            trace.append((q[1], q[2], None))
+            outs.append(np.zeros(2 * (len(q[1]) + len(q[2]) - 1), np.int64))
+    with cm.Server(max_batch=32) as srv:
+        st, lat, span = srv.replay(arrival, trace, threads=3, outputs=outs)
+    assert (st == 0).all()
+    assert (lat > 0).all() and span >= arrival[-1]
+    for q, o in zip(reqs, outs):
+        if q[0] == "mod":
+            assert np.array_equal(o, oracle_mod.polymul(q[2], q[3], q[1]))
+        else:
+            assert cm.int128_words_to_ints(o) == oracle_mod.polymul_i128(q[1], q[2])
+
+
+def test_host_budget_sheds_and_server_continues(cm, oracle_mod):
+    """Beyond the pinned host budget a submission completes at once with OUT_OF_MEMORY."""
+    p = PRIMES[0]
+    r = SplitMix64(0xC0DA0106)
+    big = [r.residues(1 << 17, p) for _ in range(2)]
+    with cm.Server(host_budget=3 << 20, batch_window_us=20000) as srv:
+        # each request holds a 1 MiB operand slab and a 1 MiB result slab
+        h1 = srv.submit_mod(big[0], big[1], p)
+        h2 = srv.submit_mod(big[0], big[1], p)
+        assert srv.wait(h2[0]) == cm.OUT_OF_MEMORY
+        assert srv.wait(h1[0]) == 0
+        assert np.array_equal(h1[1], oracle_mod.polymul(big[0], big[1], p))
+        h3 = srv.submit_mod(big[0], big[1], p)  # slabs returned: admitted again
+        assert srv.wait(h3[0]) == 0
