@@ -65,10 +65,12 @@ __host__ __device__ constexpr int row_threads(int logl);
 __host__ __device__ constexpr int small_threads(int logl) { return logl >= 12 ? (1 << (logl - 5)) : 128; }
 __host__ __device__ constexpr int small_ppc(int logl) { return logl >= 12 ? 1 : (1 << (12 - logl)); }
 __host__ __device__ constexpr int row_threads(int logl) { return logl == 14 ? 1024 : small_threads(logl); }
-// Threads of the split row kernels (one operand row per CTA, two CTAs per
-// SM): one per 32-word row of the last level.
-__host__ __device__ constexpr int rowsplit_threads(int logl) { return logl >= 10 ? (1 << (logl - 5)) : 32; }
+// Threads of the split row kernels (one operand row per CTA): one per
+// 32-word row of the last level, two CTAs per SM; 2^14-word rows use 256
+// threads (up to 85 registers each) and three CTAs per SM, so that the load,
+// compute and store phases of three rows overlap on every SM.
+__host__ __device__ constexpr int rowsplit_threads(int logl) { return logl == 14 ? 256 : logl >= 10 ? (1 << (logl - 5)) : 32; }
 // Resident CTAs per SM the split row kernels are compiled for.
-__host__ __device__ constexpr int rowsplit_ctas(int logl) { return 2; }
+__host__ __device__ constexpr int rowsplit_ctas(int logl) { return logl == 14 ? 3 : 2; }
 
 }  // namespace cmb

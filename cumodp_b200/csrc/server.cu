@@ -28,6 +28,7 @@
 #include <deque>
 #include <thread>
 #include <unordered_map>
+#include <unordered_set>
 
 #include "../../include/cumodp.h"
 #include "exact.cuh"
@@ -40,71 +41,87 @@ double now_us() {
     return std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-// Pinned host slabs in power-of-two size classes, recycled: allocating pinned
-// memory is slow, so slabs outlive requests.
+// Pinned host slabs: a buddy allocator over pinned chunks of 256 MiB (less
+// under a smaller limit).  Pinning memory (cudaHostAlloc) is slow and serialises with the
+// device, so chunks are pinned up front (reserve) or, past that, at most a
+// few times, and never returned before the server ends; slabs are carved
+// from them in power-of-two sizes and coalesce with their buddies when freed,
+// so a shift in request sizes reuses the same memory.  `limit` bounds the
+// pinned bytes: beyond it get() fails (the server sheds the request).
 struct PinnedPool {
+    static constexpr int kMinOrder = 12, kMaxChunkOrder = 28;
+    int kChunkOrder = kMaxChunkOrder;  // chunk size: 256 MiB, or less under a smaller limit
     std::mutex m;
-    std::vector<std::vector<void*>> free_by_class = std::vector<std::vector<void*>>(40);
-    size_t held = 0;
-    size_t in_use = 0;             // bytes of slabs handed out and not yet returned
-    size_t limit = ~(size_t)0;     // get() fails beyond this (load shedding)
-    static int cls(size_t bytes) {
-        int c = 12;
+    std::vector<char*> chunks;
+    std::vector<std::unordered_set<uintptr_t>> free_blocks =
+        std::vector<std::unordered_set<uintptr_t>>(kMaxChunkOrder + 1);
+    size_t in_use = 0;          // bytes of slabs handed out and not yet returned
+    size_t limit = ~(size_t)0;  // pinned bytes at most
+    static int order(size_t bytes) {
+        int c = kMinOrder;
         while (((size_t)1 << c) < bytes) ++c;
         return c;
     }
-    void* get(size_t bytes) {
-        const int c = cls(bytes);
-        const size_t sz = (size_t)1 << c;
-        {
-            std::lock_guard<std::mutex> g(m);
-            if (in_use + sz > limit) return nullptr;
-            in_use += sz;
-            if (!free_by_class[c].empty()) {
-                void* p = free_by_class[c].back();
-                free_by_class[c].pop_back();
-                return p;
-            }
-        }
+    bool add_chunk() {  // with m held
+        if ((chunks.size() + 1) << kChunkOrder > limit) return false;
         void* p = nullptr;
-        if (cudaHostAlloc(&p, sz, cudaHostAllocDefault) != cudaSuccess) {
+        if (cudaHostAlloc(&p, (size_t)1 << kChunkOrder, cudaHostAllocDefault) != cudaSuccess) {
             cudaGetLastError();
-            std::lock_guard<std::mutex> g(m);
-            in_use -= sz;
-            return nullptr;
+            return false;
         }
-        std::lock_guard<std::mutex> g(m);
-        held += sz;
-        return p;
+        chunks.push_back((char*)p);
+        free_blocks[kChunkOrder].insert((uintptr_t)p);
+        return true;
     }
-    // Allocates `count` slabs of each class in [lo, hi] up front so that
-    // serving does not call cudaHostAlloc (slow, and it synchronises with
-    // the device) on its hot path.
-    void warm(int lo, int hi, size_t budget) {
-        for (int c = lo; c <= hi; ++c) {
-            const int count = c <= 18 ? 16 : (c <= 21 ? 8 : 4);
-            for (int k = 0; k < count && ((size_t)1 << c) <= budget; ++k) {
-                void* p = nullptr;
-                if (cudaHostAlloc(&p, (size_t)1 << c, cudaHostAllocDefault) != cudaSuccess) {
-                    cudaGetLastError();
-                    return;
-                }
-                std::lock_guard<std::mutex> g(m);
-                free_by_class[c].push_back(p);
-                held += (size_t)1 << c;
-                budget -= (size_t)1 << c;
-            }
+    void set_limit(size_t bytes) {
+        limit = bytes;
+        while (kChunkOrder > kMinOrder && ((size_t)1 << kChunkOrder) > limit) --kChunkOrder;
+    }
+    // Pins chunks for up to `bytes` (within the limit) ahead of serving.
+    void reserve(size_t bytes) {
+        std::lock_guard<std::mutex> g(m);
+        while (chunks.size() << kChunkOrder < bytes && add_chunk()) {
         }
+    }
+    void* get(size_t bytes) {
+        const int c = order(bytes);
+        if (c > kChunkOrder) return nullptr;
+        std::lock_guard<std::mutex> g(m);
+        int o = c;
+        while (o <= kChunkOrder && free_blocks[o].empty()) ++o;
+        if (o > kChunkOrder) {
+            if (!add_chunk()) return nullptr;
+            o = kChunkOrder;
+        }
+        uintptr_t blk = *free_blocks[o].begin();
+        free_blocks[o].erase(free_blocks[o].begin());
+        while (o > c) {  // split, keeping the lower half
+            --o;
+            free_blocks[o].insert(blk + ((uintptr_t)1 << o));
+        }
+        in_use += (size_t)1 << c;
+        return (void*)blk;
     }
     void put(void* p, size_t bytes) {
         if (!p) return;
+        int o = order(bytes);
         std::lock_guard<std::mutex> g(m);
-        free_by_class[cls(bytes)].push_back(p);
-        in_use -= (size_t)1 << cls(bytes);
+        in_use -= (size_t)1 << o;
+        uintptr_t blk = (uintptr_t)p, base = 0;
+        for (char* ch : chunks)
+            if (blk >= (uintptr_t)ch && blk < (uintptr_t)ch + ((uintptr_t)1 << kChunkOrder)) base = (uintptr_t)ch;
+        while (o < kChunkOrder) {  // coalesce with free buddies
+            const uintptr_t buddy = base + ((blk - base) ^ ((uintptr_t)1 << o));
+            auto it = free_blocks[o].find(buddy);
+            if (it == free_blocks[o].end()) break;
+            free_blocks[o].erase(it);
+            blk = std::min(blk, buddy);
+            ++o;
+        }
+        free_blocks[o].insert(blk);
     }
     ~PinnedPool() {
-        for (auto& v : free_by_class)
-            for (void* p : v) cudaFreeHost(p);
+        for (char* ch : chunks) cudaFreeHost(ch);
     }
 };
 
@@ -619,9 +636,9 @@ cumodp_server* cumodp_server_create(const cumodp_server_config* cfg) {
     Server* S = new Server(c);
     S->lanes.resize(c.lanes);
     for (Lane& L : S->lanes) recreate_lane(L);
-    // pinned slabs for operands and results of up to 2^21 words, at most 1 GiB
-    S->pool.warm(12, 23, 1ull << 30);
-    S->pool.limit = c.host_budget ? c.host_budget : (8ull << 30);
+    // pinned slabs: up to host_budget, the first 1 GiB pinned now
+    S->pool.set_limit(c.host_budget ? c.host_budget : (8ull << 30));
+    S->pool.reserve(1ull << 30);
     S->batcher = std::thread(batcher_loop, S);
     S->completer = std::thread(completer_loop, S);
     return (cumodp_server*)S;

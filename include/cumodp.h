@@ -214,9 +214,11 @@ typedef struct {
     int batch_window_us;     /* wait for more arrivals once work is queued (default 50) */
     int lanes;               /* batches in flight at once (default 4) */
     int inject_fault_batch;  /* tests: the n-th batch fails on the host before launching (0 = off) */
-    size_t host_budget;      /* pinned host bytes held by unfinished requests (operand and result
-                                slabs in power-of-two classes); a submission beyond it completes at
-                                once with CUMODP_OUT_OF_MEMORY (load shedding).  0 = 8 GiB */
+    size_t host_budget;      /* pinned host memory for the operand and result slabs of unfinished
+                                requests (power-of-two slabs carved from pinned chunks; 1 GiB is
+                                pinned at creation, the rest on demand); a submission that finds
+                                no room completes at once with CUMODP_OUT_OF_MEMORY (load
+                                shedding).  0 = 8 GiB */
 } cumodp_server_config;
 typedef struct {
     long long completed, failed, batches, pending;
