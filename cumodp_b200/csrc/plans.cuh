@@ -64,13 +64,18 @@ __host__ __device__ constexpr int row_threads(int logl);
 // Threads and products per CTA for the fused single-CTA product of length L.
 __host__ __device__ constexpr int small_threads(int logl) { return logl >= 12 ? (1 << (logl - 5)) : 128; }
 __host__ __device__ constexpr int small_ppc(int logl) { return logl >= 12 ? 1 : (1 << (12 - logl)); }
+// Resident CTAs per SM the fused single-CTA product is compiled for: six
+// 32 KiB CTAs of 128 threads (80 registers) for lengths <= 2^12, three
+// 64 KiB CTAs for 2^13, one 128 KiB CTA for 2^14.
+__host__ __device__ constexpr int small_ctas(int logl) { return logl <= 12 ? 6 : logl == 13 ? 3 : 1; }
 __host__ __device__ constexpr int row_threads(int logl) { return logl == 14 ? 1024 : small_threads(logl); }
 // Threads of the split row kernels (one operand row per CTA): one per
 // 32-word row of the last level, two CTAs per SM; 2^14-word rows use 256
 // threads (up to 85 registers each) and three CTAs per SM, so that the load,
 // compute and store phases of three rows overlap on every SM.
 __host__ __device__ constexpr int rowsplit_threads(int logl) { return logl == 14 ? 256 : logl >= 10 ? (1 << (logl - 5)) : 32; }
-// Resident CTAs per SM the split row kernels are compiled for.
-__host__ __device__ constexpr int rowsplit_ctas(int logl) { return logl == 14 ? 3 : 2; }
+// Resident CTAs per SM the split row kernels are compiled for: three for
+// 2^14-word rows, else enough for 1024 threads per SM (64 registers).
+__host__ __device__ constexpr int rowsplit_ctas(int logl) { return logl == 14 ? 3 : (1024 / rowsplit_threads(logl) < 32 ? 1024 / rowsplit_threads(logl) : 32); }
 
 }  // namespace cmb

@@ -191,7 +191,7 @@ __device__ __forceinline__ void store_row32(u32* sm, int base, const u32 (&x)[32
 }
 
 template <int LOGL>
-__global__ void __launch_bounds__(small_threads(LOGL), 1)
+__global__ void __launch_bounds__(small_threads(LOGL), small_ctas(LOGL))
 k_small_product(const __grid_constant__ SmallArgs A) {
     constexpr int L = 1 << LOGL;
     constexpr int T = small_threads(LOGL);
