@@ -106,6 +106,14 @@ def _lib():
         L.cumodp_list_fft_dev.restype = C.c_int
         L.cumodp_list_fft_dev.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int,
                                           C.c_void_p]
+        L.cumodp_bivariate_mul_dev.restype = C.c_int
+        L.cumodp_bivariate_mul_dev.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]
+        L.cumodp_bivariate_mul.restype = C.c_int
+        L.cumodp_bivariate_mul.argtypes = [C.c_int32, C.c_int32, _i32p, C.c_int32, C.c_int32, _i32p, _i32p,
+                                           C.c_int32]
+        L.cumodp_subproduct_level_dev.restype = C.c_int
+        L.cumodp_subproduct_level_dev.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
+                                                  C.c_void_p]
         L.cumodp_select_device.restype = C.c_int
         L.cumodp_select_device.argtypes = [C.c_int]
         L.cumodp_trace_passes.restype = None
@@ -300,6 +308,33 @@ def fft_uni_dev(x_ptr: int, k: int, w: int, p: int, inverse: bool = False, strea
 def list_fft_dev(x_ptr: int, m: int, k: int, w: int, p: int, inverse: bool = False, stream: int = 0) -> None:
     """m natural-order transforms of 2^k device words each, in place (``cumodp_list_fft_dev``)."""
     _check(_lib().cumodp_list_fft_dev(x_ptr, m, k, w, p, int(inverse), stream or None), "cumodp_list_fft_dev")
+
+
+def bivariate_mul(F, G, p: int) -> np.ndarray:
+    """Bivariate product mod p (``cumodp_bivariate_mul``).
+
+    F, G: 2-D arrays indexed [y, x] (row j holds the coefficients of y^j).
+    Returns the product as a uint32 array of shape (nyf + nyg - 1, nxf + nxg - 1).
+    """
+    F = np.asarray(F)
+    G = np.asarray(G)
+    (nyf, nxf), (nyg, nxg) = F.shape, G.shape
+    f = _as_i32(np.ascontiguousarray(F).reshape(-1))
+    g = _as_i32(np.ascontiguousarray(G).reshape(-1))
+    h = np.empty((nyf + nyg - 1) * (nxf + nxg - 1), dtype=np.int32)
+    _check(_lib().cumodp_bivariate_mul(nxf, nyf, f, nxg, nyg, g, h, p), "cumodp_bivariate_mul")
+    return h.view(np.uint32).reshape(nyf + nyg - 1, nxf + nxg - 1)
+
+
+def bivariate_mul_dev(em: int, en: int, f_ptr: int, g_ptr: int, p: int, stream: int = 0) -> None:
+    """In-place 2-D cyclic convolution on a 2^em x 2^en device grid (``cumodp_bivariate_mul_dev``)."""
+    _check(_lib().cumodp_bivariate_mul_dev(em, en, f_ptr, g_ptr, p, stream or None), "cumodp_bivariate_mul_dev")
+
+
+def subproduct_level_dev(l: int, npairs: int, in_ptr: int, out_ptr: int, p: int, stream: int = 0) -> None:
+    """One subproduct-tree level on device arrays (``cumodp_subproduct_level_dev``)."""
+    _check(_lib().cumodp_subproduct_level_dev(l, npairs, in_ptr, out_ptr, p, stream or None),
+           "cumodp_subproduct_level_dev")
 
 
 def select_device(dev: int) -> None:

@@ -487,11 +487,72 @@ int batch_launch_count(int count, const sfixn* df, const sfixn* dg) {
     return n;
 }
 
+// out[j][l + t] += a_j[t] + b_j[t] (t < l - 1), out[j][2l - 1] = a_j[l - 1] + b_j[l - 1]:
+// the x^l (a + b) term of (x^l + a)(x^l + b) = x^2l + x^l (a + b) + a b.
+__global__ void k_monic_level_fixup(const u32* __restrict__ in, u32* __restrict__ out, long long l, long long npairs,
+                                    u32 p) {
+    const long long total = npairs * l;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long j = i / l, t = i % l;
+        const u32 a = in[2 * j * l + t] % p, b = in[(2 * j + 1) * l + t] % p;
+        u32 s = a + b;
+        s = s >= p ? s - p : s;
+        u32* o = out + 2 * j * l + l + t;
+        if (t < l - 1) {
+            u32 v = *o + s;
+            *o = v >= p ? v - p : v;
+        } else {
+            *o = s;
+        }
+    }
+}
+
+// One level of a subproduct tree of monic polynomials stored without their
+// leading coefficient: out[j] = in[2j] * in[2j+1] (degree l each, l words;
+// the product has degree 2l, 2l words).  The products a b run as one batch
+// of equal-size pairs (the graph-captured batch path), then one kernel adds
+// the x^l (a + b) term.
+int subproduct_level_dev(long long l, long long npairs, const u32* in, u32* out, u32 p, cudaStream_t st) {
+    if (l <= 0 || npairs < 0 || npairs > INT32_MAX || l > (1ll << 23)) return ASSUMPTION_ERROR;
+    if (npairs == 0) return OK;
+    if (!in || !out) return ASSUMPTION_ERROR;
+    if (out < in + 2 * npairs * l && in < out + 2 * npairs * l) return ASSUMPTION_ERROR;  // no aliasing
+    const int cnt = (int)npairs;
+    std::vector<sfixn> d(cnt, (sfixn)(l - 1));
+    std::vector<int64_t> fo(cnt), go(cnt), ho(cnt);
+    for (int j = 0; j < cnt; ++j) {
+        fo[j] = 2 * (int64_t)j * l;
+        go[j] = (2 * (int64_t)j + 1) * l;
+        ho[j] = 2 * (int64_t)j * l;
+    }
+    int err = batch_mul_dev(cnt, d.data(), fo.data(), in, d.data(), go.data(), in, ho.data(), out, p, st);
+    if (err != OK) return err;
+    const long long total = npairs * l;
+    const int grid = (int)std::max<long long>(1, std::min<long long>((total + 255) / 256, 148 * 16));
+    k_monic_level_fixup<<<grid, 256, 0, st>>>(in, out, l, npairs, p);
+    return cuda_err(cudaGetLastError());
+}
+
 }  // namespace cmb
 
 using namespace cmb;
 
 extern "C" {
+
+cumodp_err cumodp_subproduct_level_dev(sfixn l, sfixn npairs, const sfixn* M_in, sfixn* M_out, sfixn p,
+                                       void* stream) {
+    int cnt = 0;
+    if (cudaGetDeviceCount(&cnt) != cudaSuccess || cnt == 0) {
+        cudaGetLastError();
+        return CUMODP_NO_CUDA_DEVICE;
+    }
+    std::lock_guard<std::mutex> g(lib_mutex());
+    cudaStream_t st = stream ? (cudaStream_t)stream : lib_stream(current_device());
+    int e = subproduct_level_dev(l, npairs, (const u32*)M_in, (u32*)M_out, (u32)p, st);
+    if (e == OK && !stream) e = cuda_err(cudaStreamSynchronize(st));
+    return (cumodp_err)e;
+}
 
 cumodp_err cumodp_fftmul_batch_dev(int count, const sfixn* df, const int64_t* f_off, const sfixn* F,
                                    const sfixn* dg, const int64_t* g_off, const sfixn* G, const int64_t* h_off,

@@ -358,6 +358,103 @@ int bivariate_dev(u32* x, int em, u32 wm, int en, u32 wn, u32 p, bool inverse, c
     return cuda_err(cudaGetLastError());
 }
 
+// out[c * rows + r] = in[r * cols + c] for any shape: 32 x 32 tiles through
+// shared memory, bounds-checked.
+__global__ void k_transpose_any(const u32* __restrict__ in, u32* __restrict__ out, int rows, int cols) {
+    __shared__ u32 t[32][33];
+    const long long c0 = (long long)blockIdx.x * 32, r0 = (long long)blockIdx.y * 32;
+    for (int y = threadIdx.y; y < 32; y += blockDim.y)
+        if (r0 + y < rows && c0 + threadIdx.x < cols) t[y][threadIdx.x] = in[(r0 + y) * cols + c0 + threadIdx.x];
+    __syncthreads();
+    for (int y = threadIdx.y; y < 32; y += blockDim.y)
+        if (c0 + y < cols && r0 + threadIdx.x < rows) out[(c0 + y) * rows + r0 + threadIdx.x] = t[threadIdx.x][y];
+}
+
+// a[i] = a[i] * b[i] mod p (inputs in [0, p)).
+__global__ void k_pointwise_mod(u32* __restrict__ a, const u32* __restrict__ b, long long n, u32 p) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        a[i] = (u32)(((u64)a[i] * b[i]) % p);
+}
+
+// dst (2^ey2 rows of 2^ex2) = src (ny1 rows of nx1) zero-padded, reduced mod p.
+__global__ void k_expand2(const u32* __restrict__ src, int nx1, int ny1, u32* __restrict__ dst, int ex2, int ey2,
+                          u32 p) {
+    const long long total = 1ll << (ex2 + ey2);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long y = i >> ex2, x = i & ((1ll << ex2) - 1);
+        dst[i] = (x < nx1 && y < ny1) ? src[y * nx1 + x] % p : 0u;
+    }
+}
+
+// dst (ny1 rows of nx1) = the top-left corner of src (rows of 2^ex2).
+__global__ void k_extract2(const u32* __restrict__ src, int ex2, u32* __restrict__ dst, int nx1, int ny1) {
+    const long long total = (long long)nx1 * ny1;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long y = i / nx1, x = i % nx1;
+        dst[i] = src[(y << ex2) + x];
+    }
+}
+
+int grid_for(long long n) { return (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148 * 16)); }
+
+// F <- DFT^-1(DFT F * DFT G) on a 2^em x 2^en row-major grid (rows: y, of
+// length 2^en in x): the 2-D cyclic convolution, i.e. the bivariate product
+// when both operands are zero-padded to the product's size.  Row transforms,
+// a transpose, column transforms (as rows) give both spectra in transposed
+// order; the pointwise product and the inverse steps run in that order, so
+// nothing is permuted back before the last transpose.  G is overwritten.
+int bivariate_mul_dev(u32* F, u32* G, int em, int en, u32 p, cudaStream_t st) {
+    int err = OK;
+    const PrimeCtx* pc = prime_ctx(p, &err);
+    if (!pc) return err;
+    if (em < 0 || en < 0) return ASSUMPTION_ERROR;
+    if (em > pc->info.two_adic || en > pc->info.two_adic || em + en > 30) return FFT_SIZE_TOO_LARGE;
+    const long long m = 1ll << em, n = 1ll << en, total = m * n;
+    const u32 wm = em ? canonical_root(*pc, em) : 1u, wn = en ? canonical_root(*pc, en) : 1u;
+    const int dev = current_device();
+    u32* ws = (u32*)workspace(dev, kWsBiv, (size_t)2 * total * sizeof(u32), &err);
+    if (!ws) return err;
+    u32 *W1 = ws, *W2 = ws + total;
+    const dim3 tb(32, 8);
+    const dim3 g_mn((unsigned)((n + 31) / 32), (unsigned)((m + 31) / 32));  // m rows x n columns
+    const dim3 g_nm((unsigned)((m + 31) / 32), (unsigned)((n + 31) / 32));  // n rows x m columns
+    u32* src[2] = {F, G};
+    u32* spec[2] = {W1, W2};
+    for (int o = 0; o < 2; ++o) {
+        if ((err = list_ntt_dev(src[o], m, en, wn, p, false, st)) != OK) return err;
+        k_transpose_any<<<g_mn, tb, 0, st>>>(src[o], spec[o], (int)m, (int)n);
+        if ((err = list_ntt_dev(spec[o], n, em, wm, p, false, st)) != OK) return err;
+    }
+    k_pointwise_mod<<<grid_for(total), 256, 0, st>>>(W1, W2, total, p);
+    if ((err = list_ntt_dev(W1, n, em, wm, p, true, st)) != OK) return err;
+    k_transpose_any<<<g_nm, tb, 0, st>>>(W1, F, (int)n, (int)m);
+    if ((err = list_ntt_dev(F, m, en, wn, p, true, st)) != OK) return err;
+    return cuda_err(cudaGetLastError());
+}
+
+// Bivariate product of (nx, ny)-dense operands (coefficient of x^i y^j at
+// j * nx + i), device buffers: H gets (nxf + nxg - 1) x (nyf + nyg - 1).
+int bivariate_product_dev(const u32* F, int nxf, int nyf, const u32* G, int nxg, int nyg, u32* H, u32 p,
+                          cudaStream_t st) {
+    int err = OK;
+    const long long lx = (long long)nxf + nxg - 1, ly = (long long)nyf + nyg - 1;
+    int ex = 0, ey = 0;
+    while ((1ll << ex) < lx) ++ex;
+    while ((1ll << ey) < ly) ++ey;
+    if (ex + ey > 30) return FFT_SIZE_TOO_LARGE;
+    const long long total = 1ll << (ex + ey);
+    u32* ws = (u32*)workspace(current_device(), kWsBivHost, (size_t)2 * total * sizeof(u32), &err);
+    if (!ws) return err;
+    u32 *F2 = ws, *G2 = ws + total;
+    k_expand2<<<grid_for(total), 256, 0, st>>>(F, nxf, nyf, F2, ex, ey, p);
+    k_expand2<<<grid_for(total), 256, 0, st>>>(G, nxg, nyg, G2, ex, ey, p);
+    if ((err = bivariate_mul_dev(F2, G2, ey, ex, p, st)) != OK) return err;
+    k_extract2<<<grid_for(lx * ly), 256, 0, st>>>(F2, ex, H, (int)lx, (int)ly);
+    return cuda_err(cudaGetLastError());
+}
+
 }  // namespace cmb
 
 using namespace cmb;
@@ -445,6 +542,50 @@ cumodp_err cumodp_list_fft_dev(sfixn* X, sfixn m, sfixn k, sfixn w, sfixn p, int
     int e = list_ntt_dev((u32*)X, m, k, (u32)w, (u32)p, inverse != 0, st);
     if (e == OK && !stream) e = cuda_err(cudaStreamSynchronize(st));
     return (cumodp_err)e;
+}
+
+cumodp_err cumodp_bivariate_mul_dev(sfixn em, sfixn en, sfixn* F, sfixn* G, sfixn p, void* stream) {
+    int cnt = 0;
+    if (cudaGetDeviceCount(&cnt) != cudaSuccess || cnt == 0) {
+        cudaGetLastError();
+        return CUMODP_NO_CUDA_DEVICE;
+    }
+    if (!F || !G || em < 0 || en < 0 || p <= 0) return CUMODP_ASSUMPTION_ERROR;
+    std::lock_guard<std::mutex> g(lib_mutex());
+    cudaStream_t st = stream ? (cudaStream_t)stream : lib_stream(current_device());
+    int e = bivariate_mul_dev((u32*)F, (u32*)G, em, en, (u32)p, st);
+    if (e == OK && !stream) e = cuda_err(cudaStreamSynchronize(st));
+    return (cumodp_err)e;
+}
+
+cumodp_err cumodp_bivariate_mul(sfixn nxf, sfixn nyf, const sfixn* F, sfixn nxg, sfixn nyg, const sfixn* G,
+                                sfixn* H, sfixn p) {
+    int cnt = 0;
+    if (cudaGetDeviceCount(&cnt) != cudaSuccess || cnt == 0) {
+        cudaGetLastError();
+        return CUMODP_NO_CUDA_DEVICE;
+    }
+    if (!F || !G || !H || nxf <= 0 || nyf <= 0 || nxg <= 0 || nyg <= 0 || p <= 0) return CUMODP_ASSUMPTION_ERROR;
+    const long long nf = (long long)nxf * nyf, ng = (long long)nxg * nyg;
+    const long long nh = ((long long)nxf + nxg - 1) * ((long long)nyf + nyg - 1);
+    if (nh > (1ll << 30)) return CUMODP_FFT_SIZE_TOO_LARGE;
+    std::lock_guard<std::mutex> g(lib_mutex());
+    const int dev = current_device();
+    cudaStream_t st = lib_stream(dev);
+    int err = OK;
+    u32* d = (u32*)workspace(dev, kWsStage, (size_t)(nf + ng + nh) * sizeof(u32), &err);
+    if (!d) return (cumodp_err)err;
+    cudaError_t ce = cudaMemcpyAsync(d, F, nf * 4, cudaMemcpyHostToDevice, st);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(d + nf, G, ng * 4, cudaMemcpyHostToDevice, st);
+    if (ce != cudaSuccess) return (cumodp_err)cuda_err(ce);
+    err = bivariate_product_dev(d, nxf, nyf, d + nf, nxg, nyg, d + nf + ng, (u32)p, st);
+    if (err != OK) {
+        cudaStreamSynchronize(st);
+        return (cumodp_err)err;
+    }
+    ce = cudaMemcpyAsync(H, d + nf + ng, nh * 4, cudaMemcpyDeviceToHost, st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    return (cumodp_err)cuda_err(ce);
 }
 
 cumodp_err cumodp_fft_uni(sfixn* X, sfixn n, sfixn k, sfixn w, sfixn p) { return host_ntt(X, n, k, w, p, false); }

@@ -275,6 +275,41 @@ cumodp_err cumodp_fft_uni_dev(sfixn *X, sfixn n, sfixn k, sfixn w, sfixn p, int 
  * synchronised. */
 cumodp_err cumodp_list_fft_dev(sfixn *X, sfixn m, sfixn k, sfixn w, sfixn p, int inverse, void *stream);
 
+/* Addition.  Bivariate product on a 2^em x 2^en grid of DEVICE words (row
+ * j, of 2^en words, holds the coefficients of y^j; x^i at column i):
+ * F <- DFT^-1(DFT F * DFT G), the 2-D cyclic convolution, which is the
+ * bivariate product when both operands are zero-padded to the product's
+ * size.  G is overwritten.  Counterpart of the reference's C++
+ * bi_stockham_poly_mul_dev (src/list_stockham.cu:1317-1348, declared in
+ * include/list_stockham.h:103-104; include/list_stockham_b200.h gives that
+ * signature), for any em, en within the prime's 2-adic order (em + en <= 30).
+ * stream: 0 = library stream, then synchronised. */
+cumodp_err cumodp_bivariate_mul_dev(sfixn em, sfixn en, sfixn *F, sfixn *G, sfixn p, void *stream);
+
+/* Addition.  Bivariate product of HOST operands in the (nx, ny) dense layout
+ * (coefficient of x^i y^j at j * nx + i): H receives
+ * (nxf + nxg - 1) * (nyf + nyg - 1) words in the (nxf + nxg - 1,
+ * nyf + nyg - 1) layout.  Counterpart of the reference's
+ * bi_stockham_poly_mul_host (src/list_stockham.cu:1352-1390, with
+ * expand_to_fft2_dev / extract_from_fft2_dev, src/fft_aux.cu:630-681), on
+ * plain arrays instead of its rdr_poly class. */
+cumodp_err cumodp_bivariate_mul(sfixn nxf, sfixn nyf, const sfixn *F, sfixn nxg, sfixn nyg, const sfixn *G,
+                                sfixn *H, sfixn p);
+
+/* Addition.  One level of a subproduct tree, as one call on DEVICE arrays:
+ * M_in holds 2*npairs monic polynomials of degree l stored without their
+ * leading coefficient (l words each, constant term first, polynomial j at
+ * M_in + j*l); M_out (not overlapping M_in) receives the npairs products
+ * M_in[2j] * M_in[2j+1], monic of degree 2l, likewise without the leading
+ * coefficient (2l words each, at M_out + 2*j*l).  Replaces the reference's
+ * level step of subProductTree (src/fastPolyEvaluation.cu:604-650:
+ * zeroInbetween, list_stockham_dev, pointMul, inverse transform, scalarMul,
+ * pointAdd2 and pointAdd, whose kernels are at :83-160) for any l >= 1 and
+ * any number of pairs (the reference: powers of two).
+ * stream: 0 = library stream, then synchronised. */
+cumodp_err cumodp_subproduct_level_dev(sfixn l, sfixn npairs, const sfixn *M_in, sfixn *M_out, sfixn p,
+                                       void *stream);
+
 /* Addition.  Makes `dev` the current device of the calling thread for the
  * library's own CUDA runtime (one process per GPU). */
 cumodp_err cumodp_select_device(int dev);

@@ -1,6 +1,7 @@
 /*
- * list_stockham_b200.h -- C++ signatures of the reference's list transform,
- * forwarding to cumodp_list_fft_dev.
+ * list_stockham_b200.h -- C++ signatures of the reference's list transform
+ * and bivariate product, forwarding to cumodp_list_fft_dev and
+ * cumodp_bivariate_mul_dev.
  *
  * Replaces list_stockham_dev (include/list_stockham.h:48-49,
  * src/list_stockham.cu:595-665): X = I_m (x) DFT_n(X) for a device array of m
@@ -25,6 +26,13 @@ inline cumodp_err list_stockham_dev(sfixn *X, sfixn m, sfixn k, const sfixn *W, 
     if (k > 0 && cudaMemcpy(&w, W + 1, sizeof(sfixn), cudaMemcpyDeviceToHost) != cudaSuccess)
         return CUMODP_FFT_ERROR;
     return cumodp_list_fft_dev(X, m, k, w, p, 0, 0);
+}
+// Replaces bi_stockham_poly_mul_dev (include/list_stockham.h:103-104,
+// src/list_stockham.cu:1317-1348): F <- DFT^-1(DFT F * DFT G) on an m x n
+// grid (m = 2^em rows in y, n = 2^en columns in x); G is overwritten.
+inline cumodp_err bi_stockham_poly_mul_dev(sfixn m, sfixn em, sfixn n, sfixn en, sfixn *F, sfixn *G, sfixn p) {
+    if (m != ((sfixn)1 << em) || n != ((sfixn)1 << en)) return CUMODP_ASSUMPTION_ERROR;
+    return cumodp_bivariate_mul_dev(em, en, F, G, p, 0);
 }
 #endif
 

@@ -159,6 +159,48 @@ def polymul(a: np.ndarray, b: np.ndarray, p: int) -> np.ndarray:
     return h
 
 
+def bivariate_mul(F: np.ndarray, G: np.ndarray, p: int) -> np.ndarray:
+    """Bivariate product mod p of 2-D arrays indexed [y, x].
+
+    Follows bi_stockham_poly_mul_host (reference src/list_stockham.cu:1352-1390):
+    the product of the (nx, ny)-dense operands, here computed by Kronecker
+    substitution x^i y^j -> z^(j X + i) with X = nxf + nxg - 1 (no carry
+    between y-rows) and the oracle's univariate product.
+    """
+    F = np.asarray(F, dtype=np.uint32)
+    G = np.asarray(G, dtype=np.uint32)
+    (nyf, nxf), (nyg, nxg) = F.shape, G.shape
+    X, Y = nxf + nxg - 1, nyf + nyg - 1
+    f = np.zeros(nyf * X, np.uint32)
+    g = np.zeros(nyg * X, np.uint32)
+    f.reshape(nyf, X)[:, :nxf] = F % p
+    g.reshape(nyg, X)[:, :nxg] = G % p
+    h = polymul_school(f, g, p) if len(f) * len(g) <= 1 << 22 else polymul(f, g, p)
+    assert not h[Y * X:].any()  # the product's degree is below Y X
+    out = np.zeros(Y * X, np.uint32)
+    out[:min(len(h), Y * X)] = h[:Y * X]
+    return out.reshape(Y, X)
+
+
+def subproduct_level(M: np.ndarray, l: int, p: int) -> np.ndarray:
+    """One subproduct-tree level of monic polynomials stored without leading coefficient.
+
+    Follows subProductTree's FFT level step (reference
+    src/fastPolyEvaluation.cu:604-650 with pointAdd2 :83-92 and pointAdd
+    :153-158): out[j] = (x^l + M[2j]) (x^l + M[2j+1]) - x^(2l), 2l words.
+    Computed here with explicit leading ones and the oracle's product.
+    """
+    M = np.asarray(M, dtype=np.uint32).reshape(-1, l)
+    out = np.empty((M.shape[0] // 2, 2 * l), np.uint32)
+    for j in range(M.shape[0] // 2):
+        a = np.append(M[2 * j] % p, 1).astype(np.uint32)
+        b = np.append(M[2 * j + 1] % p, 1).astype(np.uint32)
+        h = polymul_school(a, b, p) if l <= 512 else polymul(a, b, p)
+        assert h[2 * l] == 1
+        out[j] = h[:2 * l]
+    return out.reshape(-1)
+
+
 def polymul_i128(a: np.ndarray, b: np.ndarray) -> list[int]:
     """Exact integer product (Python ints) by __int128 schoolbook."""
     a = np.ascontiguousarray(a, dtype=np.int64)

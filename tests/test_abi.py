@@ -77,7 +77,8 @@ def test_cpp_forwarding_header_compiles():
         "void use(sfixn* X, const sfixn* W) {\n"
         "  cumodp_err a = list_stockham_dev(X, 4, 10, 3, 469762049);\n"
         "  cumodp_err b = list_stockham_dev(X, 4, 10, W, 469762049);\n"
-        "  (void)a; (void)b;\n}\n")
+        "  cumodp_err c = bi_stockham_poly_mul_dev(64, 6, 512, 9, X, X + 32768, 469762049);\n"
+        "  (void)a; (void)b; (void)c;\n}\n")
     with tempfile.TemporaryDirectory() as d:
         f = os.path.join(d, "use.cpp")
         open(f, "w").write(src)

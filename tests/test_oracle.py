@@ -128,3 +128,33 @@ def test_crt_signed(oracle_mod):
     for v in [0, 1, -1, 10**20, -(10**20), P // 2, -(P // 2) + 1, 2**80 + 12345]:
         assert oracle_mod.crt_signed([v % q for q in ps], ps) == v
     assert oracle_mod.crt_signed([7 % 962592769, 7 % 950009857], ps[:2]) == 7
+
+
+def test_oracle_bivariate_mul_matches_direct_sum(oracle_mod):
+    """The Kronecker-substitution bivariate product equals the direct double sum."""
+    p = 469762049
+    r = np.random.default_rng(5)
+    for (a, b), (c, d) in [((3, 3), (3, 3)), ((4, 7), (6, 2)), ((1, 9), (5, 1)), ((13, 11), (8, 17))]:
+        F = r.integers(0, p, (a, b)).astype(np.uint32)
+        G = r.integers(0, p, (c, d)).astype(np.uint32)
+        H = np.zeros((a + c - 1, b + d - 1), dtype=object)
+        for y in range(a):
+            for x in range(b):
+                H[y:y + c, x:x + d] += int(F[y, x]) * G.astype(object)
+        assert np.array_equal(oracle_mod.bivariate_mul(F, G, p), (H % p).astype(np.uint32))
+
+
+def test_oracle_subproduct_level_is_monic_product(oracle_mod):
+    p = 469762049
+    r = np.random.default_rng(9)
+    for l in (1, 2, 5, 16):
+        M = r.integers(0, p, 4 * l).astype(np.uint32)
+        out = oracle_mod.subproduct_level(M, l, p)
+        for j in range(2):
+            a = [int(v) for v in M[2 * j * l:(2 * j + 1) * l]] + [1]
+            b = [int(v) for v in M[(2 * j + 1) * l:(2 * j + 2) * l]] + [1]
+            h = [0] * (2 * l + 1)
+            for i, x in enumerate(a):
+                for k, y in enumerate(b):
+                    h[i + k] = (h[i + k] + x * y) % p
+            assert [int(v) for v in out[2 * j * l:(2 * j + 2) * l]] == h[:2 * l]
