@@ -532,8 +532,8 @@ def serving_c5(cm, rates=(1000, 3000, 10000, 30000, 100000), max_requests=20000,
     out = {}
     with cm.Server(max_batch=256, batch_window_us=50, lanes=4) as srv:
         # warm-up: tables for every prime and size class, lane buffers
-        warm = [(pool_u[:(1 << k) + 1], pool_u[:(1 << k) + 1], p) for p in primes for k in range(5, 21, 3)]
-        warm += [(pool_i[:(1 << k) + 1], pool_i[:(1 << k) + 1], None) for k in range(5, 15, 3)]
+        warm = [(pool_u[:(1 << k) + 1], pool_u[:(1 << k) + 1], p) for p in primes for k in range(4, 21)]
+        warm += [(pool_i[:(1 << k) + 1], pool_i[:(1 << k) + 1], None) for k in range(4, 15)]
         srv.replay(np.zeros(len(warm)), warm, threads=threads)
         for rate in rates:
             n = int(min(max_requests, rate * max_seconds))

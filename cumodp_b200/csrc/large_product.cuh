@@ -81,30 +81,52 @@ __device__ __forceinline__ u32 col_slot_to_k1(u32 s, const LevelPlan& PL, int L1
 }
 
 // ------------------------------------------------------ column tiles ----
-// A column CTA owns a tile of 32 adjacent columns x n1 rows, stored row-major
-// in shared memory (128 bytes per row).  The tile is loaded and stored with
-// 16-byte accesses by all threads at once, so every load of the tile is in
-// flight together; the levels then run on shared memory with lane = column
-// (conflict-free, and every twiddle is warp-uniform: a broadcast).
+// A column CTA owns a tile of TC = col_tile_cols(L1) adjacent columns x n1
+// rows, stored row-major in shared memory (tile_row gives a row's offset).
+// The tile is loaded and stored with 16-byte accesses by all threads at
+// once, so every load of the tile is in flight together; the levels then run
+// on shared memory with lane = column (32-column tiles) or half-warp = task,
+// lane % 16 = column (16-column tiles): conflict-free, and every twiddle is a
+// broadcast to the (half-)warp.
 
-// Bulk-loads rows [0, n1) x columns [c0, c0 + 32) of src (row stride n2),
+// Word offset of tile row r.
+template <int L1>
+__device__ __forceinline__ int tile_row(int r) {
+    constexpr int TC = col_tile_cols(L1);
+    if constexpr (TC == 32) return r * 32;
+    else return (r + (r >> col_pad_log(L1))) * TC;
+}
+
+// Bulk-loads rows [0, n1) x columns [c0, c0 + TC) of src (row stride n2),
 // zero beyond `len` elements, reducing every word to [0, 2p) when `reduce`.
 // Rows entirely inside `len` take a branch-free 16-byte path when src is
 // 16-byte aligned; only the boundary row checks elements one by one, and
 // rows entirely past `len` are zero-filled without loads.
-template <int L1, int T>
+// With ASYNC (and no reduction) the full rows are copied with cp.async,
+// global to shared without a register round trip.
+template <int L1, int T, bool ASYNC = false>
 __device__ __forceinline__ void tile_load(u32* tile, const u32* __restrict__ src, long long len, int c0, int n2,
                                           bool reduce, const PrimeK& pk) {
-    constexpr int n1 = 1 << L1;
-    constexpr int Q = n1 * 8;  // 16-byte quads in the tile
+    constexpr int n1 = 1 << L1, TC = col_tile_cols(L1), QR = TC / 4;
+    constexpr int Q = n1 * QR;  // 16-byte quads in the tile
     const bool vec = ((reinterpret_cast<uintptr_t>(src) & 15) == 0);
     // rows [0, rf) lie fully below len; rows [re, n1) fully at or above it
     const long long lc = len - c0;
-    const int rf = vec ? (int)(lc >= 32 ? min((long long)n1, (lc - 32) / n2 + 1) : 0) : 0;
+    const int rf = vec ? (int)(lc >= TC ? min((long long)n1, (lc - TC) / n2 + 1) : 0) : 0;
     const int re = (int)(lc > 0 ? min((long long)n1, (lc - 1) / n2 + 1) : 0);
+    if constexpr (ASYNC) {
 #pragma unroll 4
-    for (int idx = threadIdx.x; idx < rf * 8; idx += T) {
-        const int r = idx >> 3, q = idx & 7;
+        for (int idx = threadIdx.x; idx < rf * QR; idx += T) {
+            const int r = idx / QR, q = idx % QR;
+            const unsigned dst = (unsigned)__cvta_generic_to_shared(tile + tile_row<L1>(r) + 4 * q);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst),
+                         "l"(src + (long long)r * n2 + c0 + 4 * q) : "memory");
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < (ASYNC ? 0 : rf * QR); idx += T) {
+        const int r = idx / QR, q = idx % QR;
         uint4 v = __ldg(reinterpret_cast<const uint4*>(src + (long long)r * n2 + c0 + 4 * q));
         if (reduce) {
             v.x = mul_shoup(v.x, 1u, pk.one_q, pk.p);
@@ -112,10 +134,10 @@ __device__ __forceinline__ void tile_load(u32* tile, const u32* __restrict__ src
             v.z = mul_shoup(v.z, 1u, pk.one_q, pk.p);
             v.w = mul_shoup(v.w, 1u, pk.one_q, pk.p);
         }
-        *reinterpret_cast<uint4*>(tile + r * 32 + 4 * q) = v;
+        *reinterpret_cast<uint4*>(tile + tile_row<L1>(r) + 4 * q) = v;
     }
-    for (int idx = rf * 8 + threadIdx.x; idx < re * 8; idx += T) {
-        const int r = idx >> 3, q = idx & 7;
+    for (int idx = rf * QR + threadIdx.x; idx < re * QR; idx += T) {
+        const int r = idx / QR, q = idx % QR;
         const long long gi = (long long)r * n2 + c0 + 4 * q;
         uint4 v;
         v.x = gi < len ? __ldg(src + gi) : 0u;
@@ -128,25 +150,26 @@ __device__ __forceinline__ void tile_load(u32* tile, const u32* __restrict__ src
             v.z = mul_shoup(v.z, 1u, pk.one_q, pk.p);
             v.w = mul_shoup(v.w, 1u, pk.one_q, pk.p);
         }
-        *reinterpret_cast<uint4*>(tile + r * 32 + 4 * q) = v;
+        *reinterpret_cast<uint4*>(tile + tile_row<L1>(r) + 4 * q) = v;
     }
-    for (int idx = re * 8 + threadIdx.x; idx < Q; idx += T)
-        *reinterpret_cast<uint4*>(tile + (idx >> 3) * 32 + 4 * (idx & 7)) = make_uint4(0u, 0u, 0u, 0u);
+    for (int idx = re * QR + threadIdx.x; idx < Q; idx += T)
+        *reinterpret_cast<uint4*>(tile + tile_row<L1>(idx / QR) + 4 * (idx % QR)) = make_uint4(0u, 0u, 0u, 0u);
+    if constexpr (ASYNC) asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
 // Bulk-stores the tile; `final` reduces to [0, p) and stops at `len`.
 template <int L1, int T>
 __device__ __forceinline__ void tile_store(const u32* tile, u32* __restrict__ dst, long long len, int c0, int n2,
                                            bool final, const PrimeK& pk) {
-    constexpr int n1 = 1 << L1;
+    constexpr int n1 = 1 << L1, TC = col_tile_cols(L1), QR = TC / 4;
     const bool vec = ((reinterpret_cast<uintptr_t>(dst) & 15) == 0);
     const long long lc = len - c0;
-    const int rf = vec ? (int)(lc >= 32 ? min((long long)n1, (lc - 32) / n2 + 1) : 0) : 0;
+    const int rf = vec ? (int)(lc >= TC ? min((long long)n1, (lc - TC) / n2 + 1) : 0) : 0;
     const int re = (int)(lc > 0 ? min((long long)n1, (lc - 1) / n2 + 1) : 0);
 #pragma unroll 4
-    for (int idx = threadIdx.x; idx < rf * 8; idx += T) {
-        const int r = idx >> 3, q = idx & 7;
-        uint4 v = *reinterpret_cast<const uint4*>(tile + r * 32 + 4 * q);
+    for (int idx = threadIdx.x; idx < rf * QR; idx += T) {
+        const int r = idx / QR, q = idx % QR;
+        uint4 v = *reinterpret_cast<const uint4*>(tile + tile_row<L1>(r) + 4 * q);
         if (final) {
             v.x = red1(red2(v.x, pk.p2), pk.p);
             v.y = red1(red2(v.y, pk.p2), pk.p);
@@ -155,10 +178,10 @@ __device__ __forceinline__ void tile_store(const u32* tile, u32* __restrict__ ds
         }
         *reinterpret_cast<uint4*>(dst + (long long)r * n2 + c0 + 4 * q) = v;
     }
-    for (int idx = rf * 8 + threadIdx.x; idx < re * 8; idx += T) {
-        const int r = idx >> 3, q = idx & 7;
+    for (int idx = rf * QR + threadIdx.x; idx < re * QR; idx += T) {
+        const int r = idx / QR, q = idx % QR;
         const long long gi = (long long)r * n2 + c0 + 4 * q;
-        uint4 v = *reinterpret_cast<const uint4*>(tile + r * 32 + 4 * q);
+        uint4 v = *reinterpret_cast<const uint4*>(tile + tile_row<L1>(r) + 4 * q);
         if (final) {
             v.x = red1(red2(v.x, pk.p2), pk.p);
             v.y = red1(red2(v.y, pk.p2), pk.p);
@@ -180,25 +203,27 @@ __device__ __forceinline__ void col_fwd_level(u32* tile, const PrimeK& pk, const
     constexpr int R = LV::R, TB = LV::TB, B = LV::B;
     constexpr bool LAST = LEV + 1 == PL.nlev;
     constexpr int TASKS = (1 << L1) / R;
+    constexpr int TC = col_tile_cols(L1), SUB = 32 / TC;
     const u32 p = pk.p, p2 = pk.p2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int id = warp; id < TASKS; id += NW) {
+    const int col = lane % TC;
+    for (int id = warp * SUB + lane / TC; id < TASKS; id += NW * SUB) {
         const int blk = id / TB, o = id % TB;
         const int row0 = blk * B + o;
         u32 x[R];
 #pragma unroll
-        for (int m = 0; m < R; ++m) x[m] = tile[(row0 + TB * m) * 32 + lane];
+        for (int m = 0; m < R; ++m) x[m] = tile[tile_row<L1>(row0 + TB * m) + col];
         dif_regs<R, !LAST>(x, pk.rc.f, p, p2);
         if constexpr (!LAST) {
             const Tw* t = twc + LV::TWOFF + o * R;
 #pragma unroll
             for (int j = 1; j < R; ++j) {
-                const Tw w = t[j];  // uniform across the warp: broadcast
+                const Tw w = t[j];  // uniform across the (half-)warp: broadcast
                 x[j] = mul_shoup(x[j], w.w, w.wq, p);
             }
         }
 #pragma unroll
-        for (int m = 0; m < R; ++m) tile[(row0 + TB * m) * 32 + lane] = x[m];
+        for (int m = 0; m < R; ++m) tile[tile_row<L1>(row0 + TB * m) + col] = x[m];
     }
 }
 
@@ -220,14 +245,16 @@ __device__ __forceinline__ void col_inv_level(u32* tile, const PrimeK& pk, const
     constexpr int R = LV::R, TB = LV::TB, B = LV::B;
     constexpr bool DEEPEST = LEV + 1 == PL.nlev;
     constexpr int TASKS = (1 << L1) / R;
+    constexpr int TC = col_tile_cols(L1), SUB = 32 / TC;
     const u32 p = pk.p, p2 = pk.p2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int id = warp; id < TASKS; id += NW) {
+    const int col = lane % TC;
+    for (int id = warp * SUB + lane / TC; id < TASKS; id += NW * SUB) {
         const int blk = id / TB, o = id % TB;
         const int row0 = blk * B + o;
         u32 x[R];
 #pragma unroll
-        for (int m = 0; m < R; ++m) x[m] = tile[(row0 + TB * m) * 32 + lane];
+        for (int m = 0; m < R; ++m) x[m] = tile[tile_row<L1>(row0 + TB * m) + col];
         if constexpr (!DEEPEST) {
             const Tw* t = twci + LV::TWOFF + o * R;
 #pragma unroll
@@ -238,7 +265,7 @@ __device__ __forceinline__ void col_inv_level(u32* tile, const PrimeK& pk, const
         }
         dit_regs<R, !DEEPEST>(x, pk.rc.i, p, p2);
 #pragma unroll
-        for (int m = 0; m < R; ++m) tile[(row0 + TB * m) * 32 + lane] = x[m];
+        for (int m = 0; m < R; ++m) tile[tile_row<L1>(row0 + TB * m) + col] = x[m];
     }
 }
 
@@ -251,9 +278,9 @@ __device__ __forceinline__ void col_inv_levels(u32* tile, const PrimeK& pk, cons
     }
 }
 
-// pass A, grid: (n2/32 column tiles, operands, jobs)
+// pass A, grid: (n2/TC column tiles, operands, jobs)
 template <int L1, int NW>
-__global__ void __launch_bounds__(NW * 32, 1) k_col_fwd(const __grid_constant__ LargeArgs A) {
+__global__ void __launch_bounds__(NW * 32, col_ctas(L1)) k_col_fwd(const __grid_constant__ LargeArgs A) {
     extern __shared__ __align__(16) u32 tile[];
     const LargeJob& J = A.jobs ? A.jobs[blockIdx.z] : A.job0;
     const int op = blockIdx.y;
@@ -261,28 +288,29 @@ __global__ void __launch_bounds__(NW * 32, 1) k_col_fwd(const __grid_constant__ 
     const int len = op ? J.lb : J.la;
     u32* dst = op ? J.wb : J.wa;
     const int n2 = 1 << A.l2;
-    const int c0 = blockIdx.x * 32;
-    // the plan's twiddles (warp-uniform reads) next to the tile
+    const int c0 = blockIdx.x * col_tile_cols(L1);
+    // the plan's twiddles (broadcast reads) next to the tile
     constexpr int NTW = col_tw_entries(L1);
-    Tw* tws = reinterpret_cast<Tw*>(tile + (32 << L1));
+    Tw* tws = reinterpret_cast<Tw*>(tile + col_tile_words(L1));
     for (int i = threadIdx.x; i < NTW; i += NW * 32) tws[i] = A.twc[i];
+    // reduced while loaded (an input row half made of padding costs nothing)
     tile_load<L1, NW * 32>(tile, src, len, c0, n2, true, A.pkc);
     __syncthreads();
     col_fwd_levels<L1, 0, NW>(tile, A.pkc, tws);
     tile_store<L1, NW * 32>(tile, dst, 1ll << (L1 + A.l2), c0, n2, false, A.pkc);
 }
 
-// pass C, grid: (n2/32 column tiles, 1, jobs)
+// pass C, grid: (n2/TC column tiles, 1, jobs)
 template <int L1, int NW>
-__global__ void __launch_bounds__(NW * 32, 1) k_col_inv(const __grid_constant__ LargeArgs A) {
+__global__ void __launch_bounds__(NW * 32, col_ctas(L1)) k_col_inv(const __grid_constant__ LargeArgs A) {
     extern __shared__ __align__(16) u32 tile[];
     const LargeJob& J = A.jobs ? A.jobs[blockIdx.z] : A.job0;
     const int n2 = 1 << A.l2;
-    const int c0 = blockIdx.x * 32;
+    const int c0 = blockIdx.x * col_tile_cols(L1);
     constexpr int NTW = col_tw_entries(L1);
-    Tw* tws = reinterpret_cast<Tw*>(tile + (32 << L1));
+    Tw* tws = reinterpret_cast<Tw*>(tile + col_tile_words(L1));
     for (int i = threadIdx.x; i < NTW; i += NW * 32) tws[i] = A.twc[A.twc_inv + i];
-    tile_load<L1, NW * 32>(tile, J.wa, 1ll << (L1 + A.l2), c0, n2, false, A.pkc);
+    tile_load<L1, NW * 32, true>(tile, J.wa, 1ll << (L1 + A.l2), c0, n2, false, A.pkc);
     __syncthreads();
     col_inv_levels<L1, col_plan(L1).nlev - 1, NW>(tile, A.pkc, tws);
     tile_store<L1, NW * 32>(tile, J.h, J.lh, c0, n2, true, A.pkc);
@@ -345,8 +373,8 @@ __global__ void __launch_bounds__(row_threads(L2), 1) k_row_fused(const __grid_c
 #pragma unroll
         for (int m = 0; m < R0; ++m) {
             const u32 cm = mul_shoup(mo, bf[m].w, bf[m].wq, p);  // w^(k1 (o + TB0 m)) * 2^32
-            xf[m] = mul_mont(sm[swz(o + TB0 * m)], cm, p, pinv);
-            xg[m] = mul_mont(sm[swz(n2 + o + TB0 * m)], cm, p, pinv);
+            xf[m] = mul_mont(sm[swz_task<TB0, n2>(o, swz(o), m)], cm, p, pinv);
+            xg[m] = mul_mont(sm[swz_task<TB0, n2>(n2 + o, swz(n2 + o), m)], cm, p, pinv);
         }
         dif_regs<R0, true>(xf, A.pk.rc.f, p, p2);
         dif_regs<R0, true>(xg, A.pk.rc.f, p, p2);
@@ -359,8 +387,8 @@ __global__ void __launch_bounds__(row_threads(L2), 1) k_row_fused(const __grid_c
         }
 #pragma unroll
         for (int m = 0; m < R0; ++m) {
-            sm[swz(o + TB0 * m)] = xf[m];
-            sm[swz(n2 + o + TB0 * m)] = xg[m];
+            sm[swz_task<TB0, n2>(o, swz(o), m)] = xf[m];
+            sm[swz_task<TB0, n2>(n2 + o, swz(n2 + o), m)] = xg[m];
         }
     }
     __syncthreads();
@@ -398,7 +426,7 @@ __global__ void __launch_bounds__(row_threads(L2), 1) k_row_fused(const __grid_c
     for (int o = threadIdx.x; o < TB0; o += T) {
         u32 x[R0];
 #pragma unroll
-        for (int m = 0; m < R0; ++m) x[m] = sm[swz(o + TB0 * m)];
+        for (int m = 0; m < R0; ++m) x[m] = sm[swz_task<TB0, n2>(o, swz(o), m)];
         Tw t[R0];
         load_tw<R0>(t, A.twr + A.twr_inv + o * R0);
 #pragma unroll
@@ -442,13 +470,19 @@ __device__ __forceinline__ void row_slot_factors(const LargeArgs& A, u32 k1, Tw*
     }
 }
 
-// Loads one row into swizzled shared memory with 16-byte loads.
+// Loads one row into swizzled shared memory with 16-byte asynchronous
+// copies (cp.async: global to shared without a register round trip, all of
+// a thread's copies in flight at once); the caller's __syncthreads follows
+// the wait.
 template <int L2, int T>
 __device__ __forceinline__ void row_load(u32* sm, const u32* __restrict__ row) {
     constexpr int n2 = 1 << L2;
 #pragma unroll 8
-    for (int i = threadIdx.x * 4; i < n2; i += T * 4)
-        *reinterpret_cast<uint4*>(sm + swz(i)) = __ldg(reinterpret_cast<const uint4*>(row + i));
+    for (int i = threadIdx.x * 4; i < n2; i += T * 4) {
+        const unsigned dst = (unsigned)__cvta_generic_to_shared(sm + swz(i));
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(row + i) : "memory");
+    }
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
 // Level 0 forward of one operand with the inter-pass twiddle w_n^(k1 c).
@@ -465,12 +499,12 @@ __device__ __forceinline__ void row_level0_fwd(u32* sm, const LargeArgs& A, u32 
         u32 x[R0];
 #pragma unroll
         for (int m = 0; m < R0; ++m)
-            x[m] = mul_mont(sm[swz(o + TB0 * m)], mul_shoup(mo, bf[m].w, bf[m].wq, p), p, pinv);
+            x[m] = mul_mont(sm[swz_task<TB0, (1 << L2)>(o, swz(o), m)], mul_shoup(mo, bf[m].w, bf[m].wq, p), p, pinv);
         dif_regs<R0, true>(x, A.pk.rc.f, p, p2);
 #pragma unroll
         for (int j = 1; j < R0; ++j) x[j] = mul_shoup(x[j], t[j].w, t[j].wq, p);
 #pragma unroll
-        for (int m = 0; m < R0; ++m) sm[swz(o + TB0 * m)] = x[m];
+        for (int m = 0; m < R0; ++m) sm[swz_task<TB0, (1 << L2)>(o, swz(o), m)] = x[m];
     }
 }
 
@@ -550,7 +584,7 @@ __global__ void __launch_bounds__(rowsplit_threads(L2), rowsplit_ctas(L2)) k_row
     for (int o = threadIdx.x; o < TB0; o += T) {
         u32 x[R0];
 #pragma unroll
-        for (int m = 0; m < R0; ++m) x[m] = sm[swz(o + TB0 * m)];
+        for (int m = 0; m < R0; ++m) x[m] = sm[swz_task<TB0, n2>(o, swz(o), m)];
         Tw t[R0];
         load_tw<R0>(t, A.twr + A.twr_inv + o * R0);
 #pragma unroll

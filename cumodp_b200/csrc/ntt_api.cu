@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(small_threads(L2), 1) k_row_ntt(const __grid_c
 #pragma unroll
         for (int j = 1; j < R0; ++j) x[j] = mul_shoup(x[j], t[j].w, t[j].wq, p);
 #pragma unroll
-        for (int m = 0; m < R0; ++m) sm[swz(o + TB0 * m)] = x[m];
+        for (int m = 0; m < R0; ++m) sm[swz_task<TB0, n2>(o, swz(o), m)] = x[m];
     }
     __syncthreads();
     fwd1_levels<L2, 1, T>(sm, A.pk, A.twr);
@@ -171,10 +171,10 @@ void launch_colfwd1_t(const LargeArgs& a, int tiles, cudaStream_t st) {
     const size_t smem = col_smem_bytes(L1);
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_col_fwd<L1, (L1 == 10 ? 32 : 16)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_col_fwd<L1, col_warps(L1)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    k_col_fwd<L1, (L1 == 10 ? 32 : 16)><<<dim3(tiles, 1, 1), (L1 == 10 ? 32 : 16) * 32, smem, st>>>(a);
+    k_col_fwd<L1, col_warps(L1)><<<dim3(tiles, 1, 1), col_warps(L1) * 32, smem, st>>>(a);
 }
 typedef void (*ColFn)(const LargeArgs&, int, cudaStream_t);
 const ColFn kColFwd1[11] = {nullptr, launch_colfwd1_t<1>, launch_colfwd1_t<2>, launch_colfwd1_t<3>,
@@ -208,7 +208,7 @@ int column_pass(const PrimeCtx& pc, u32 root_c, int l1, int l2, const u32* src, 
     A.colpl = col_plan(l1);
     A.job0 = LargeJob{src, nullptr, nullptr, (int)std::min<long long>(len, 1ll << 30), 0, 0, 0, dst, nullptr};
     A.njobs = 1;
-    kColFwd1[l1](A, (1 << l2) / 32, st);
+    kColFwd1[l1](A, (1 << l2) / col_tile_cols_rt(l1), st);
     return OK;
 }
 

@@ -43,6 +43,19 @@ struct PrimeK {
 // consecutive 16/8/4-word groups) are both bank-conflict free.
 __device__ __forceinline__ int swz(int i) { return i ^ (((i >> 5) & 7) << 2); }
 
+// swz(base + TB * m) for the m-th element of a level task, where base is a
+// multiple of the block size B plus the task index o < TB, and m is an
+// unrolled constant.  With TB a multiple of 256 words the row bits that feed
+// the XOR do not change with m: the address is swz(base) + TB * m (an
+// immediate offset).  With TB = 32 and B a multiple of 256, base lies in a
+// row that is a multiple of 8, so the XOR is the constant (m & 7) << 2.
+template <int TB, int B>
+__device__ __forceinline__ int swz_task(int base, int bswz, int m) {
+    if constexpr (TB % 256 == 0) return bswz + TB * m;
+    else if constexpr (TB == 32 && B % 256 == 0) return (base ^ ((m & 7) << 2)) + 32 * m;
+    else return swz(base + TB * m);
+}
+
 // Forward R-point DIF on registers; x[j] ends holding X[bitrev_r(j)].
 // Inputs in [0, 2p).  Outputs in [0, 2p), except that with TW (the caller
 // multiplies every output j >= 1 by a Shoup twiddle next, which accepts any

@@ -53,8 +53,30 @@ __host__ __device__ constexpr int col_tw_entries(int logl) {
     for (int i = 0; i + 1 < pl.nlev; ++i) { n += 1 << lb; lb -= pl.logr[i]; }
     return n;
 }
-// Dynamic shared memory of a column CTA: the 32-column tile and its twiddles.
-__host__ __device__ constexpr int col_smem_bytes(int logl) { return (32 << logl) * 4 + col_tw_entries(logl) * 8; }
+// Column tiles: col_tile_cols adjacent columns x 2^logl rows in shared
+// memory, processed by col_warps warps, col_ctas resident CTAs per SM.
+// 32-column tiles put one column on each lane; 16-column tiles put two tasks
+// on each warp (one per half-warp) and insert a 16-word pad after every
+// 2^col_pad_log rows (the plan's last radix), so that the two half-warps
+// always read opposite halves of the banks.
+__host__ __device__ constexpr int col_tile_cols(int logl) { return 32; }
+__host__ __device__ constexpr int col_warps(int logl) { return logl == 10 ? 32 : 16; }
+__host__ __device__ constexpr int col_ctas(int logl) { return 1; }
+__host__ __device__ constexpr int col_pad_log(int logl) { return col_plan(logl).logr[col_plan(logl).nlev - 1]; }
+__host__ __device__ constexpr int col_tile_words(int logl) {
+    return col_tile_cols(logl) == 32 ? (32 << logl)
+                                     : ((1 << logl) + ((1 << logl) >> col_pad_log(logl))) * col_tile_cols(logl);
+}
+// col_tile_cols for a run-time logl.
+__host__ __device__ inline int col_tile_cols_rt(int logl) {
+    constexpr int t[13] = {col_tile_cols(0), col_tile_cols(1), col_tile_cols(2), col_tile_cols(3),
+                           col_tile_cols(4), col_tile_cols(5), col_tile_cols(6), col_tile_cols(7),
+                           col_tile_cols(8), col_tile_cols(9), col_tile_cols(10), col_tile_cols(11),
+                           col_tile_cols(12)};
+    return t[logl];
+}
+// Dynamic shared memory of a column CTA: the tile and its twiddles.
+__host__ __device__ constexpr int col_smem_bytes(int logl) { return col_tile_words(logl) * 4 + col_tw_entries(logl) * 8; }
 
 // Threads of the three-pass row kernel: 2^14-word rows use 1024 threads with
 // at most 64 registers each (32 warps per SM; the plan's twiddled levels

@@ -636,9 +636,10 @@ cumodp_server* cumodp_server_create(const cumodp_server_config* cfg) {
     Server* S = new Server(c);
     S->lanes.resize(c.lanes);
     for (Lane& L : S->lanes) recreate_lane(L);
-    // pinned slabs: up to host_budget, the first 1 GiB pinned now
-    S->pool.set_limit(c.host_budget ? c.host_budget : (8ull << 30));
-    S->pool.reserve(1ull << 30);
+    // pinned slabs: the whole host budget is pinned now, so that serving never
+    // calls cudaHostAlloc (slow, and it stalls other CUDA calls)
+    S->pool.set_limit(c.host_budget ? c.host_budget : (2ull << 30));
+    S->pool.reserve(S->pool.limit);
     S->batcher = std::thread(batcher_loop, S);
     S->completer = std::thread(completer_loop, S);
     return (cumodp_server*)S;

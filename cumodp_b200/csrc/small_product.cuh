@@ -75,11 +75,12 @@ __device__ __forceinline__ void small_fwd_level(u32* sm, const Ctx& A) {
         const int rest = id % (L / R);
         const int blk = rest / TB, o = rest % TB;
         const int base = q * 2 * L + blk * B + o;
+        const int bs = swz(base), bsg = swz(base + L);
         u32 xf[R], xg[R];
 #pragma unroll
         for (int m = 0; m < R; ++m) {
-            xf[m] = sm[swz(base + TB * m)];
-            xg[m] = sm[swz(base + L + TB * m)];
+            xf[m] = sm[swz_task<TB, B>(base, bs, m)];
+            xg[m] = sm[swz_task<TB, B>(base + L, bsg, m)];
         }
         dif_regs<R, true>(xf, A.pk.rc.f, p, p2);
         dif_regs<R, true>(xg, A.pk.rc.f, p, p2);
@@ -92,8 +93,8 @@ __device__ __forceinline__ void small_fwd_level(u32* sm, const Ctx& A) {
         }
 #pragma unroll
         for (int m = 0; m < R; ++m) {
-            sm[swz(base + TB * m)] = xf[m];
-            sm[swz(base + L + TB * m)] = xg[m];
+            sm[swz_task<TB, B>(base, bs, m)] = xf[m];
+            sm[swz_task<TB, B>(base + L, bsg, m)] = xg[m];
         }
     }
 }
@@ -110,16 +111,17 @@ __device__ __forceinline__ void small_inv_level(u32* sm, const Ctx& A) {
         const int rest = id % (L / R);
         const int blk = rest / TB, o = rest % TB;
         const int base = q * 2 * L + blk * B + o;
+        const int bs = swz(base);
         u32 x[R];
 #pragma unroll
-        for (int m = 0; m < R; ++m) x[m] = sm[swz(base + TB * m)];
+        for (int m = 0; m < R; ++m) x[m] = sm[swz_task<TB, B>(base, bs, m)];
         Tw t[R];
         load_tw<R>(t, A.tw + A.tw_inv_off + LV::TWOFF + o * R);
 #pragma unroll
         for (int j = 1; j < R; ++j) x[j] = mul_shoup(x[j], t[j].w, t[j].wq, p);
         dit_regs<R, true>(x, A.pk.rc.i, p, p2);
 #pragma unroll
-        for (int m = 0; m < R; ++m) sm[swz(base + TB * m)] = x[m];
+        for (int m = 0; m < R; ++m) sm[swz_task<TB, B>(base, bs, m)] = x[m];
     }
 }
 
@@ -153,16 +155,17 @@ __device__ __forceinline__ void fwd1_level(u32* sm, const PrimeK& pk, const Tw* 
     for (int id = threadIdx.x; id < L / R; id += T) {
         const int blk = id / TB, o = id % TB;
         const int base = blk * B + o;
+        const int bs = swz(base);
         u32 x[R];
 #pragma unroll
-        for (int m = 0; m < R; ++m) x[m] = sm[swz(base + TB * m)];
+        for (int m = 0; m < R; ++m) x[m] = sm[swz_task<TB, B>(base, bs, m)];
         dif_regs<R, true>(x, pk.rc.f, p, p2);
         Tw t[R];
         load_tw<R>(t, tw + LV::TWOFF + o * R);
 #pragma unroll
         for (int j = 1; j < R; ++j) x[j] = mul_shoup(x[j], t[j].w, t[j].wq, p);
 #pragma unroll
-        for (int m = 0; m < R; ++m) sm[swz(base + TB * m)] = x[m];
+        for (int m = 0; m < R; ++m) sm[swz_task<TB, B>(base, bs, m)] = x[m];
     }
 }
 

@@ -215,10 +215,9 @@ typedef struct {
     int lanes;               /* batches in flight at once (default 4) */
     int inject_fault_batch;  /* tests: the n-th batch fails on the host before launching (0 = off) */
     size_t host_budget;      /* pinned host memory for the operand and result slabs of unfinished
-                                requests (power-of-two slabs carved from pinned chunks; 1 GiB is
-                                pinned at creation, the rest on demand); a submission that finds
-                                no room completes at once with CUMODP_OUT_OF_MEMORY (load
-                                shedding).  0 = 8 GiB */
+                                requests (power-of-two slabs carved from chunks pinned when the
+                                server is created); a submission that finds no room completes at
+                                once with CUMODP_OUT_OF_MEMORY (load shedding).  0 = 2 GiB */
 } cumodp_server_config;
 typedef struct {
     long long completed, failed, batches, pending;
