@@ -81,7 +81,7 @@ __device__ __forceinline__ u32 col_slot_to_k1(u32 s, const LevelPlan& PL, int L1
 }
 
 // ------------------------------------------------------ column tiles ----
-// A column CTA owns a tile of TC = col_tile_cols(L1) adjacent columns x n1
+// A column CTA owns a tile of TC = col_tile_cols(L1, INV) adjacent columns x n1
 // rows, stored row-major in shared memory (tile_row gives a row's offset).
 // The tile is loaded and stored with 16-byte accesses by all threads at
 // once, so every load of the tile is in flight together; the levels then run
@@ -90,9 +90,9 @@ __device__ __forceinline__ u32 col_slot_to_k1(u32 s, const LevelPlan& PL, int L1
 // broadcast to the (half-)warp.
 
 // Word offset of tile row r.
-template <int L1>
+template <int L1, bool INV>
 __device__ __forceinline__ int tile_row(int r) {
-    constexpr int TC = col_tile_cols(L1);
+    constexpr int TC = col_tile_cols(L1, INV);
     if constexpr (TC == 32) return r * 32;
     else return (r + (r >> col_pad_log(L1))) * TC;
 }
@@ -104,10 +104,10 @@ __device__ __forceinline__ int tile_row(int r) {
 // rows entirely past `len` are zero-filled without loads.
 // With ASYNC (and no reduction) the full rows are copied with cp.async,
 // global to shared without a register round trip.
-template <int L1, int T, bool ASYNC = false>
+template <int L1, bool INV, int T, bool ASYNC = false>
 __device__ __forceinline__ void tile_load(u32* tile, const u32* __restrict__ src, long long len, int c0, int n2,
                                           bool reduce, const PrimeK& pk) {
-    constexpr int n1 = 1 << L1, TC = col_tile_cols(L1), QR = TC / 4;
+    constexpr int n1 = 1 << L1, TC = col_tile_cols(L1, INV), QR = TC / 4;
     constexpr int Q = n1 * QR;  // 16-byte quads in the tile
     const bool vec = ((reinterpret_cast<uintptr_t>(src) & 15) == 0);
     // rows [0, rf) lie fully below len; rows [re, n1) fully at or above it
@@ -118,7 +118,7 @@ __device__ __forceinline__ void tile_load(u32* tile, const u32* __restrict__ src
 #pragma unroll 4
         for (int idx = threadIdx.x; idx < rf * QR; idx += T) {
             const int r = idx / QR, q = idx % QR;
-            const unsigned dst = (unsigned)__cvta_generic_to_shared(tile + tile_row<L1>(r) + 4 * q);
+            const unsigned dst = (unsigned)__cvta_generic_to_shared(tile + tile_row<L1, INV>(r) + 4 * q);
             asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst),
                          "l"(src + (long long)r * n2 + c0 + 4 * q) : "memory");
         }
@@ -134,7 +134,7 @@ __device__ __forceinline__ void tile_load(u32* tile, const u32* __restrict__ src
             v.z = mul_shoup(v.z, 1u, pk.one_q, pk.p);
             v.w = mul_shoup(v.w, 1u, pk.one_q, pk.p);
         }
-        *reinterpret_cast<uint4*>(tile + tile_row<L1>(r) + 4 * q) = v;
+        *reinterpret_cast<uint4*>(tile + tile_row<L1, INV>(r) + 4 * q) = v;
     }
     for (int idx = rf * QR + threadIdx.x; idx < re * QR; idx += T) {
         const int r = idx / QR, q = idx % QR;
@@ -150,18 +150,18 @@ __device__ __forceinline__ void tile_load(u32* tile, const u32* __restrict__ src
             v.z = mul_shoup(v.z, 1u, pk.one_q, pk.p);
             v.w = mul_shoup(v.w, 1u, pk.one_q, pk.p);
         }
-        *reinterpret_cast<uint4*>(tile + tile_row<L1>(r) + 4 * q) = v;
+        *reinterpret_cast<uint4*>(tile + tile_row<L1, INV>(r) + 4 * q) = v;
     }
     for (int idx = re * QR + threadIdx.x; idx < Q; idx += T)
-        *reinterpret_cast<uint4*>(tile + tile_row<L1>(idx / QR) + 4 * (idx % QR)) = make_uint4(0u, 0u, 0u, 0u);
+        *reinterpret_cast<uint4*>(tile + tile_row<L1, INV>(idx / QR) + 4 * (idx % QR)) = make_uint4(0u, 0u, 0u, 0u);
     if constexpr (ASYNC) asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
 // Bulk-stores the tile; `final` reduces to [0, p) and stops at `len`.
-template <int L1, int T>
+template <int L1, bool INV, int T>
 __device__ __forceinline__ void tile_store(const u32* tile, u32* __restrict__ dst, long long len, int c0, int n2,
                                            bool final, const PrimeK& pk) {
-    constexpr int n1 = 1 << L1, TC = col_tile_cols(L1), QR = TC / 4;
+    constexpr int n1 = 1 << L1, TC = col_tile_cols(L1, INV), QR = TC / 4;
     const bool vec = ((reinterpret_cast<uintptr_t>(dst) & 15) == 0);
     const long long lc = len - c0;
     const int rf = vec ? (int)(lc >= TC ? min((long long)n1, (lc - TC) / n2 + 1) : 0) : 0;
@@ -169,7 +169,7 @@ __device__ __forceinline__ void tile_store(const u32* tile, u32* __restrict__ ds
 #pragma unroll 4
     for (int idx = threadIdx.x; idx < rf * QR; idx += T) {
         const int r = idx / QR, q = idx % QR;
-        uint4 v = *reinterpret_cast<const uint4*>(tile + tile_row<L1>(r) + 4 * q);
+        uint4 v = *reinterpret_cast<const uint4*>(tile + tile_row<L1, INV>(r) + 4 * q);
         if (final) {
             v.x = red1(red2(v.x, pk.p2), pk.p);
             v.y = red1(red2(v.y, pk.p2), pk.p);
@@ -181,7 +181,7 @@ __device__ __forceinline__ void tile_store(const u32* tile, u32* __restrict__ ds
     for (int idx = rf * QR + threadIdx.x; idx < re * QR; idx += T) {
         const int r = idx / QR, q = idx % QR;
         const long long gi = (long long)r * n2 + c0 + 4 * q;
-        uint4 v = *reinterpret_cast<const uint4*>(tile + tile_row<L1>(r) + 4 * q);
+        uint4 v = *reinterpret_cast<const uint4*>(tile + tile_row<L1, INV>(r) + 4 * q);
         if (final) {
             v.x = red1(red2(v.x, pk.p2), pk.p);
             v.y = red1(red2(v.y, pk.p2), pk.p);
@@ -203,7 +203,8 @@ __device__ __forceinline__ void col_fwd_level(u32* tile, const PrimeK& pk, const
     constexpr int R = LV::R, TB = LV::TB, B = LV::B;
     constexpr bool LAST = LEV + 1 == PL.nlev;
     constexpr int TASKS = (1 << L1) / R;
-    constexpr int TC = col_tile_cols(L1), SUB = 32 / TC;
+    constexpr bool INV = false;
+    constexpr int TC = col_tile_cols(L1, INV), SUB = 32 / TC;
     const u32 p = pk.p, p2 = pk.p2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int col = lane % TC;
@@ -212,7 +213,7 @@ __device__ __forceinline__ void col_fwd_level(u32* tile, const PrimeK& pk, const
         const int row0 = blk * B + o;
         u32 x[R];
 #pragma unroll
-        for (int m = 0; m < R; ++m) x[m] = tile[tile_row<L1>(row0 + TB * m) + col];
+        for (int m = 0; m < R; ++m) x[m] = tile[tile_row<L1, INV>(row0 + TB * m) + col];
         dif_regs<R, !LAST>(x, pk.rc.f, p, p2);
         if constexpr (!LAST) {
             const Tw* t = twc + LV::TWOFF + o * R;
@@ -223,7 +224,7 @@ __device__ __forceinline__ void col_fwd_level(u32* tile, const PrimeK& pk, const
             }
         }
 #pragma unroll
-        for (int m = 0; m < R; ++m) tile[tile_row<L1>(row0 + TB * m) + col] = x[m];
+        for (int m = 0; m < R; ++m) tile[tile_row<L1, INV>(row0 + TB * m) + col] = x[m];
     }
 }
 
@@ -245,7 +246,8 @@ __device__ __forceinline__ void col_inv_level(u32* tile, const PrimeK& pk, const
     constexpr int R = LV::R, TB = LV::TB, B = LV::B;
     constexpr bool DEEPEST = LEV + 1 == PL.nlev;
     constexpr int TASKS = (1 << L1) / R;
-    constexpr int TC = col_tile_cols(L1), SUB = 32 / TC;
+    constexpr bool INV = true;
+    constexpr int TC = col_tile_cols(L1, INV), SUB = 32 / TC;
     const u32 p = pk.p, p2 = pk.p2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int col = lane % TC;
@@ -254,7 +256,7 @@ __device__ __forceinline__ void col_inv_level(u32* tile, const PrimeK& pk, const
         const int row0 = blk * B + o;
         u32 x[R];
 #pragma unroll
-        for (int m = 0; m < R; ++m) x[m] = tile[tile_row<L1>(row0 + TB * m) + col];
+        for (int m = 0; m < R; ++m) x[m] = tile[tile_row<L1, INV>(row0 + TB * m) + col];
         if constexpr (!DEEPEST) {
             const Tw* t = twci + LV::TWOFF + o * R;
 #pragma unroll
@@ -265,7 +267,7 @@ __device__ __forceinline__ void col_inv_level(u32* tile, const PrimeK& pk, const
         }
         dit_regs<R, !DEEPEST>(x, pk.rc.i, p, p2);
 #pragma unroll
-        for (int m = 0; m < R; ++m) tile[tile_row<L1>(row0 + TB * m) + col] = x[m];
+        for (int m = 0; m < R; ++m) tile[tile_row<L1, INV>(row0 + TB * m) + col] = x[m];
     }
 }
 
@@ -280,7 +282,7 @@ __device__ __forceinline__ void col_inv_levels(u32* tile, const PrimeK& pk, cons
 
 // pass A, grid: (n2/TC column tiles, operands, jobs)
 template <int L1, int NW>
-__global__ void __launch_bounds__(NW * 32, col_ctas(L1)) k_col_fwd(const __grid_constant__ LargeArgs A) {
+__global__ void __launch_bounds__(NW * 32, col_ctas(L1, false)) k_col_fwd(const __grid_constant__ LargeArgs A) {
     extern __shared__ __align__(16) u32 tile[];
     const LargeJob& J = A.jobs ? A.jobs[blockIdx.z] : A.job0;
     const int op = blockIdx.y;
@@ -288,32 +290,32 @@ __global__ void __launch_bounds__(NW * 32, col_ctas(L1)) k_col_fwd(const __grid_
     const int len = op ? J.lb : J.la;
     u32* dst = op ? J.wb : J.wa;
     const int n2 = 1 << A.l2;
-    const int c0 = blockIdx.x * col_tile_cols(L1);
+    const int c0 = blockIdx.x * col_tile_cols(L1, false);
     // the plan's twiddles (broadcast reads) next to the tile
     constexpr int NTW = col_tw_entries(L1);
-    Tw* tws = reinterpret_cast<Tw*>(tile + col_tile_words(L1));
+    Tw* tws = reinterpret_cast<Tw*>(tile + col_tile_words(L1, false));
     for (int i = threadIdx.x; i < NTW; i += NW * 32) tws[i] = A.twc[i];
     // reduced while loaded (an input row half made of padding costs nothing)
-    tile_load<L1, NW * 32>(tile, src, len, c0, n2, true, A.pkc);
+    tile_load<L1, false, NW * 32>(tile, src, len, c0, n2, true, A.pkc);
     __syncthreads();
     col_fwd_levels<L1, 0, NW>(tile, A.pkc, tws);
-    tile_store<L1, NW * 32>(tile, dst, 1ll << (L1 + A.l2), c0, n2, false, A.pkc);
+    tile_store<L1, false, NW * 32>(tile, dst, 1ll << (L1 + A.l2), c0, n2, false, A.pkc);
 }
 
 // pass C, grid: (n2/TC column tiles, 1, jobs)
 template <int L1, int NW>
-__global__ void __launch_bounds__(NW * 32, col_ctas(L1)) k_col_inv(const __grid_constant__ LargeArgs A) {
+__global__ void __launch_bounds__(NW * 32, col_ctas(L1, true)) k_col_inv(const __grid_constant__ LargeArgs A) {
     extern __shared__ __align__(16) u32 tile[];
     const LargeJob& J = A.jobs ? A.jobs[blockIdx.z] : A.job0;
     const int n2 = 1 << A.l2;
-    const int c0 = blockIdx.x * col_tile_cols(L1);
+    const int c0 = blockIdx.x * col_tile_cols(L1, true);
     constexpr int NTW = col_tw_entries(L1);
-    Tw* tws = reinterpret_cast<Tw*>(tile + col_tile_words(L1));
+    Tw* tws = reinterpret_cast<Tw*>(tile + col_tile_words(L1, true));
     for (int i = threadIdx.x; i < NTW; i += NW * 32) tws[i] = A.twc[A.twc_inv + i];
-    tile_load<L1, NW * 32, true>(tile, J.wa, 1ll << (L1 + A.l2), c0, n2, false, A.pkc);
+    tile_load<L1, true, NW * 32, true>(tile, J.wa, 1ll << (L1 + A.l2), c0, n2, false, A.pkc);
     __syncthreads();
     col_inv_levels<L1, col_plan(L1).nlev - 1, NW>(tile, A.pkc, tws);
-    tile_store<L1, NW * 32>(tile, J.h, J.lh, c0, n2, true, A.pkc);
+    tile_store<L1, true, NW * 32>(tile, J.h, J.lh, c0, n2, true, A.pkc);
 }
 
 // ------------------------------------------------------------- pass B ----

@@ -54,29 +54,41 @@ __host__ __device__ constexpr int col_tw_entries(int logl) {
     return n;
 }
 // Column tiles: col_tile_cols adjacent columns x 2^logl rows in shared
-// memory, processed by col_warps warps, col_ctas resident CTAs per SM.
-// 32-column tiles put one column on each lane; 16-column tiles put two tasks
-// on each warp (one per half-warp) and insert a 16-word pad after every
-// 2^col_pad_log rows (the plan's last radix), so that the two half-warps
-// always read opposite halves of the banks.
-__host__ __device__ constexpr int col_tile_cols(int logl) { return 32; }
-__host__ __device__ constexpr int col_warps(int logl) { return logl == 10 ? 32 : 16; }
-__host__ __device__ constexpr int col_ctas(int logl) { return 1; }
+// memory, processed by col_warps warps, col_ctas resident CTAs per SM, each
+// chosen per direction (inv: the inverse column pass).  32-column tiles put
+// one column on each lane; 16-column tiles put two tasks on each warp (one
+// per half-warp) and insert a 16-word pad after every 2^col_pad_log rows (the
+// plan's last radix), so that the two half-warps always read opposite halves
+// of the banks.  The inverse pass over 2^10-row tiles uses 16 columns and
+// two CTAs per SM (their load, compute and store phases overlap); the
+// forward pass keeps 32 columns (its loads skip the zero-padded half).
+__host__ __device__ constexpr int col_tile_cols(int logl, bool inv) { return inv && logl == 10 ? 16 : 32; }
+__host__ __device__ constexpr int col_warps(int logl, bool inv) { return logl == 10 && !inv ? 32 : 16; }
+__host__ __device__ constexpr int col_ctas(int logl, bool inv) { return inv && logl == 10 ? 2 : 1; }
 __host__ __device__ constexpr int col_pad_log(int logl) { return col_plan(logl).logr[col_plan(logl).nlev - 1]; }
-__host__ __device__ constexpr int col_tile_words(int logl) {
-    return col_tile_cols(logl) == 32 ? (32 << logl)
-                                     : ((1 << logl) + ((1 << logl) >> col_pad_log(logl))) * col_tile_cols(logl);
+__host__ __device__ constexpr int col_tile_words(int logl, bool inv) {
+    return col_tile_cols(logl, inv) == 32
+               ? (32 << logl)
+               : ((1 << logl) + ((1 << logl) >> col_pad_log(logl))) * col_tile_cols(logl, inv);
 }
 // col_tile_cols for a run-time logl.
-__host__ __device__ inline int col_tile_cols_rt(int logl) {
-    constexpr int t[13] = {col_tile_cols(0), col_tile_cols(1), col_tile_cols(2), col_tile_cols(3),
-                           col_tile_cols(4), col_tile_cols(5), col_tile_cols(6), col_tile_cols(7),
-                           col_tile_cols(8), col_tile_cols(9), col_tile_cols(10), col_tile_cols(11),
-                           col_tile_cols(12)};
-    return t[logl];
+__host__ __device__ inline int col_tile_cols_rt(int logl, bool inv) {
+    constexpr int f[13] = {col_tile_cols(0, false), col_tile_cols(1, false), col_tile_cols(2, false),
+                           col_tile_cols(3, false), col_tile_cols(4, false), col_tile_cols(5, false),
+                           col_tile_cols(6, false), col_tile_cols(7, false), col_tile_cols(8, false),
+                           col_tile_cols(9, false), col_tile_cols(10, false), col_tile_cols(11, false),
+                           col_tile_cols(12, false)};
+    constexpr int i[13] = {col_tile_cols(0, true), col_tile_cols(1, true), col_tile_cols(2, true),
+                           col_tile_cols(3, true), col_tile_cols(4, true), col_tile_cols(5, true),
+                           col_tile_cols(6, true), col_tile_cols(7, true), col_tile_cols(8, true),
+                           col_tile_cols(9, true), col_tile_cols(10, true), col_tile_cols(11, true),
+                           col_tile_cols(12, true)};
+    return inv ? i[logl] : f[logl];
 }
 // Dynamic shared memory of a column CTA: the tile and its twiddles.
-__host__ __device__ constexpr int col_smem_bytes(int logl) { return col_tile_words(logl) * 4 + col_tw_entries(logl) * 8; }
+__host__ __device__ constexpr int col_smem_bytes(int logl, bool inv) {
+    return col_tile_words(logl, inv) * 4 + col_tw_entries(logl) * 8;
+}
 
 // Threads of the three-pass row kernel: 2^14-word rows use 1024 threads with
 // at most 64 registers each (32 warps per SM; the plan's twiddled levels

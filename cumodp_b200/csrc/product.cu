@@ -31,23 +31,23 @@ const SmallFn kSmall[15] = {nullptr, nullptr, nullptr, nullptr, nullptr,
 
 template <int L1>
 void launch_col_fwd_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
-    const size_t smem = col_smem_bytes(L1);
+    const size_t smem = col_smem_bytes(L1, false);
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_col_fwd<L1, col_warps(L1)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_col_fwd<L1, col_warps(L1, false)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    k_col_fwd<L1, col_warps(L1)><<<grid, col_warps(L1) * 32, smem, st>>>(a);
+    k_col_fwd<L1, col_warps(L1, false)><<<grid, col_warps(L1, false) * 32, smem, st>>>(a);
 }
 template <int L1>
 void launch_col_inv_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
-    const size_t smem = col_smem_bytes(L1);
+    const size_t smem = col_smem_bytes(L1, true);
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_col_inv<L1, col_warps(L1)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_col_inv<L1, col_warps(L1, true)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    k_col_inv<L1, col_warps(L1)><<<grid, col_warps(L1) * 32, smem, st>>>(a);
+    k_col_inv<L1, col_warps(L1, true)><<<grid, col_warps(L1, true) * 32, smem, st>>>(a);
 }
 template <int L2>
 void launch_row_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
@@ -90,9 +90,10 @@ void attr_small() {
 }
 template <int L1>
 void attr_col() {
-    const int smem = col_smem_bytes(L1);
-    cudaFuncSetAttribute(k_col_fwd<L1, col_warps(L1)>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(k_col_inv<L1, col_warps(L1)>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_col_fwd<L1, col_warps(L1, false)>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         col_smem_bytes(L1, false));
+    cudaFuncSetAttribute(k_col_inv<L1, col_warps(L1, true)>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         col_smem_bytes(L1, true));
 }
 template <int L2>
 void attr_row() {
@@ -223,7 +224,7 @@ void launch_large(const LargeArgs& a, int njobs, cudaStream_t st) {
     const int n1 = 1 << a.l1, n2 = 1 << a.l2;
     cudaEvent_t e0;
     bool tr = pass_timing_begin(st, &e0);
-    kColFwd[a.l1](a, dim3(n2 / col_tile_cols_rt(a.l1), 2, njobs), st);
+    kColFwd[a.l1](a, dim3(n2 / col_tile_cols_rt(a.l1, false), 2, njobs), st);
     if (tr) pass_timing_end(st, kColFwdName[a.l1], e0);
     if (a.row_fused) {
         tr = pass_timing_begin(st, &e0);
@@ -238,7 +239,7 @@ void launch_large(const LargeArgs& a, int njobs, cudaStream_t st) {
         if (tr) pass_timing_end(st, kRowFName[a.l2], e0);
     }
     tr = pass_timing_begin(st, &e0);
-    kColInv[a.l1](a, dim3(n2 / col_tile_cols_rt(a.l1), 1, njobs), st);
+    kColInv[a.l1](a, dim3(n2 / col_tile_cols_rt(a.l1, true), 1, njobs), st);
     if (tr) pass_timing_end(st, kColInvName[a.l1], e0);
 }
 
