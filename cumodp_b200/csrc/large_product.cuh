@@ -97,6 +97,19 @@ __device__ __forceinline__ int tile_row(int r) {
     else return (r + (r >> col_pad_log(L1))) * TC;
 }
 
+// tile_row(row0 + TB * m) - tile_row(row0) for element m of a level task
+// with TB rows between its elements (row0 = a multiple of the block size plus
+// the task index): a constant.  Every non-last level of a column plan has TB
+// a multiple of the padding period; the last level has TB = 1 and blocks of
+// exactly one period.
+template <int L1, bool INV, int TB>
+__device__ __forceinline__ constexpr int tile_step(int m) {
+    constexpr int TC = col_tile_cols(L1, INV), PAD = 1 << col_pad_log(L1);
+    if constexpr (TC == 32) return TB * m * 32;
+    else if constexpr (TB % PAD == 0) return TB * m * TC + (TB / PAD) * m * TC;
+    else return m * TC;
+}
+
 // Bulk-loads rows [0, n1) x columns [c0, c0 + TC) of src (row stride n2),
 // zero beyond `len` elements, reducing every word to [0, 2p) when `reduce`.
 // Rows entirely inside `len` take a branch-free 16-byte path when src is
@@ -212,8 +225,9 @@ __device__ __forceinline__ void col_fwd_level(u32* tile, const PrimeK& pk, const
         const int blk = id / TB, o = id % TB;
         const int row0 = blk * B + o;
         u32 x[R];
+        u32* base = tile + tile_row<L1, INV>(row0) + col;
 #pragma unroll
-        for (int m = 0; m < R; ++m) x[m] = tile[tile_row<L1, INV>(row0 + TB * m) + col];
+        for (int m = 0; m < R; ++m) x[m] = base[tile_step<L1, INV, TB>(m)];
         dif_regs<R, !LAST>(x, pk.rc.f, p, p2);
         if constexpr (!LAST) {
             const Tw* t = twc + LV::TWOFF + o * R;
@@ -224,7 +238,7 @@ __device__ __forceinline__ void col_fwd_level(u32* tile, const PrimeK& pk, const
             }
         }
 #pragma unroll
-        for (int m = 0; m < R; ++m) tile[tile_row<L1, INV>(row0 + TB * m) + col] = x[m];
+        for (int m = 0; m < R; ++m) base[tile_step<L1, INV, TB>(m)] = x[m];
     }
 }
 
@@ -255,8 +269,9 @@ __device__ __forceinline__ void col_inv_level(u32* tile, const PrimeK& pk, const
         const int blk = id / TB, o = id % TB;
         const int row0 = blk * B + o;
         u32 x[R];
+        u32* base = tile + tile_row<L1, INV>(row0) + col;
 #pragma unroll
-        for (int m = 0; m < R; ++m) x[m] = tile[tile_row<L1, INV>(row0 + TB * m) + col];
+        for (int m = 0; m < R; ++m) x[m] = base[tile_step<L1, INV, TB>(m)];
         if constexpr (!DEEPEST) {
             const Tw* t = twci + LV::TWOFF + o * R;
 #pragma unroll
@@ -267,7 +282,7 @@ __device__ __forceinline__ void col_inv_level(u32* tile, const PrimeK& pk, const
         }
         dit_regs<R, !DEEPEST>(x, pk.rc.i, p, p2);
 #pragma unroll
-        for (int m = 0; m < R; ++m) tile[tile_row<L1, INV>(row0 + TB * m) + col] = x[m];
+        for (int m = 0; m < R; ++m) base[tile_step<L1, INV, TB>(m)] = x[m];
     }
 }
 

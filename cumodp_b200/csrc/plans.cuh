@@ -71,6 +71,9 @@ __host__ __device__ constexpr int col_tile_words(int logl, bool inv) {
                ? (32 << logl)
                : ((1 << logl) + ((1 << logl) >> col_pad_log(logl))) * col_tile_cols(logl, inv);
 }
+// Whether a column CTA stages its twiddles in shared memory next to the
+// tile (else the levels read them from global memory, as broadcasts).
+__host__ __device__ constexpr bool col_tw_smem(int logl, bool inv) { return true; }
 // col_tile_cols for a run-time logl.
 __host__ __device__ inline int col_tile_cols_rt(int logl, bool inv) {
     constexpr int f[13] = {col_tile_cols(0, false), col_tile_cols(1, false), col_tile_cols(2, false),
@@ -87,7 +90,7 @@ __host__ __device__ inline int col_tile_cols_rt(int logl, bool inv) {
 }
 // Dynamic shared memory of a column CTA: the tile and its twiddles.
 __host__ __device__ constexpr int col_smem_bytes(int logl, bool inv) {
-    return col_tile_words(logl, inv) * 4 + col_tw_entries(logl) * 8;
+    return col_tile_words(logl, inv) * 4 + (col_tw_smem(logl, inv) ? col_tw_entries(logl) * 8 : 0);
 }
 
 // Threads of the three-pass row kernel: 2^14-word rows use 1024 threads with
