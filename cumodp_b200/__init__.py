@@ -114,6 +114,19 @@ def _lib():
         L.cumodp_subproduct_level_dev.restype = C.c_int
         L.cumodp_subproduct_level_dev.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32,
                                                   C.c_void_p]
+        L.cumodp_twoconv_mul_big.restype = C.c_int
+        L.cumodp_twoconv_mul_big.argtypes = [C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p, C.c_int,
+                                             C.c_void_p, C.c_int]
+        L.cumodp_twoconv_mul_big_dev.restype = C.c_int
+        L.cumodp_twoconv_mul_big_dev.argtypes = [C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p, C.c_int,
+                                                 C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+        L.cumodp_twoconv_big_bit_width.restype = C.c_int
+        L.cumodp_twoconv_big_bit_width.argtypes = [C.c_longlong, C.c_void_p, C.c_longlong, C.c_void_p, C.c_int]
+        L.cumodp_twoconv_big_out_words.restype = C.c_int
+        L.cumodp_twoconv_big_out_words.argtypes = [C.c_longlong, C.c_longlong, C.c_int]
+        L.cumodp_twoconv_big_plan.restype = C.c_int
+        L.cumodp_twoconv_big_plan.argtypes = [C.c_int, C.c_longlong, C.c_longlong, C.POINTER(C.c_int),
+                                              C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.cumodp_select_device.restype = C.c_int
         L.cumodp_select_device.argtypes = [C.c_int]
         L.cumodp_trace_passes.restype = None
@@ -392,6 +405,57 @@ def twoconv_plan(bit_width_a: int, bit_width_b: int, na: int, nb: int, method: i
     _check(_lib().cumodp_twoconv_plan(bit_width_a, bit_width_b, na, nb, method, C.byref(K), C.byref(M),
                                       C.byref(npr)), "cumodp_twoconv_plan")
     return K.value, M.value, npr.value
+
+
+def ints_to_words(values, words: int) -> np.ndarray:
+    """Python ints -> `words` little-endian 64-bit two's-complement words each."""
+    out = np.empty(len(values) * words, dtype=np.uint64)
+    mask = (1 << (64 * words)) - 1
+    for i, v in enumerate(values):
+        u = int(v) & mask
+        out[i * words:(i + 1) * words] = [(u >> (64 * k)) & 0xFFFFFFFFFFFFFFFF for k in range(words)]
+    return out
+
+
+def words_to_ints(w: np.ndarray, words: int) -> list:
+    """`words` little-endian 64-bit two's-complement words each -> Python ints."""
+    w = np.asarray(w, dtype=np.uint64).reshape(-1, words)
+    top = 1 << (64 * words)
+    res = []
+    for row in w:
+        u = 0
+        for k in range(words - 1, -1, -1):
+            u = (u << 64) | int(row[k])
+        res.append(u - top if u >> (64 * words - 1) else u)
+    return res
+
+
+def twoconv_big_words(values) -> int:
+    """64-bit words a signed coefficient list needs (two's complement)."""
+    bits = max((abs(int(v)).bit_length() for v in values), default=0) + 1
+    return max(1, (bits + 63) // 64)
+
+
+def twoconv_mul_big(a, b, in_words: int | None = None, out_words: int | None = None):
+    """Exact product of big-integer polynomials (``cumodp_twoconv_mul_big``); Python ints in and out."""
+    if in_words is None:
+        in_words = max(twoconv_big_words(a), twoconv_big_words(b))
+    wa, wb = ints_to_words(a, in_words), ints_to_words(b, in_words)
+    if out_words is None:
+        bw = int(_lib().cumodp_twoconv_big_bit_width(len(a), wa.ctypes.data, len(b), wb.ctypes.data, in_words))
+        out_words = int(_lib().cumodp_twoconv_big_out_words(len(a), len(b), bw))
+    c = np.empty((len(a) + len(b) - 1) * out_words, dtype=np.uint64)
+    _check(_lib().cumodp_twoconv_mul_big(len(a), wa.ctypes.data, len(b), wb.ctypes.data, in_words, c.ctypes.data,
+                                         out_words), "cumodp_twoconv_mul_big")
+    return words_to_ints(c, out_words)
+
+
+def twoconv_big_plan(bit_width: int, na: int, nb: int):
+    """(K, M, number of primes, log2 transform length) of the big-coefficient product."""
+    K, M, npr, lg = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    _check(_lib().cumodp_twoconv_big_plan(bit_width, na, nb, C.byref(K), C.byref(M), C.byref(npr), C.byref(lg)),
+           "cumodp_twoconv_big_plan")
+    return K.value, M.value, npr.value, lg.value
 
 
 # ------------------------------------------------------------- serving ----

@@ -1,0 +1,433 @@
+// Exact product of polynomials with big signed integer coefficients.
+//
+// Reference: the general two_convolution_poly_mul
+// (src/two_convolution_poly_mul.cu:532-569) on std::vector<mpz_class>: the
+// base table picks N-bit coefficients cut into K >= 32 limbs of M bits
+// (determine_bivariate_base, :72-82; convert_to_modular_bivariate, :84-203),
+// the x-direction is handled by a cyclic and a negacyclic convolution of
+// length K (two_convolution_2d_dev, :431-530), three primes are lifted by
+// CRT on the host with GMP (reconstruct_mpz_with_crt, :292-385) and the
+// product is (u+v)(2^M)/2 + 2^N (u-v)(2^M)/2 (recover_product_host,
+// :387-428).
+//
+// Here the coefficients travel as fixed-width two's-complement words (no GMP
+// on either side of the boundary) and the whole computation stays on the
+// GPU:
+//   1. k_big_abs: |a_j| and its sign, one thread per coefficient;
+//   2. k_big_split: per prime, the Kronecker layout A_p[j*(2K-1) + i] =
+//      sign_j * limb_i(|a_j|) mod p for i < K and 0 for K <= i < 2K-1, one
+//      thread per word.  The zero tail of every block keeps the
+//      (2K-1)-coefficient linear x-convolution of two K-limb numbers inside
+//      its block, so one univariate product per prime equals the bivariate
+//      product (about the total transform length of a cyclic plus a
+//      negacyclic convolution of length K);
+//   3. one univariate product per prime (fused single-CTA or three-pass
+//      kernels);
+//   4. k_big_crt: per output coefficient, Garner's CRT of every x-coefficient
+//      to a signed 128-bit integer and the sum of them shifted by M*i bits,
+//      in separate positive and negative multiword accumulators, stored as
+//      out_words two's-complement words.
+// The planner picks the number of primes (3 or 4) and the limb width M with
+// the cheapest transform such that every x-coefficient satisfies
+// K * min(la, lb) * (2^M - 1)^2 < P / 2.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "../../include/cumodp.h"
+#include "product.cuh"
+
+namespace cmb {
+
+namespace {
+
+constexpr int kBigMaxInWords = 64;    // coefficients up to 4096 bits
+constexpr int kBigMaxAccWords = 136;  // 2 * 4096 + 192 bits of accumulator
+constexpr int kBigMaxPrimes = 4;
+
+// Fourier primes below 2^30, largest first, with their 2-adic orders.
+const u32 kBigPrimes[] = {998244353u, 897581057u, 880803841u, 754974721u, 645922817u,
+                          595591169u, 469762049u, 377487361u, 167772161u};
+const int kBigPrimeOrder[] = {23, 23, 23, 24, 23, 23, 26, 23, 25};
+
+struct BigPlan {
+    int K, M, nprimes, logn;
+    u32 p[kBigMaxPrimes];
+};
+
+int ceil_log2_ll(long long v) {
+    int l = 0;
+    while ((1ll << l) < v) ++l;
+    return l;
+}
+
+// log2 of a product of primes (a lower bound by a hair, for the bound test).
+double log2_prod(const u32* p, int r) {
+    double s = 0;
+    for (int i = 0; i < r; ++i) s += std::log2((double)p[i]);
+    return s;
+}
+
+int big_plan(int bw, long long na, long long nb, BigPlan* out) {
+    if (bw < 0 || bw > 64 * kBigMaxInWords || na <= 0 || nb <= 0) return ASSUMPTION_ERROR;
+    const int bits = std::max(bw, 1);
+    const long long nmin = std::min(na, nb);
+    bool found = false;
+    BigPlan best{};
+    double best_cost = 0;
+    for (int r = 3; r <= kBigMaxPrimes; ++r) {
+        for (int M = std::min(62, bits); M >= 1; --M) {
+            const int K = (bits + M - 1) / M;
+            const long long la = (2ll * K - 1) * (na - 1) + K, lb = (2ll * K - 1) * (nb - 1) + K;
+            const int logn = ceil_log2_ll(la + lb - 1);
+            if (logn > kMaxLog) continue;
+            u32 p[kBigMaxPrimes];
+            int k = 0;
+            for (size_t i = 0; i < sizeof(kBigPrimes) / sizeof(kBigPrimes[0]) && k < r; ++i)
+                if (kBigPrimeOrder[i] >= logn) p[k++] = kBigPrimes[i];
+            if (k < r) continue;
+            // |x-coefficient| <= K * nmin * (2^M - 1)^2 < 2^(2M + log2(K nmin)) < P / 2
+            const double need = 2.0 * M + std::log2((double)K * (double)nmin) + 1.0;
+            if (need >= log2_prod(p, r) - 0.01) continue;
+            const double cost = (double)r * std::ldexp(1.0, logn) * logn;
+            if (!found || cost < best_cost) {
+                found = true;
+                best_cost = cost;
+                best.K = K;
+                best.M = M;
+                best.nprimes = r;
+                best.logn = logn;
+                for (int i = 0; i < r; ++i) best.p[i] = p[i];
+            }
+            break;  // the largest feasible M for this r
+        }
+    }
+    if (!found) return FFT_SIZE_TOO_LARGE;
+    *out = best;
+    return OK;
+}
+
+// Words of a product coefficient: |c| <= min(na, nb) * (2^bw - 1)^2.
+int big_out_words(long long na, long long nb, int bw) {
+    const int bits = 2 * std::max(bw, 1) + ceil_log2_ll(std::min(na, nb) + 1) + 1;
+    return (bits + 63) / 64;
+}
+
+// |x_j| (in_words words) and sign, one thread per coefficient.
+__global__ void k_big_abs(const unsigned long long* __restrict__ x, long long len, int words,
+                          unsigned long long* __restrict__ mag, unsigned char* __restrict__ neg) {
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= len) return;
+    const unsigned long long* w = x + j * words;
+    unsigned long long* m = mag + j * words;
+    const bool s = (long long)w[words - 1] < 0;
+    unsigned long long carry = 1;
+    for (int i = 0; i < words; ++i) {
+        if (s) {
+            const unsigned long long v = ~w[i] + carry;
+            carry = (carry && v == 0) ? 1 : 0;
+            m[i] = v;
+        } else {
+            m[i] = w[i];
+        }
+    }
+    neg[j] = s ? 1 : 0;
+}
+
+struct BigSplitArgs {
+    const unsigned long long* mag;
+    const unsigned char* neg;
+    long long len;  // coefficients
+    int words, K, M, nprimes;
+    u32 p[kBigMaxPrimes];
+    u32* out[kBigMaxPrimes];  // (2K - 1)(len - 1) + K words each
+};
+
+// out_p[j*(2K-1) + i] = sign_j * (bits [M i, M i + M) of |x_j|) mod p, i < K;
+// 0 for K <= i < 2K-1 (the last block is cut at K words).
+__global__ void k_big_split(const __grid_constant__ BigSplitArgs A) {
+    const int blk = 2 * A.K - 1;
+    const long long total = (long long)blk * (A.len - 1) + A.K;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long j = t / blk;
+        const int i = (int)(t % blk);
+        unsigned long long limb = 0;
+        if (i < A.K) {
+            const long long s = (long long)A.M * i;
+            const int w = (int)(s >> 6), b = (int)(s & 63);
+            const unsigned long long* m = A.mag + j * A.words;
+            if (w < A.words) {
+                limb = m[w] >> b;
+                if (b && w + 1 < A.words) limb |= m[w + 1] << (64 - b);
+                if (A.M < 64) limb &= (1ull << A.M) - 1;
+            }
+        }
+        const bool ng = A.neg[j] != 0;
+        for (int k = 0; k < A.nprimes; ++k) {
+            const u32 p = A.p[k];
+            u32 r = (u32)(limb % p);
+            if (ng && r) r = p - r;
+            A.out[k][t] = r;
+        }
+    }
+}
+
+struct BigCrtArgs {
+    const u32* prod[kBigMaxPrimes];  // (2K - 1) lc words each
+    long long lc;                    // output coefficients
+    int K, M, nprimes, out_words;
+    u32 p[kBigMaxPrimes];
+    u32 inv[kBigMaxPrimes][kBigMaxPrimes];  // inv[a][b] = p_a^-1 mod p_b (a < b)
+    unsigned long long* c;
+};
+
+// Adds v (unsigned 128-bit) shifted left by s bits into acc (n words).
+__device__ __forceinline__ void acc_add(unsigned long long* acc, int n, unsigned __int128 v, long long s) {
+    const int w = (int)(s >> 6), b = (int)(s & 63);
+    unsigned long long part[3];
+    part[0] = (unsigned long long)v << b;
+    part[1] = b ? (unsigned long long)(v >> (64 - b)) : (unsigned long long)(v >> 64);
+    part[2] = b ? (unsigned long long)((v >> 64) >> (64 - b)) : 0ull;
+    unsigned long long carry = 0;
+    int i = 0;
+    for (; i < 3 && w + i < n; ++i) {
+        const unsigned long long a = acc[w + i];
+        const unsigned long long t = a + part[i];
+        const unsigned long long c1 = t < a;
+        const unsigned long long u = t + carry;
+        carry = c1 + (u < t);
+        acc[w + i] = u;
+    }
+    for (int k = w + i; carry && k < n; ++k) {
+        acc[k] += 1;
+        carry = acc[k] == 0;
+    }
+}
+
+__global__ void k_big_crt(const __grid_constant__ BigCrtArgs A) {
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= A.lc) return;
+    const int nacc = min(kBigMaxAccWords, (int)((2ll * A.M * A.K + 192 + 63) / 64));
+    unsigned long long pos[kBigMaxAccWords], negv[kBigMaxAccWords];
+    for (int i = 0; i < nacc; ++i) pos[i] = negv[i] = 0;
+    // P and P / 2 as unsigned 128-bit
+    unsigned __int128 P = 1;
+    for (int k = 0; k < A.nprimes; ++k) P *= A.p[k];
+    const unsigned __int128 half = P >> 1;
+    for (int i = 0; i < 2 * A.K - 1; ++i) {
+        const long long idx = j * (2ll * A.K - 1) + i;
+        // Garner: mixed-radix digits v_k with x = v_0 + v_1 p_0 + v_2 p_0 p_1 + ...
+        u32 v[kBigMaxPrimes];
+        for (int k = 0; k < A.nprimes; ++k) {
+            u64 t = A.prod[k][idx];
+            for (int a = 0; a < k; ++a) {
+                // t = (t - v_a) * p_a^-1 mod p_k
+                const u32 pk = A.p[k];
+                const u64 d = (t + pk - (v[a] % pk)) % pk;
+                t = (d * A.inv[a][k]) % pk;
+            }
+            v[k] = (u32)t;
+        }
+        unsigned __int128 x = 0, radix = 1;
+        for (int k = 0; k < A.nprimes; ++k) {
+            x += (unsigned __int128)v[k] * radix;
+            radix *= A.p[k];
+        }
+        const long long s = (long long)A.M * i;
+        if (x > half) acc_add(negv, nacc, P - x, s);
+        else if (x) acc_add(pos, nacc, x, s);
+    }
+    // c = pos - neg, truncated to out_words
+    unsigned long long* out = A.c + j * A.out_words;
+    unsigned long long borrow = 0;
+    for (int k = 0; k < A.out_words; ++k) {
+        const unsigned long long a = k < nacc ? pos[k] : 0ull, b = k < nacc ? negv[k] : 0ull;
+        const unsigned long long d = a - b;
+        const unsigned long long b1 = a < b;
+        const unsigned long long e = d - borrow;
+        borrow = b1 + (d < borrow);
+        out[k] = e;
+    }
+}
+
+int grid_of(long long n) { return (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148 * 32)); }
+
+}  // namespace
+
+// c (lc = na + nb - 1 coefficients of out_words words) = a * b exactly;
+// device pointers, coefficients of in_words two's-complement words, bw the
+// largest magnitude bit width of any coefficient.
+int bigconv_mul_dev(const unsigned long long* a, long long na, const unsigned long long* b, long long nb,
+                    int in_words, unsigned long long* c, int out_words, int bw, cudaStream_t st, BigPlan* used) {
+    if (in_words <= 0 || in_words > kBigMaxInWords || out_words <= 0 || na <= 0 || nb <= 0)
+        return ASSUMPTION_ERROR;
+    if (bw < 0 || bw > 64 * in_words) return ASSUMPTION_ERROR;
+    BigPlan pl;
+    int err = big_plan(bw, na, nb, &pl);
+    if (err != OK) return err;
+    if (used) *used = pl;
+    const long long lc = na + nb - 1;
+    const long long la = (2ll * pl.K - 1) * (na - 1) + pl.K, lb = (2ll * pl.K - 1) * (nb - 1) + pl.K;
+    const long long lp = la + lb - 1;
+    const int r = pl.nprimes;
+    // scratch: |a|, |b| (64-bit words), signs, split operands and products per prime
+    const size_t mag_bytes = (size_t)(na + nb) * in_words * 8;
+    const size_t sign_bytes = ((size_t)(na + nb) + 255) & ~(size_t)255;
+    const size_t words = (size_t)r * (la + lb + lp);
+    const int dev = current_device();
+    char* ws = (char*)workspace(dev, kWsBig, mag_bytes + sign_bytes + words * 4, &err);
+    if (!ws) return err;
+    unsigned long long* mag = (unsigned long long*)ws;
+    unsigned char* sg = (unsigned char*)(ws + mag_bytes);
+    u32* w32 = (u32*)(ws + mag_bytes + sign_bytes);
+    k_big_abs<<<grid_of(na), 256, 0, st>>>(a, na, in_words, mag, sg);
+    k_big_abs<<<grid_of(nb), 256, 0, st>>>(b, nb, in_words, mag + (size_t)na * in_words, sg + na);
+    u32 *ap[kBigMaxPrimes], *bp[kBigMaxPrimes], *cp[kBigMaxPrimes];
+    for (int k = 0; k < r; ++k) {
+        ap[k] = w32 + (size_t)k * (la + lb + lp);
+        bp[k] = ap[k] + la;
+        cp[k] = bp[k] + lb;
+    }
+    BigSplitArgs S;
+    memset(&S, 0, sizeof(S));
+    S.words = in_words;
+    S.K = pl.K;
+    S.M = pl.M;
+    S.nprimes = r;
+    for (int k = 0; k < r; ++k) S.p[k] = pl.p[k];
+    S.mag = mag;
+    S.neg = sg;
+    S.len = na;
+    for (int k = 0; k < r; ++k) S.out[k] = ap[k];
+    k_big_split<<<grid_of(la), 256, 0, st>>>(S);
+    S.mag = mag + (size_t)na * in_words;
+    S.neg = sg + na;
+    S.len = nb;
+    for (int k = 0; k < r; ++k) S.out[k] = bp[k];
+    k_big_split<<<grid_of(lb), 256, 0, st>>>(S);
+    if ((err = cuda_err(cudaGetLastError())) != OK) return err;
+    for (int k = 0; k < r; ++k)
+        if ((err = mul_dev(ap[k], la, bp[k], lb, cp[k], lp, pl.p[k], st)) != OK) return err;
+    BigCrtArgs C;
+    memset(&C, 0, sizeof(C));
+    for (int k = 0; k < r; ++k) {
+        C.prod[k] = cp[k];
+        C.p[k] = pl.p[k];
+    }
+    for (int x = 0; x < r; ++x)
+        for (int y = x + 1; y < r; ++y) C.inv[x][y] = powmod_exact(pl.p[x] % pl.p[y], pl.p[y] - 2, pl.p[y]);
+    C.lc = lc;
+    C.K = pl.K;
+    C.M = pl.M;
+    C.nprimes = r;
+    C.out_words = out_words;
+    C.c = c;
+    k_big_crt<<<(unsigned)((lc + 127) / 128), 128, 0, st>>>(C);
+    return cuda_err(cudaGetLastError());
+}
+
+}  // namespace cmb
+
+using namespace cmb;
+
+namespace {
+
+int bw_words(const uint64_t* x, long long n, int words) {
+    int bw = 0;
+    for (long long j = 0; j < n; ++j) {
+        const uint64_t* w = x + j * words;
+        const bool neg = (int64_t)w[words - 1] < 0;
+        // magnitude bit width: for negative x, |x| = ~x + 1
+        unsigned long long carry = 1;
+        int top = 0;
+        for (int i = 0; i < words; ++i) {
+            unsigned long long v = w[i];
+            if (neg) {
+                v = ~v + carry;
+                carry = (carry && v == 0) ? 1 : 0;
+            }
+            if (v) top = i * 64 + 64 - __builtin_clzll(v);
+        }
+        bw = std::max(bw, top);
+    }
+    return bw;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cumodp_twoconv_big_out_words(long long na, long long nb, int bit_width) {
+    if (na <= 0 || nb <= 0 || bit_width < 0) return 0;
+    return big_out_words(na, nb, bit_width);
+}
+
+int cumodp_twoconv_big_bit_width(long long na, const uint64_t* a, long long nb, const uint64_t* b, int in_words) {
+    if (na < 0 || nb < 0 || in_words <= 0 || (na && !a) || (nb && !b)) return -1;
+    return std::max(bw_words(a, na, in_words), bw_words(b, nb, in_words));
+}
+
+cumodp_err cumodp_twoconv_big_plan(int bit_width, long long na, long long nb, int* K, int* M, int* nprimes,
+                                   int* log_transform) {
+    BigPlan pl;
+    const int e = big_plan(bit_width, na, nb, &pl);
+    if (e != OK) return (cumodp_err)e;
+    if (K) *K = pl.K;
+    if (M) *M = pl.M;
+    if (nprimes) *nprimes = pl.nprimes;
+    if (log_transform) *log_transform = pl.logn;
+    return CUMODP_SUCCESS;
+}
+
+cumodp_err cumodp_twoconv_mul_big_dev(long long na, const uint64_t* a, long long nb, const uint64_t* b, int in_words,
+                                      uint64_t* c, int out_words, int bit_width, void* stream) {
+    int cnt = 0;
+    if (cudaGetDeviceCount(&cnt) != cudaSuccess || cnt == 0) {
+        cudaGetLastError();
+        return CUMODP_NO_CUDA_DEVICE;
+    }
+    if (!a || !b || !c) return CUMODP_ASSUMPTION_ERROR;
+    std::lock_guard<std::mutex> g(lib_mutex());
+    cudaStream_t st = stream ? (cudaStream_t)stream : lib_stream(current_device());
+    int e = bigconv_mul_dev((const unsigned long long*)a, na, (const unsigned long long*)b, nb, in_words,
+                            (unsigned long long*)c, out_words, bit_width, st, nullptr);
+    if (e == OK && !stream) e = cuda_err(cudaStreamSynchronize(st));
+    return (cumodp_err)e;
+}
+
+cumodp_err cumodp_twoconv_mul_big(long long na, const uint64_t* a, long long nb, const uint64_t* b, int in_words,
+                                  uint64_t* c, int out_words) {
+    int cnt = 0;
+    if (cudaGetDeviceCount(&cnt) != cudaSuccess || cnt == 0) {
+        cudaGetLastError();
+        return CUMODP_NO_CUDA_DEVICE;
+    }
+    if (na <= 0 || nb <= 0 || !a || !b || !c || in_words <= 0 || in_words > kBigMaxInWords || out_words <= 0)
+        return CUMODP_ASSUMPTION_ERROR;
+    const int bw = std::max(bw_words(a, na, in_words), bw_words(b, nb, in_words));
+    std::lock_guard<std::mutex> g(lib_mutex());
+    const int dev = current_device();
+    cudaStream_t st = lib_stream(dev);
+    const long long lc = na + nb - 1;
+    int err = OK;
+    const size_t in_bytes = (size_t)(na + nb) * in_words * 8, out_bytes = (size_t)lc * out_words * 8;
+    char* d = (char*)workspace(dev, kWsStage, in_bytes + out_bytes, &err);
+    if (!d) return (cumodp_err)err;
+    unsigned long long* da = (unsigned long long*)d;
+    unsigned long long* db = da + (size_t)na * in_words;
+    unsigned long long* dc = (unsigned long long*)(d + in_bytes);
+    cudaError_t ce = cudaMemcpyAsync(da, a, (size_t)na * in_words * 8, cudaMemcpyHostToDevice, st);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(db, b, (size_t)nb * in_words * 8, cudaMemcpyHostToDevice, st);
+    if (ce != cudaSuccess) return (cumodp_err)cuda_err(ce);
+    err = bigconv_mul_dev(da, na, db, nb, in_words, dc, out_words, bw, st, nullptr);
+    if (err != OK) {
+        cudaStreamSynchronize(st);
+        return (cumodp_err)err;
+    }
+    ce = cudaMemcpyAsync(c, dc, out_bytes, cudaMemcpyDeviceToHost, st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    return (cumodp_err)cuda_err(ce);
+}
+
+}  // extern "C"

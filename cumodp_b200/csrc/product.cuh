@@ -14,7 +14,7 @@ constexpr int kMaxLog = kMaxColLog + kMaxRowLog;  // 2^24
 
 // workspace slots (runtime.cuh: workspace)
 enum WsSlot { kWsSingle = 0, kWsBatch = 1, kWsStage = 2, kWsNtt = 3, kWsTwoConv = 4, kWsServer = 5,
-              kWsBiv = 6, kWsBivHost = 7 };
+              kWsBiv = 6, kWsBivHost = 7, kWsBig = 8 };
 
 // Transform length log2 for a product of la and lb coefficients.
 int product_logn(long long la, long long lb);

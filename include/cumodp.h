@@ -309,6 +309,31 @@ cumodp_err cumodp_bivariate_mul(sfixn nxf, sfixn nyf, const sfixn *F, sfixn nxg,
 cumodp_err cumodp_subproduct_level_dev(sfixn l, sfixn npairs, const sfixn *M_in, sfixn *M_out, sfixn p,
                                        void *stream);
 
+/* Addition.  Exact product of polynomials with big signed integer
+ * coefficients: the general two_convolution_poly_mul
+ * (src/two_convolution_poly_mul.cu:532-569, std::vector<mpz_class>) without
+ * GMP at the boundary.  Every coefficient of a and b is `in_words`
+ * little-endian 64-bit words in two's complement (in_words <= 64: up to 4096
+ * bits); c receives na+nb-1 coefficients of `out_words` words in two's
+ * complement, truncated to out_words (cumodp_twoconv_big_out_words gives the
+ * width that always holds the product).  Host arrays.  The whole computation
+ * (limb split, one univariate product per prime, CRT and recombination) runs
+ * on the GPU; cumodp_twoconv_big_plan reports the limb split and primes. */
+cumodp_err cumodp_twoconv_mul_big(long long na, const uint64_t *a, long long nb, const uint64_t *b, int in_words,
+                                  uint64_t *c, int out_words);
+/* The same on DEVICE arrays; bit_width bounds the magnitude bit width of
+ * every coefficient (cumodp_twoconv_big_bit_width computes it on the host). */
+cumodp_err cumodp_twoconv_mul_big_dev(long long na, const uint64_t *a, long long nb, const uint64_t *b, int in_words,
+                                      uint64_t *c, int out_words, int bit_width, void *stream);
+int cumodp_twoconv_big_bit_width(long long na, const uint64_t *a, long long nb, const uint64_t *b, int in_words);
+int cumodp_twoconv_big_out_words(long long na, long long nb, int bit_width);
+/* K limbs of M bits per coefficient, `nprimes` Fourier primes, transform
+ * length 2^log_transform: the cheapest split whose CRT bound
+ * K * min(na, nb) * (2^M - 1)^2 < P/2 holds (the reference picks from
+ * base_table with K >= 32, include/two_convolution_poly_mul.h:94-527). */
+cumodp_err cumodp_twoconv_big_plan(int bit_width, long long na, long long nb, int *K, int *M, int *nprimes,
+                                   int *log_transform);
+
 /* Addition.  Makes `dev` the current device of the calling thread for the
  * library's own CUDA runtime (one process per GPU). */
 cumodp_err cumodp_select_device(int dev);

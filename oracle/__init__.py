@@ -201,6 +201,25 @@ def subproduct_level(M: np.ndarray, l: int, p: int) -> np.ndarray:
     return out.reshape(-1)
 
 
+def bigint_polymul(a, b) -> list:
+    """Exact product of big-integer polynomials (Python ints, schoolbook).
+
+    The reference's general two_convolution_poly_mul
+    (src/two_convolution_poly_mul.cu:532-569) and its benchmark's Kronecker
+    baseline (benchmark/bench_two_convolution_poly_mul.cpp:11-100) both
+    compute this exact product; schoolbook over Python ints is its
+    definition (small cases only).
+    """
+    a = [int(v) for v in a]
+    b = [int(v) for v in b]
+    out = [0] * (len(a) + len(b) - 1)
+    for i, x in enumerate(a):
+        if x:
+            for j, y in enumerate(b):
+                out[i + j] += x * y
+    return out
+
+
 def polymul_i128(a: np.ndarray, b: np.ndarray) -> list[int]:
     """Exact integer product (Python ints) by __int128 schoolbook."""
     a = np.ascontiguousarray(a, dtype=np.int64)

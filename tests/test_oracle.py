@@ -48,16 +48,12 @@ def test_i128_oracle_matches_golden_files(oracle_mod, name):
 
 
 @pytest.mark.parametrize("name", BIG)
-def test_big_golden_files_are_products(name):
+def test_big_golden_files_are_products(oracle_mod, name):
     """The big-coefficient files are self-consistent exact products (python ints)."""
     a, b, c = read_golden(name)
-    if len(a) > 128:
+    if len(a) > 256:
         pytest.skip("python schoolbook only for the small big-integer files")
-    out = [0] * (len(a) + len(b) - 1)
-    for i, x in enumerate(a):
-        for j, y in enumerate(b):
-            out[i + j] += x * y
-    assert out == c
+    assert oracle_mod.bigint_polymul(a, b) == c
 
 
 def test_unit_kat_products(oracle_mod):
