@@ -345,13 +345,15 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         extras["ntt_2_24"] = ntt_2_24(cm, torch, dev, stream, hbm_peak)
         extras["batched_c4"] = batched_c4(cm, torch, dev, stream)
         extras["c1_4095x4095"] = c1_latency(cm, torch, dev, stream)
+        extras["c3_exact_int64"] = c3_exact(cm, torch, dev, stream)
+        extras["big_1024bit_1024terms"] = big_coefficients(cm, torch, dev, stream)
         extras["serving_c5"] = serving_c5(cm)
     cpu = None
     if rank == 0 and world == 1 and not args.no_extras:
         cpu = cpu_baseline()
 
     if rank == 0:
-        launches = args.steps * 3
+        launches = args.steps * len(passes)  # one launch per traced pass per product
         line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 5), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "u32",
@@ -454,6 +456,104 @@ def batched_c4(cm, torch, dev, stream):
     return {"pairs": cnt, "ms_batched": round(t_batch, 4), "products_per_s_batched": round(cnt / (t_batch / 1000), 1),
             "ms_one_call_per_pair": round(t_single, 4), "ms_one_call_per_pair_wall": round(t_single_wall, 4),
             "speedup_vs_one_call": round(t_single / t_batch, 2), "batched_equals_single": same}
+
+
+def c3_exact(cm, torch, dev, stream):
+    """Config 3: exact products of int64 polynomials, |c| <= 10^10, degrees 8191 and 16383.
+
+    Device latency through cumodp_twoconv_mul_i64_dev (device buffers) and
+    through the host entry cumodp_twoconv_mul_i64; checked by the identity
+    c(1) = a(1) b(1) on Python ints (size-independent).
+    """
+    import ctypes as C
+    from cumodp_b200.workloads import SplitMix64, seed_for
+    r = SplitMix64(seed_for(2))
+    out = {}
+    for d in (8191, 16383):
+        a, b = r.int64_in(d + 1, 10**10), r.int64_in(d + 1, 10**10)
+        bw = cm.twoconv_bit_width(a, b)
+        dA = torch.from_numpy(a).to(dev)
+        dB = torch.from_numpy(b).to(dev)
+        dC = torch.empty(2 * (2 * d + 1), dtype=torch.int64, device=dev)
+        sp = stream.cuda_stream
+        f = cm.lib().cumodp_twoconv_mul_i64_dev
+
+        def run():
+            rc = f(d + 1, dA.data_ptr(), d + 1, dB.data_ptr(), dC.data_ptr(), bw, 0, C.c_void_p(sp))
+            assert rc == 0, rc
+        for _ in range(3):
+            run()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        reps = 20
+        e0.record(stream)
+        for _ in range(reps):
+            run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dev_ms = e0.elapsed_time(e1) / reps
+        t0 = time.perf_counter()
+        for _ in range(5):
+            c = cm.twoconv_mul(a, b)
+        host_ms = (time.perf_counter() - t0) * 1000 / 5
+        ok = sum(c) == sum(int(x) for x in a) * sum(int(x) for x in b)
+        K, M, npr = cm.twoconv_plan(bw, bw, d + 1, d + 1)
+        out[f"deg_{d}"] = {"device_ms": round(dev_ms, 4), "host_entry_ms": round(host_ms, 3),
+                           "products_per_s_device": round(1000 / dev_ms, 1), "plan": {"K": K, "M": M, "primes": npr},
+                           "sum_identity": bool(ok)}
+    return out
+
+
+def big_coefficients(cm, torch, dev, stream):
+    """Big-coefficient exact product at the shape of the reference's benchmark/n1024.test:
+    1024 x 1024 coefficients of 1024 bits (signed here), device latency and host entry."""
+    import ctypes as C
+    from cumodp_b200.workloads import SplitMix64, seed_for
+    r = SplitMix64(seed_for(5))
+    n, bits, words = 1024, 1024, 17
+
+    def ints(k):
+        raw = r.next_u64(k * 16).reshape(k, 16)
+        vals = []
+        for row in raw:
+            v = 0
+            for w in row[::-1]:
+                v = (v << 64) | int(w)
+            vals.append(-v if int(row[0]) & 1 else v)
+        return vals
+    a, b = ints(n), ints(n)
+    wa, wb = cm.ints_to_words(a, words), cm.ints_to_words(b, words)
+    bw = bits
+    ow = int(cm.lib().cumodp_twoconv_big_out_words(n, n, bw))
+    dA = torch.from_numpy(wa.view(np.int64)).to(dev)
+    dB = torch.from_numpy(wb.view(np.int64)).to(dev)
+    dC = torch.empty((2 * n - 1) * ow, dtype=torch.int64, device=dev)
+    f = cm.lib().cumodp_twoconv_mul_big_dev
+    sp = stream.cuda_stream
+
+    def run():
+        rc = f(n, dA.data_ptr(), n, dB.data_ptr(), words, dC.data_ptr(), ow, bw, C.c_void_p(sp))
+        assert rc == 0, rc
+    for _ in range(3):
+        run()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    reps = 20
+    e0.record(stream)
+    for _ in range(reps):
+        run()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    dev_ms = e0.elapsed_time(e1) / reps
+    t0 = time.perf_counter()
+    c = cm.twoconv_mul_big(a, b, in_words=words)
+    host_ms = (time.perf_counter() - t0) * 1000
+    ok = sum(c) == sum(a) * sum(b)
+    K, M, npr, lg = cm.twoconv_big_plan(bw, n, n)
+    return {"device_ms": round(dev_ms, 4), "host_entry_ms_incl_python_conversion": round(host_ms, 2),
+            "plan": {"K": K, "M": M, "primes": npr, "log2_transform": lg}, "sum_identity": bool(ok)}
 
 
 def c1_latency(cm, torch, dev, stream):
