@@ -212,12 +212,14 @@ int build_plan(BatchPlan& P, const PrimeCtx& pc, cudaStream_t st) {
         if (logn > pc.info.two_adic || logn > kMaxLog) return FFT_SIZE_TOO_LARGE;
         ClassPlan& c = by[logn];
         c.logn = logn;
-        c.large = logn > kMaxSmallLog;
         c.members.push_back((int)i);
     }
     size_t jb = 0, ws = 0;
     for (auto& kv : by) {
         ClassPlan c = kv.second;
+        // a few products of a length one CTA could hold still run faster
+        // spread over many CTAs (the three-pass kernels)
+        c.large = c.logn > kMaxSmallLog || (c.logn >= single_large_min_log() && c.members.size() <= 16);
         c.job_off = jb;
         jb += c.members.size() * (c.large ? sizeof(LargeJob) : sizeof(ProdJob));
         jb = (jb + 255) & ~(size_t)255;

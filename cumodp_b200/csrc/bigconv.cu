@@ -39,6 +39,9 @@
 
 namespace cmb {
 
+int batch_mul_dev(int count, const sfixn* df, const int64_t* f_off, const u32* F, const sfixn* dg,
+                  const int64_t* g_off, const u32* G, const int64_t* h_off, u32* H, u32 p, cudaStream_t st);
+
 namespace {
 
 constexpr int kBigMaxInWords = 64;    // coefficients up to 4096 bits
@@ -307,8 +310,17 @@ int bigconv_mul_dev(const unsigned long long* a, long long na, const unsigned lo
     for (int k = 0; k < r; ++k) S.out[k] = bp[k];
     k_big_split<<<grid_of(lb), 256, 0, st>>>(S);
     if ((err = cuda_err(cudaGetLastError())) != OK) return err;
-    for (int k = 0; k < r; ++k)
-        if ((err = mul_dev(ap[k], la, bp[k], lb, cp[k], lp, pl.p[k], st)) != OK) return err;
+    // one product per prime, on side streams (each batch plan owns its
+    // workspace), joined before the CRT
+    {
+        const sfixn df = (sfixn)(la - 1), dg = (sfixn)(lb - 1);
+        const int64_t zero = 0;
+        aux_fork(dev, st, r);
+        for (int k = 0; k < r && err == OK; ++k)
+            err = batch_mul_dev(1, &df, &zero, ap[k], &dg, &zero, bp[k], &zero, cp[k], pl.p[k], aux_stream(dev, k));
+        aux_join(dev, st, r);
+        if (err != OK) return err;
+    }
     BigCrtArgs C;
     memset(&C, 0, sizeof(C));
     for (int k = 0; k < r; ++k) {

@@ -93,6 +93,11 @@ __host__ __device__ constexpr int col_smem_bytes(int logl, bool inv) {
     return col_tile_words(logl, inv) * 4 + (col_tw_smem(logl, inv) ? col_tw_entries(logl) * 8 : 0);
 }
 
+// A single product (no batch) of transform length 2^logn uses the three-pass
+// kernels from this length on, even where one CTA could hold it: spread over
+// many CTAs it finishes sooner than on one SM.
+__host__ __device__ constexpr int single_large_min_log() { return 13; }
+
 // Threads of the three-pass row kernel: 2^14-word rows use 1024 threads with
 // at most 64 registers each (32 warps per SM; the plan's twiddled levels
 // have radix <= 8 so both operands fit), shorter rows the single-CTA count.

@@ -262,7 +262,7 @@ int mul_dev(const u32* a, long long la, const u32* b, long long lb, u32* h, long
         lh = n;
     }
     const u32 root = canonical_root(*pc, logn);
-    if (logn <= kMaxSmallLog) {
+    if (logn <= kMaxSmallLog && logn < single_large_min_log()) {
         SmallArgs A;
         if ((err = small_args(*pc, root, logn, dev, &A)) != OK) return err;
         A.job0 = ProdJob{a, b, h, (int)la, (int)lb, (int)lh, 0};

@@ -9,6 +9,7 @@
 #include "runtime.cuh"
 
 #include <cstdio>
+#include <map>
 #include <cstring>
 
 namespace cmb {
@@ -303,6 +304,47 @@ cudaStream_t lib_stream(int dev) {
     cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
     C.streams[dev] = s;
     return s;
+}
+
+namespace {
+struct AuxSet {
+    cudaStream_t s[kAuxStreams];
+    cudaEvent_t fork, join[kAuxStreams];
+};
+}  // namespace
+
+// Side streams for independent work inside one call (fork/join by events).
+static AuxSet& aux_set(int dev) {
+    static std::mutex m;
+    static std::map<int, AuxSet*> sets;
+    std::lock_guard<std::mutex> g(m);
+    auto it = sets.find(dev);
+    if (it != sets.end()) return *it->second;
+    AuxSet* a = new AuxSet();
+    for (int i = 0; i < kAuxStreams; ++i) {
+        cudaStreamCreateWithFlags(&a->s[i], cudaStreamNonBlocking);
+        cudaEventCreateWithFlags(&a->join[i], cudaEventDisableTiming);
+    }
+    cudaEventCreateWithFlags(&a->fork, cudaEventDisableTiming);
+    sets[dev] = a;
+    return *a;
+}
+
+cudaStream_t aux_fork(int dev, cudaStream_t st, int n) {
+    AuxSet& a = aux_set(dev);
+    cudaEventRecord(a.fork, st);
+    for (int i = 0; i < n && i < kAuxStreams; ++i) cudaStreamWaitEvent(a.s[i], a.fork, 0);
+    return a.s[0];
+}
+
+cudaStream_t aux_stream(int dev, int i) { return aux_set(dev).s[i]; }
+
+void aux_join(int dev, cudaStream_t st, int n) {
+    AuxSet& a = aux_set(dev);
+    for (int i = 0; i < n && i < kAuxStreams; ++i) {
+        cudaEventRecord(a.join[i], a.s[i]);
+        cudaStreamWaitEvent(st, a.join[i], 0);
+    }
 }
 
 std::mutex& lib_mutex() {

@@ -77,6 +77,16 @@ cudaStream_t lib_stream(int dev);
 // Serialises host entry points that share workspace and caches.
 std::mutex& lib_mutex();
 
+// Side streams of the library (per device) for independent pieces of one
+// call: aux_fork makes streams 0..n-1 wait for `st`'s work so far,
+// aux_stream(dev, i) is stream i, aux_join makes `st` wait for all of them.
+// Calls are serialised by lib_mutex, so the side streams are never shared by
+// two calls at once.
+constexpr int kAuxStreams = 4;
+cudaStream_t aux_fork(int dev, cudaStream_t st, int n);
+cudaStream_t aux_stream(int dev, int i);
+void aux_join(int dev, cudaStream_t st, int n);
+
 int current_device();
 
 // Device bytes held by the caches and workspace of this process.

@@ -281,12 +281,19 @@ int twoconv_mul_dev(const long long* a, long long la, const long long* b, long l
         ho[s] = (int64_t)s * lc;
     }
     if (!bufs) {
+        // the primes are independent: one side stream each (each batch plan
+        // owns its workspace), joined before the CRT
+        aux_fork(dev, st, np);
         for (int r = 0; r < np; ++r) {
             err = batch_mul_dev(npts, df.data(), fo.data(), ea + (size_t)r * npts * la, dg.data(), go.data(),
                                 eb + (size_t)r * npts * lb, ho.data(), ec + (size_t)r * npts * lc,
-                                kTwoConvPrimes[r], st);
-            if (err != OK) return err;
+                                kTwoConvPrimes[r], aux_stream(dev, r));
+            if (err != OK) {
+                aux_join(dev, st, np);
+                return err;
+            }
         }
+        aux_join(dev, st, np);
     } else {
         std::vector<long long> LA(npts, la), LB(npts, lb), LH(npts, lc);
         const size_t wsw = direct_ws_words(npts, LA.data(), LB.data());
