@@ -335,10 +335,40 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     for _ in range(e2e_steps):
         rc = cm_fn(n - 2, hH.data_ptr(), DEG, hA.data_ptr(), DEG, hB.data_ptr(), P)
         assert rc == 0, rc
+    single_s = max_over_ranks(time.perf_counter() - t0, dev)
+    single_ok = product_check(ops[0][0], ops[0][1], hH.numpy().view(np.uint32))
+    # the same steps through the batched host entry point cumodp_fftmul_batch
+    # (pinned host arrays; the library pipelines each product's copies in and
+    # out against the kernels of its neighbours): step i multiplies operand
+    # set i % 4 into output region i % 4
+    sets = len(ops)
+    hF = torch.from_numpy(np.concatenate([o[0] for o in ops]).view(np.int32)).pin_memory()
+    hG = torch.from_numpy(np.concatenate([o[1] for o in ops]).view(np.int32)).pin_memory()
+    hHb = torch.empty(sets * (n - 1), dtype=torch.int32).pin_memory()
+    bfn = L.cumodp_fftmul_batch
+    bfn.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32]
+    dfa = np.full(e2e_steps, DEG, np.int32)
+    f_off = (np.arange(e2e_steps, dtype=np.int64) % sets) * (DEG + 1)
+    h_off = (np.arange(e2e_steps, dtype=np.int64) % sets) * (n - 1)
+
+    def batch_call(k):
+        rc = bfn(k, dfa.ctypes.data, f_off.ctypes.data, hF.data_ptr(), dfa.ctypes.data, f_off.ctypes.data,
+                 hG.data_ptr(), h_off.ctypes.data, hHb.data_ptr(), P)
+        assert rc == 0, rc
+    batch_call(min(4, e2e_steps))
+    if dist:
+        td.barrier()
+    t0 = time.perf_counter()
+    batch_call(e2e_steps)
     e2e_s = max_over_ranks(time.perf_counter() - t0, dev)
-    e2e_ok = product_check(ops[0][0], ops[0][1], hH.numpy().view(np.uint32))
+    e2e_ok = all(product_check(ops[k][0], ops[k][1], hHb[k * (n - 1):(k + 1) * (n - 1)].numpy().view(np.uint32))
+                 for k in range(min(sets, e2e_steps)))
     e2e = {"value": replica_throughput(world, e2e_steps, e2e_s), "unit": UNIT, "h2d_bytes_per_step": 2 * (DEG + 1) * 4,
-           "d2h_bytes_per_step": (n - 1) * 4, "steps": e2e_steps, "eval_point_identity": e2e_ok}
+           "d2h_bytes_per_step": (n - 1) * 4, "steps": e2e_steps, "eval_point_identity": e2e_ok,
+           "api": "cumodp_fftmul_batch (host arrays, pinned)",
+           "single_call": {"value": replica_throughput(world, e2e_steps, single_s), "api": "cumodp_fftmul_uni",
+                           "eval_point_identity": single_ok}}
 
     extras = {}
     if rank == 0 and not args.no_extras:

@@ -17,6 +17,7 @@
 //     replayed; job tables live in device memory and are refreshed with one
 //     copy when the caller's pointers change.
 #include <algorithm>
+#include <map>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -536,6 +537,77 @@ int subproduct_level_dev(long long l, long long npairs, const u32* in, u32* out,
     return cuda_err(cudaGetLastError());
 }
 
+// Host-buffer batch of large products, pipelined: product i's operands are
+// copied in on one stream, its kernels run on the library stream, its result
+// is copied out on a third stream, so the copies of products i+1 and i-1
+// (both directions of the host link at once) overlap the kernels of product
+// i.  Three device slots (operands and result) rotate; a slot is refilled
+// only after the result copy that last used it has finished.
+int pipelined_host_batch(int count, const sfixn* df, const int64_t* f_off, const u32* F, const sfixn* dg,
+                         const int64_t* g_off, const u32* G, const int64_t* h_off, u32* H, u32 p, cudaStream_t st) {
+    constexpr int kSlots = 3;
+    const int dev = current_device();
+    long long maxa = 0, maxb = 0, maxh = 0;
+    for (int i = 0; i < count; ++i) {
+        maxa = std::max<long long>(maxa, (long long)df[i] + 1);
+        maxb = std::max<long long>(maxb, (long long)dg[i] + 1);
+        maxh = std::max<long long>(maxh, (long long)df[i] + dg[i] + 1);
+    }
+    const size_t slot_words = (size_t)(maxa + maxb + maxh);
+    int err = OK;
+    u32* d = (u32*)workspace(dev, kWsBatch, kSlots * slot_words * sizeof(u32), &err);
+    if (!d) return err;
+    struct Streams {
+        cudaStream_t in, out;
+        cudaEvent_t in_done[kSlots], comp_done[kSlots], out_done[kSlots];
+    };
+    static std::map<int, Streams*> per_dev;  // guarded by lib_mutex
+    Streams*& S = per_dev[dev];
+    if (!S) {
+        S = new Streams();
+        cudaStreamCreateWithFlags(&S->in, cudaStreamNonBlocking);
+        cudaStreamCreateWithFlags(&S->out, cudaStreamNonBlocking);
+        for (int k = 0; k < kSlots; ++k) {
+            cudaEventCreateWithFlags(&S->in_done[k], cudaEventDisableTiming);
+            cudaEventCreateWithFlags(&S->comp_done[k], cudaEventDisableTiming);
+            cudaEventCreateWithFlags(&S->out_done[k], cudaEventDisableTiming);
+        }
+    }
+    // nothing of an earlier call may still use the slots
+    cudaEventRecord(S->out_done[0], st);
+    cudaStreamWaitEvent(S->in, S->out_done[0], 0);
+    cudaStreamWaitEvent(S->out, S->out_done[0], 0);
+    for (int i = 0; i < count && err == OK; ++i) {
+        const int k = i % kSlots;
+        u32* a = d + (size_t)k * slot_words;
+        u32* b = a + maxa;
+        u32* h = b + maxb;
+        const long long la = (long long)df[i] + 1, lb = (long long)dg[i] + 1, lh = la + lb - 1;
+        if (i >= kSlots) cudaStreamWaitEvent(S->in, S->out_done[k], 0);
+        cudaError_t ce = cudaMemcpyAsync(a, F + f_off[i], la * 4, cudaMemcpyHostToDevice, S->in);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(b, G + g_off[i], lb * 4, cudaMemcpyHostToDevice, S->in);
+        if (ce != cudaSuccess) {
+            err = cuda_err(ce);
+            break;
+        }
+        cudaEventRecord(S->in_done[k], S->in);
+        cudaStreamWaitEvent(st, S->in_done[k], 0);
+        if ((err = mul_dev(a, la, b, lb, h, lh, p, st)) != OK) break;
+        cudaEventRecord(S->comp_done[k], st);
+        cudaStreamWaitEvent(S->out, S->comp_done[k], 0);
+        ce = cudaMemcpyAsync(H + h_off[i], h, lh * 4, cudaMemcpyDeviceToHost, S->out);
+        if (ce != cudaSuccess) {
+            err = cuda_err(ce);
+            break;
+        }
+        cudaEventRecord(S->out_done[k], S->out);
+    }
+    cudaStreamSynchronize(S->in);
+    cudaStreamSynchronize(st);
+    cudaStreamSynchronize(S->out);
+    return err;
+}
+
 }  // namespace cmb
 
 using namespace cmb;
@@ -586,12 +658,19 @@ cumodp_err cumodp_fftmul_batch(int count, const sfixn* df, const int64_t* f_off,
     const int dev = current_device();
     cudaStream_t st = lib_stream(dev);
     // extents of the three host arrays
-    size_t nf = 0, ng = 0, nh = 0;
+    size_t nf = 0, ng = 0, nh = 0, total = 0;
     for (int i = 0; i < count; ++i) {
         if (df[i] < 0 || dg[i] < 0 || f_off[i] < 0 || g_off[i] < 0 || h_off[i] < 0) return CUMODP_ASSUMPTION_ERROR;
         nf = std::max(nf, (size_t)f_off[i] + df[i] + 1);
         ng = std::max(ng, (size_t)g_off[i] + dg[i] + 1);
         nh = std::max(nh, (size_t)h_off[i] + df[i] + dg[i] + 1);
+        total += (size_t)df[i] + dg[i] + 2;
+    }
+    // several large products: pipeline the host copies against the kernels
+    if (count > 1 && total / count >= (1u << 20)) {
+        const int err = pipelined_host_batch(count, df, f_off, (const u32*)F, dg, g_off, (const u32*)G, h_off,
+                                             (u32*)H, (u32)p, st);
+        return (cumodp_err)err;
     }
     int err = OK;
     u32* d = (u32*)workspace(dev, kWsBatch, (nf + ng + nh) * sizeof(u32), &err);

@@ -63,3 +63,20 @@ def test_batch_rejects_oversize(cm):
     with pytest.raises(cm.CumodpError) as e:
         cm.fftmul_batch([(a, a)], 257)
     assert e.value.code == cm.FFT_SIZE_TOO_LARGE
+
+
+def test_large_host_batch_is_pipelined_and_exact(cm, oracle_mod):
+    """Host-buffer batch of large products (the pipelined copy path): every product
+    equals the single-call path, one checked against the oracle; more products
+    than device slots, mixed sizes, one shared operand."""
+    r = SplitMix64(0xC0DA0501)
+    shared = r.residues((1 << 19) + 7, P0)
+    pairs = [(r.residues((1 << 19), P0), r.residues((1 << 19), P0)),
+             (r.residues(700001, P0), r.residues(400000, P0)),
+             (shared, r.residues((1 << 20) - 5, P0)),
+             (r.residues(1 << 20, P0), shared),
+             (r.residues(600000, P0), r.residues(600000, P0))]
+    outs = cm.fftmul_batch(pairs, P0)
+    for (a, b), h in zip(pairs, outs):
+        assert np.array_equal(h, cm.fftmul_uni(a, b, P0))
+    assert np.array_equal(outs[1], oracle_mod.polymul(pairs[1][0], pairs[1][1], P0))
