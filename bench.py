@@ -326,7 +326,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     cm_fn = L.cumodp_fftmul_uni
     cm_fn.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32,
                       ctypes.c_void_p, ctypes.c_int32]
-    e2e_steps = max(3, min(args.steps, 20))
+    e2e_steps = max(3, min(args.steps, 40))
     for _ in range(2):
         cm_fn(n - 2, hH.data_ptr(), DEG, hA.data_ptr(), DEG, hB.data_ptr(), P)
     if dist:
@@ -713,6 +713,23 @@ def cpu_baseline():
                       f"({secs:.1f} s wall)"}
 
 
+def run_leg(name: str) -> None:
+    import torch
+    import cumodp_b200 as cm
+    dev = torch.device("cuda:0")
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    hbm_peak, _ = peaks()
+    with torch.cuda.stream(stream):
+        fn = {"ntt": lambda: ntt_2_24(cm, torch, dev, stream, hbm_peak),
+              "c1": lambda: c1_latency(cm, torch, dev, stream),
+              "c3": lambda: c3_exact(cm, torch, dev, stream),
+              "c4": lambda: batched_c4(cm, torch, dev, stream),
+              "big": lambda: big_coefficients(cm, torch, dev, stream),
+              "serving": lambda: serving_c5(cm)}[name]
+        print(json.dumps({"leg": name, "result": fn()}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -721,8 +738,13 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-extras", action="store_true",
                     help="headline only (no e2e extras, transform, batch or CPU legs); for profiling")
+    ap.add_argument("--leg", choices=["ntt", "c1", "c3", "c4", "big", "serving"],
+                    help="run only this extra leg and print its result (for profiling it alone)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.leg:
+        run_leg(args.leg)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

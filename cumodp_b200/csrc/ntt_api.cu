@@ -56,15 +56,23 @@ __device__ __forceinline__ u32 row_pos_to_freq(u32 P) {
     return f;
 }
 
+// One row of the natural-order transform per CTA: the row (a column-pass
+// output row, or an independent row) is copied into shared memory with
+// cp.async, level 0 applies the inter-pass twiddle w_n^(k1 c) (or reduces
+// the input), the remaining levels run as in the product kernels, and the
+// last level leaves each thread one 32-word group in registers; after a
+// barrier the groups are written back at their natural positions in the same
+// buffer, and the row is stored with 16-byte accesses.
 template <int L2>
-__global__ void __launch_bounds__(small_threads(L2), 1) k_row_ntt(const __grid_constant__ RowNttArgs A) {
+__global__ void __launch_bounds__(ntt_row_threads(L2), ntt_row_ctas(L2)) k_row_ntt(const __grid_constant__ RowNttArgs A) {
     constexpr int n2 = 1 << L2;
-    constexpr int T = small_threads(L2);
+    constexpr int T = ntt_row_threads(L2);
     constexpr LevelPlan PL = row_plan(L2);
     static_assert(PL.nlev >= 2, "row transform needs two levels");
+    static_assert(T * 32 >= n2, "one last-level group per thread");
     using LV0 = SmallLevel<L2, 0>;
     constexpr int R0 = LV0::R, TB0 = LV0::TB;
-    extern __shared__ __align__(16) u32 sm[];  // [levels | natural order]
+    extern __shared__ __align__(16) u32 sm[];
     __shared__ Tw bf[R0];
 
     const u32 s = blockIdx.x;
@@ -78,15 +86,16 @@ __global__ void __launch_bounds__(small_threads(L2), 1) k_row_ntt(const __grid_c
         const u32 v = red1(mul_mont(seed_mont_at(A.seeds, A.nlo, e, p, pinv), 1u, p, pinv), p);
         bf[threadIdx.x] = Tw{v, (u32)(((u64)v << 32) / p)};
     }
+    row_load<L2, T>(sm, A.src + (size_t)s * n2);
     __syncthreads();
 
-    const u32* row = A.src + (size_t)s * n2;
     for (int o = threadIdx.x; o < TB0; o += T) {
         u32 x[R0];
         const u32 mo = twid ? seed_mont_at(A.seeds, A.nlo, (k1 * (u32)o) & nmask, p, pinv) : 0u;
+        const int bs = swz(o);
 #pragma unroll
         for (int m = 0; m < R0; ++m) {
-            const u32 v = row[o + TB0 * m];
+            const u32 v = sm[swz_task<TB0, n2>(o, bs, m)];
             if (twid) x[m] = mul_mont(v, mul_shoup(mo, bf[m].w, bf[m].wq, p), p, pinv);
             else x[m] = mul_shoup(v, 1u, A.pk.one_q, p);
         }
@@ -96,26 +105,56 @@ __global__ void __launch_bounds__(small_threads(L2), 1) k_row_ntt(const __grid_c
 #pragma unroll
         for (int j = 1; j < R0; ++j) x[j] = mul_shoup(x[j], t[j].w, t[j].wq, p);
 #pragma unroll
-        for (int m = 0; m < R0; ++m) sm[swz_task<TB0, n2>(o, swz(o), m)] = x[m];
+        for (int m = 0; m < R0; ++m) sm[swz_task<TB0, n2>(o, bs, m)] = x[m];
     }
     __syncthreads();
     fwd1_levels<L2, 1, T>(sm, A.pk, A.twr);
 
-    for (int r = threadIdx.x; r < n2 / 32; r += T) {
-        u32 x[32];
+    const int r = threadIdx.x;
+    const bool has = r < n2 / 32;
+    u32 x[32];
+    if (has) {
         load_row32(x, sm, r * 32);
         dif_regs<32>(x, A.pk.rc.f, p, p2);
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-            const u32 f = row_pos_to_freq<L2>((u32)(r * 32 + j));
-            sm[n2 + swz((int)f)] = red1(mul_shoup(x[j], A.scale.w, A.scale.wq, p), p);
-        }
+        for (int j = 0; j < 32; ++j) x[j] = red1(mul_shoup(x[j], A.scale.w, A.scale.wq, p), p);
+    }
+    __syncthreads();
+    if (has) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) sm[swz((int)row_pos_to_freq<L2>((u32)(r * 32 + j)))] = x[j];
     }
     __syncthreads();
     u32* out = A.dst + (size_t)out_row * n2;
-    for (int i = threadIdx.x * 4; i < n2; i += T * 4) {
-        uint4 v = *reinterpret_cast<const uint4*>(sm + n2 + swz(i));
-        *reinterpret_cast<uint4*>(out + i) = v;
+    for (int i = threadIdx.x * 4; i < n2; i += T * 4)
+        *reinterpret_cast<uint4*>(out + i) = *reinterpret_cast<const uint4*>(sm + swz(i));
+}
+
+// out[c * rows + r] = in[r * cols + c] for rows and cols multiples of 64:
+// 64 x 64 tiles through shared memory, 16-byte loads and stores, 256
+// threads (16 x 16, four 4-word groups each).
+__global__ void __launch_bounds__(256) k_transpose64(const u32* __restrict__ in, u32* __restrict__ out, int rows,
+                                                     int cols) {
+    __shared__ u32 t[64][65];
+    const size_t c0 = (size_t)blockIdx.x * 64, r0 = (size_t)blockIdx.y * 64;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const u32* src = in + r0 * cols + c0 + 4 * tx;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int rr = ty + 16 * k;
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(src + (size_t)rr * cols));
+        t[rr][4 * tx] = v.x;
+        t[rr][4 * tx + 1] = v.y;
+        t[rr][4 * tx + 2] = v.z;
+        t[rr][4 * tx + 3] = v.w;
+    }
+    __syncthreads();
+    u32* dst = out + c0 * rows + r0 + 4 * tx;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int cc = ty + 16 * k;
+        const uint4 v = make_uint4(t[4 * tx][cc], t[4 * tx + 1][cc], t[4 * tx + 2][cc], t[4 * tx + 3][cc]);
+        *reinterpret_cast<uint4*>(dst + (size_t)cc * rows) = v;
     }
 }
 
@@ -151,13 +190,13 @@ namespace {
 
 template <int L2>
 void launch_row_ntt_t(const RowNttArgs& a, int rows, cudaStream_t st) {
-    const size_t smem = (size_t)2 * (1 << L2) * sizeof(u32);
+    const size_t smem = (size_t)(1 << L2) * sizeof(u32);
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_row_ntt<L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    k_row_ntt<L2><<<rows, small_threads(L2), smem, st>>>(a);
+    k_row_ntt<L2><<<rows, ntt_row_threads(L2), smem, st>>>(a);
 }
 typedef void (*RowNttFn)(const RowNttArgs&, int, cudaStream_t);
 const RowNttFn kRowNtt[15] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
@@ -220,6 +259,7 @@ int ntt_natural_dev(const u32* x_in, u32* x_out, int k, u32 w, u32 p, bool inver
     const PrimeCtx* pc = prime_ctx(p, &err);
     if (!pc) return err;
     if (k < 0) return ASSUMPTION_ERROR;
+    if (k >= 6 && (((uintptr_t)x_in | (uintptr_t)x_out) & 15)) return ASSUMPTION_ERROR;  // 16-byte rows
     if (k > pc->info.two_adic) return FFT_SIZE_TOO_LARGE;
     if (!root_has_order(w, k, p)) return ASSUMPTION_ERROR;
     if (k > kMaxLog) return FFT_SIZE_TOO_LARGE;
@@ -275,7 +315,10 @@ int ntt_natural_dev(const u32* x_in, u32* x_out, int k, u32 w, u32 p, bool inver
     kRowNtt[l2](A, 1 << l1, st);
     if (tr) pass_timing_end(st, "ntt_row", e0);
     tr = pass_timing_begin(st, &e0);
-    k_transpose<<<dim3((1 << l2) / 32, (1 << l1) / 32), dim3(32, 8), 0, st>>>(w2, x_out, 1 << l1, 1 << l2);
+    if (l1 >= 6)
+        k_transpose64<<<dim3((1 << l2) / 64, (1 << l1) / 64), 256, 0, st>>>(w2, x_out, 1 << l1, 1 << l2);
+    else
+        k_transpose<<<dim3((1 << l2) / 32, (1 << l1) / 32), dim3(32, 8), 0, st>>>(w2, x_out, 1 << l1, 1 << l2);
     if (tr) pass_timing_end(st, "ntt_transpose", e0);
     return cuda_err(cudaGetLastError());
 }
@@ -287,6 +330,7 @@ int list_ntt_dev(u32* x, long long m, int k, u32 w, u32 p, bool inverse, cudaStr
     const PrimeCtx* pc = prime_ctx(p, &err);
     if (!pc) return err;
     if (m < 0 || k < 0) return ASSUMPTION_ERROR;
+    if (k >= 6 && ((uintptr_t)x & 15)) return ASSUMPTION_ERROR;  // 16-byte rows
     if (m == 0) return OK;
     if (k > pc->info.two_adic) return FFT_SIZE_TOO_LARGE;
     if (!root_has_order(w, k, p)) return ASSUMPTION_ERROR;
@@ -327,6 +371,7 @@ int bivariate_dev(u32* x, int em, u32 wm, int en, u32 wn, u32 p, bool inverse, c
     const PrimeCtx* pc = prime_ctx(p, &err);
     if (!pc) return err;
     if (em < 0 || en < 0) return ASSUMPTION_ERROR;
+    if ((uintptr_t)x & 15) return ASSUMPTION_ERROR;  // 16-byte rows
     if (em > pc->info.two_adic || en > pc->info.two_adic) return FFT_SIZE_TOO_LARGE;
     if (!root_has_order(wm, em, p) || !root_has_order(wn, en, p)) return ASSUMPTION_ERROR;
     if (en < 6) return FFT_SIZE_TOO_SMALL;
@@ -410,13 +455,15 @@ int bivariate_mul_dev(u32* F, u32* G, int em, int en, u32 p, cudaStream_t st) {
     const PrimeCtx* pc = prime_ctx(p, &err);
     if (!pc) return err;
     if (em < 0 || en < 0) return ASSUMPTION_ERROR;
+    if ((em >= 6 || en >= 6) && (((uintptr_t)F | (uintptr_t)G) & 15)) return ASSUMPTION_ERROR;  // 16-byte rows
     if (em > pc->info.two_adic || en > pc->info.two_adic || em + en > 30) return FFT_SIZE_TOO_LARGE;
     const long long m = 1ll << em, n = 1ll << en, total = m * n;
     const u32 wm = em ? canonical_root(*pc, em) : 1u, wn = en ? canonical_root(*pc, en) : 1u;
     const int dev = current_device();
-    u32* ws = (u32*)workspace(dev, kWsBiv, (size_t)2 * total * sizeof(u32), &err);
+    const long long tpad = (total + 3) & ~3ll;  // 16-byte aligned halves
+    u32* ws = (u32*)workspace(dev, kWsBiv, (size_t)2 * tpad * sizeof(u32), &err);
     if (!ws) return err;
-    u32 *W1 = ws, *W2 = ws + total;
+    u32 *W1 = ws, *W2 = ws + tpad;
     const dim3 tb(32, 8);
     const dim3 g_mn((unsigned)((n + 31) / 32), (unsigned)((m + 31) / 32));  // m rows x n columns
     const dim3 g_nm((unsigned)((m + 31) / 32), (unsigned)((n + 31) / 32));  // n rows x m columns
@@ -445,9 +492,10 @@ int bivariate_product_dev(const u32* F, int nxf, int nyf, const u32* G, int nxg,
     while ((1ll << ey) < ly) ++ey;
     if (ex + ey > 30) return FFT_SIZE_TOO_LARGE;
     const long long total = 1ll << (ex + ey);
-    u32* ws = (u32*)workspace(current_device(), kWsBivHost, (size_t)2 * total * sizeof(u32), &err);
+    const long long tpad = (total + 3) & ~3ll;  // 16-byte aligned halves
+    u32* ws = (u32*)workspace(current_device(), kWsBivHost, (size_t)2 * tpad * sizeof(u32), &err);
     if (!ws) return err;
-    u32 *F2 = ws, *G2 = ws + total;
+    u32 *F2 = ws, *G2 = ws + tpad;
     k_expand2<<<grid_for(total), 256, 0, st>>>(F, nxf, nyf, F2, ex, ey, p);
     k_expand2<<<grid_for(total), 256, 0, st>>>(G, nxg, nyg, G2, ex, ey, p);
     if ((err = bivariate_mul_dev(F2, G2, ey, ex, p, st)) != OK) return err;

@@ -116,6 +116,12 @@ __host__ __device__ constexpr int row_threads(int logl) { return logl == 14 ? 10
 // threads (up to 85 registers each) and three CTAs per SM, so that the load,
 // compute and store phases of three rows overlap on every SM.
 __host__ __device__ constexpr int rowsplit_threads(int logl) { return logl == 14 ? 256 : logl >= 10 ? (1 << (logl - 5)) : 32; }
+// Natural-order row transforms (k_row_ntt): one thread per 32-word group of
+// the last level (at least a warp), one row of shared memory per CTA, 1024
+// threads per SM.
+__host__ __device__ constexpr int ntt_row_threads(int logl) { return logl >= 10 ? (1 << (logl - 5)) : 32; }
+__host__ __device__ constexpr int ntt_row_ctas(int logl) { return 1024 / ntt_row_threads(logl) < 32 ? 1024 / ntt_row_threads(logl) : 32; }
+
 // Resident CTAs per SM the split row kernels are compiled for: three for
 // 2^14-word rows, else enough for 1024 threads per SM (64 registers).
 __host__ __device__ constexpr int rowsplit_ctas(int logl) { return logl == 14 ? 3 : (1024 / rowsplit_threads(logl) < 32 ? 1024 / rowsplit_threads(logl) : 32); }

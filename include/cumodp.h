@@ -261,12 +261,14 @@ void cumodp_server_destroy(cumodp_server *s);
 
 /* Addition.  Device-pointer natural-order transform on a caller stream (0 =
  * the library's stream, then synchronised): forward as cumodp_fft_uni, or
- * the inverse of it when `inverse` is nonzero.  X is a DEVICE pointer. */
+ * the inverse of it when `inverse` is nonzero.  X is a DEVICE pointer,
+ * 16-byte aligned (as cudaMalloc returns) when k >= 6. */
 cumodp_err cumodp_fft_uni_dev(sfixn *X, sfixn n, sfixn k, sfixn w, sfixn p, int inverse, void *stream);
 
 /* Addition.  The list transform I_m (x) DFT_n: m independent natural-order
  * transforms of length n = 2^k of the DEVICE array X (row i at X + i n), in
- * place, root w (inverse: w^-1 and scaling by n^-1).  Counterpart of the
+ * place, root w (inverse: w^-1 and scaling by n^-1); X 16-byte aligned when
+ * k >= 6.  Counterpart of the
  * reference's C++ list_stockham_dev (src/list_stockham.cu:595-665, declared
  * in include/list_stockham.h:48-49; include/list_stockham_b200.h here gives
  * the same C++ signatures) without its grid bug for m * n / 128 > 2^15 and
@@ -278,7 +280,7 @@ cumodp_err cumodp_list_fft_dev(sfixn *X, sfixn m, sfixn k, sfixn w, sfixn p, int
  * j, of 2^en words, holds the coefficients of y^j; x^i at column i):
  * F <- DFT^-1(DFT F * DFT G), the 2-D cyclic convolution, which is the
  * bivariate product when both operands are zero-padded to the product's
- * size.  G is overwritten.  Counterpart of the reference's C++
+ * size.  G is overwritten; F and G 16-byte aligned.  Counterpart of the reference's C++
  * bi_stockham_poly_mul_dev (src/list_stockham.cu:1317-1348, declared in
  * include/list_stockham.h:103-104; include/list_stockham_b200.h gives that
  * signature), for any em, en within the prime's 2-adic order (em + en <= 30).
