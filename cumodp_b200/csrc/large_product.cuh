@@ -90,7 +90,7 @@ __device__ __forceinline__ u32 col_slot_to_k1(u32 s, const LevelPlan& PL, int L1
 // broadcast to the (half-)warp.
 
 // Word offset of tile row r.
-template <int L1, bool INV>
+template <int L1, int INV>
 __device__ __forceinline__ int tile_row(int r) {
     constexpr int TC = col_tile_cols(L1, INV);
     if constexpr (TC == 32) return r * 32;
@@ -102,7 +102,7 @@ __device__ __forceinline__ int tile_row(int r) {
 // the task index): a constant.  Every non-last level of a column plan has TB
 // a multiple of the padding period; the last level has TB = 1 and blocks of
 // exactly one period.
-template <int L1, bool INV, int TB>
+template <int L1, int INV, int TB>
 __device__ __forceinline__ constexpr int tile_step(int m) {
     constexpr int TC = col_tile_cols(L1, INV), PAD = 1 << col_pad_log(L1);
     if constexpr (TC == 32) return TB * m * 32;
@@ -117,7 +117,7 @@ __device__ __forceinline__ constexpr int tile_step(int m) {
 // rows entirely past `len` are zero-filled without loads.
 // With ASYNC (and no reduction) the full rows are copied with cp.async,
 // global to shared without a register round trip.
-template <int L1, bool INV, int T, bool ASYNC = false>
+template <int L1, int INV, int T, bool ASYNC = false>
 __device__ __forceinline__ void tile_load(u32* tile, const u32* __restrict__ src, long long len, int c0, int n2,
                                           bool reduce, const PrimeK& pk) {
     constexpr int n1 = 1 << L1, TC = col_tile_cols(L1, INV), QR = TC / 4;
@@ -171,7 +171,7 @@ __device__ __forceinline__ void tile_load(u32* tile, const u32* __restrict__ src
 }
 
 // Bulk-stores the tile; `final` reduces to [0, p) and stops at `len`.
-template <int L1, bool INV, int T>
+template <int L1, int INV, int T>
 __device__ __forceinline__ void tile_store(const u32* tile, u32* __restrict__ dst, long long len, int c0, int n2,
                                            bool final, const PrimeK& pk) {
     constexpr int n1 = 1 << L1, TC = col_tile_cols(L1, INV), QR = TC / 4;
@@ -208,15 +208,16 @@ __device__ __forceinline__ void tile_store(const u32* tile, u32* __restrict__ ds
     }
 }
 
-// Forward column level LEV, shared memory to shared memory.
-template <int L1, int LEV, int NW>
+// Forward column level LEV, shared memory to shared memory, on a tile of
+// kind KIND (col_tile_cols).
+template <int L1, int LEV, int NW, int KIND = 0>
 __device__ __forceinline__ void col_fwd_level(u32* tile, const PrimeK& pk, const Tw* __restrict__ twc) {
     using LV = ColLevel<L1, LEV>;
     constexpr LevelPlan PL = col_plan(L1);
     constexpr int R = LV::R, TB = LV::TB, B = LV::B;
     constexpr bool LAST = LEV + 1 == PL.nlev;
     constexpr int TASKS = (1 << L1) / R;
-    constexpr bool INV = false;
+    constexpr int INV = KIND;
     constexpr int TC = col_tile_cols(L1, INV), SUB = 32 / TC;
     const u32 p = pk.p, p2 = pk.p2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -242,13 +243,13 @@ __device__ __forceinline__ void col_fwd_level(u32* tile, const PrimeK& pk, const
     }
 }
 
-template <int L1, int LEV, int NW>
+template <int L1, int LEV, int NW, int KIND = 0>
 __device__ __forceinline__ void col_fwd_levels(u32* tile, const PrimeK& pk, const Tw* __restrict__ twc) {
     constexpr LevelPlan PL = col_plan(L1);
     if constexpr (LEV < PL.nlev) {
-        col_fwd_level<L1, LEV, NW>(tile, pk, twc);
+        col_fwd_level<L1, LEV, NW, KIND>(tile, pk, twc);
         __syncthreads();
-        col_fwd_levels<L1, LEV + 1, NW>(tile, pk, twc);
+        col_fwd_levels<L1, LEV + 1, NW, KIND>(tile, pk, twc);
     }
 }
 
@@ -260,7 +261,7 @@ __device__ __forceinline__ void col_inv_level(u32* tile, const PrimeK& pk, const
     constexpr int R = LV::R, TB = LV::TB, B = LV::B;
     constexpr bool DEEPEST = LEV + 1 == PL.nlev;
     constexpr int TASKS = (1 << L1) / R;
-    constexpr bool INV = true;
+    constexpr int INV = 1;
     constexpr int TC = col_tile_cols(L1, INV), SUB = 32 / TC;
     const u32 p = pk.p, p2 = pk.p2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -295,9 +296,10 @@ __device__ __forceinline__ void col_inv_levels(u32* tile, const PrimeK& pk, cons
     }
 }
 
-// pass A, grid: (n2/TC column tiles, operands, jobs)
-template <int L1, int NW>
-__global__ void __launch_bounds__(NW * 32, col_ctas(L1, false)) k_col_fwd(const __grid_constant__ LargeArgs A) {
+// pass A, grid: (n2/TC column tiles, operands, jobs); KIND 0 for a product's
+// operands, 2 for the forward pass of a natural-order transform
+template <int L1, int NW, int KIND = 0>
+__global__ void __launch_bounds__(NW * 32, col_ctas(L1, KIND)) k_col_fwd(const __grid_constant__ LargeArgs A) {
     extern __shared__ __align__(16) u32 tile[];
     const LargeJob& J = A.jobs ? A.jobs[blockIdx.z] : A.job0;
     const int op = blockIdx.y;
@@ -305,16 +307,16 @@ __global__ void __launch_bounds__(NW * 32, col_ctas(L1, false)) k_col_fwd(const 
     const int len = op ? J.lb : J.la;
     u32* dst = op ? J.wb : J.wa;
     const int n2 = 1 << A.l2;
-    const int c0 = blockIdx.x * col_tile_cols(L1, false);
+    const int c0 = blockIdx.x * col_tile_cols(L1, KIND);
     // the plan's twiddles (broadcast reads) next to the tile
     constexpr int NTW = col_tw_entries(L1);
-    Tw* tws = reinterpret_cast<Tw*>(tile + col_tile_words(L1, false));
+    Tw* tws = reinterpret_cast<Tw*>(tile + col_tile_words(L1, KIND));
     for (int i = threadIdx.x; i < NTW; i += NW * 32) tws[i] = A.twc[i];
     // reduced while loaded (an input row half made of padding costs nothing)
-    tile_load<L1, false, NW * 32>(tile, src, len, c0, n2, true, A.pkc);
+    tile_load<L1, KIND, NW * 32>(tile, src, len, c0, n2, true, A.pkc);
     __syncthreads();
-    col_fwd_levels<L1, 0, NW>(tile, A.pkc, tws);
-    tile_store<L1, false, NW * 32>(tile, dst, 1ll << (L1 + A.l2), c0, n2, false, A.pkc);
+    col_fwd_levels<L1, 0, NW, KIND>(tile, A.pkc, tws);
+    tile_store<L1, KIND, NW * 32>(tile, dst, 1ll << (L1 + A.l2), c0, n2, false, A.pkc);
 }
 
 // pass C, grid: (n2/TC column tiles, 1, jobs)

@@ -207,13 +207,14 @@ const RowNttFn kRowNtt[15] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullp
 // Forward-column launchers shared with the product path (single operand).
 template <int L1>
 void launch_colfwd1_t(const LargeArgs& a, int tiles, cudaStream_t st) {
-    const size_t smem = col_smem_bytes(L1, false);
+    const size_t smem = col_smem_bytes(L1, 2);
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_col_fwd<L1, col_warps(L1, false)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_col_fwd<L1, col_warps(L1, 2), 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
         attr = true;
     }
-    k_col_fwd<L1, col_warps(L1, false)><<<dim3(tiles, 1, 1), col_warps(L1, false) * 32, smem, st>>>(a);
+    k_col_fwd<L1, col_warps(L1, 2), 2><<<dim3(tiles, 1, 1), col_warps(L1, 2) * 32, smem, st>>>(a);
 }
 typedef void (*ColFn)(const LargeArgs&, int, cudaStream_t);
 const ColFn kColFwd1[11] = {nullptr, launch_colfwd1_t<1>, launch_colfwd1_t<2>, launch_colfwd1_t<3>,
@@ -247,7 +248,7 @@ int column_pass(const PrimeCtx& pc, u32 root_c, int l1, int l2, const u32* src, 
     A.colpl = col_plan(l1);
     A.job0 = LargeJob{src, nullptr, nullptr, (int)std::min<long long>(len, 1ll << 30), 0, 0, 0, dst, nullptr};
     A.njobs = 1;
-    kColFwd1[l1](A, (1 << l2) / col_tile_cols_rt(l1, false), st);
+    kColFwd1[l1](A, (1 << l2) / col_tile_cols_rt(l1, 2), st);
     return OK;
 }
 

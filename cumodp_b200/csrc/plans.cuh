@@ -55,42 +55,44 @@ __host__ __device__ constexpr int col_tw_entries(int logl) {
 }
 // Column tiles: col_tile_cols adjacent columns x 2^logl rows in shared
 // memory, processed by col_warps warps, col_ctas resident CTAs per SM, each
-// chosen per direction (inv: the inverse column pass).  32-column tiles put
+// chosen per kind of pass (0: the product's forward pass, whose operands are
+// half zero padding; 1: the inverse pass; 2: the forward pass of a
+// natural-order transform).  32-column tiles put
 // one column on each lane; 16-column tiles put two tasks on each warp (one
 // per half-warp) and insert a 16-word pad after every 2^col_pad_log rows (the
 // plan's last radix), so that the two half-warps always read opposite halves
-// of the banks.  The inverse pass over 2^10-row tiles uses 16 columns and
-// two CTAs per SM (their load, compute and store phases overlap); the
-// forward pass keeps 32 columns (its loads skip the zero-padded half).
-__host__ __device__ constexpr int col_tile_cols(int logl, bool inv) { return inv && logl == 10 ? 16 : 32; }
-__host__ __device__ constexpr int col_warps(int logl, bool inv) { return logl == 10 && !inv ? 32 : 16; }
-__host__ __device__ constexpr int col_ctas(int logl, bool inv) { return inv && logl == 10 ? 2 : 1; }
+// of the banks.  Kinds 1 and 2 over 2^10-row tiles use 16 columns and two
+// CTAs per SM (their load, compute and store phases overlap); kind 0 keeps
+// 32 columns (its loads skip the zero-padded half).
+__host__ __device__ constexpr int col_tile_cols(int logl, int kind) { return kind != 0 && logl == 10 ? 16 : 32; }
+__host__ __device__ constexpr int col_warps(int logl, int kind) { return logl == 10 && kind == 0 ? 32 : 16; }
+__host__ __device__ constexpr int col_ctas(int logl, int kind) { return kind != 0 && logl == 10 ? 2 : 1; }
 __host__ __device__ constexpr int col_pad_log(int logl) { return col_plan(logl).logr[col_plan(logl).nlev - 1]; }
-__host__ __device__ constexpr int col_tile_words(int logl, bool inv) {
-    return col_tile_cols(logl, inv) == 32
+__host__ __device__ constexpr int col_tile_words(int logl, int kind) {
+    return col_tile_cols(logl, kind) == 32
                ? (32 << logl)
-               : ((1 << logl) + ((1 << logl) >> col_pad_log(logl))) * col_tile_cols(logl, inv);
+               : ((1 << logl) + ((1 << logl) >> col_pad_log(logl))) * col_tile_cols(logl, kind);
 }
 // Whether a column CTA stages its twiddles in shared memory next to the
 // tile (else the levels read them from global memory, as broadcasts).
-__host__ __device__ constexpr bool col_tw_smem(int logl, bool inv) { return true; }
+__host__ __device__ constexpr bool col_tw_smem(int logl, int kind) { return true; }
 // col_tile_cols for a run-time logl.
-__host__ __device__ inline int col_tile_cols_rt(int logl, bool inv) {
-    constexpr int f[13] = {col_tile_cols(0, false), col_tile_cols(1, false), col_tile_cols(2, false),
-                           col_tile_cols(3, false), col_tile_cols(4, false), col_tile_cols(5, false),
-                           col_tile_cols(6, false), col_tile_cols(7, false), col_tile_cols(8, false),
-                           col_tile_cols(9, false), col_tile_cols(10, false), col_tile_cols(11, false),
-                           col_tile_cols(12, false)};
-    constexpr int i[13] = {col_tile_cols(0, true), col_tile_cols(1, true), col_tile_cols(2, true),
-                           col_tile_cols(3, true), col_tile_cols(4, true), col_tile_cols(5, true),
-                           col_tile_cols(6, true), col_tile_cols(7, true), col_tile_cols(8, true),
-                           col_tile_cols(9, true), col_tile_cols(10, true), col_tile_cols(11, true),
-                           col_tile_cols(12, true)};
-    return inv ? i[logl] : f[logl];
+__host__ __device__ inline int col_tile_cols_rt(int logl, int kind) {
+    constexpr int t[3][13] = {
+        {col_tile_cols(0, 0), col_tile_cols(1, 0), col_tile_cols(2, 0), col_tile_cols(3, 0), col_tile_cols(4, 0),
+         col_tile_cols(5, 0), col_tile_cols(6, 0), col_tile_cols(7, 0), col_tile_cols(8, 0), col_tile_cols(9, 0),
+         col_tile_cols(10, 0), col_tile_cols(11, 0), col_tile_cols(12, 0)},
+        {col_tile_cols(0, 1), col_tile_cols(1, 1), col_tile_cols(2, 1), col_tile_cols(3, 1), col_tile_cols(4, 1),
+         col_tile_cols(5, 1), col_tile_cols(6, 1), col_tile_cols(7, 1), col_tile_cols(8, 1), col_tile_cols(9, 1),
+         col_tile_cols(10, 1), col_tile_cols(11, 1), col_tile_cols(12, 1)},
+        {col_tile_cols(0, 2), col_tile_cols(1, 2), col_tile_cols(2, 2), col_tile_cols(3, 2), col_tile_cols(4, 2),
+         col_tile_cols(5, 2), col_tile_cols(6, 2), col_tile_cols(7, 2), col_tile_cols(8, 2), col_tile_cols(9, 2),
+         col_tile_cols(10, 2), col_tile_cols(11, 2), col_tile_cols(12, 2)}};
+    return t[kind][logl];
 }
 // Dynamic shared memory of a column CTA: the tile and its twiddles.
-__host__ __device__ constexpr int col_smem_bytes(int logl, bool inv) {
-    return col_tile_words(logl, inv) * 4 + (col_tw_smem(logl, inv) ? col_tw_entries(logl) * 8 : 0);
+__host__ __device__ constexpr int col_smem_bytes(int logl, int kind) {
+    return col_tile_words(logl, kind) * 4 + (col_tw_smem(logl, kind) ? col_tw_entries(logl) * 8 : 0);
 }
 
 // A single product (no batch) of transform length 2^logn uses the three-pass
