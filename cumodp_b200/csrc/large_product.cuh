@@ -329,6 +329,7 @@ __global__ void __launch_bounds__(NW * 32, col_ctas(L1, true)) k_col_inv(const _
     constexpr int NTW = col_tw_entries(L1);
     Tw* tws = reinterpret_cast<Tw*>(tile + col_tile_words(L1, true));
     for (int i = threadIdx.x; i < NTW; i += NW * 32) tws[i] = A.twc[A.twc_inv + i];
+    pdl_wait();  // pass B's output
     tile_load<L1, true, NW * 32, true>(tile, J.wa, 1ll << (L1 + A.l2), c0, n2, false, A.pkc);
     __syncthreads();
     col_inv_levels<L1, col_plan(L1).nlev - 1, NW>(tile, A.pkc, tws);
@@ -541,7 +542,9 @@ __global__ void __launch_bounds__(rowsplit_threads(L2), rowsplit_ctas(L2)) k_row
     const u32 k1 = col_slot_to_k1(s, A.colpl, A.l1);
     const u32 p = A.pk.p, p2 = A.pk.p2;
     u32* row = J.wb + (size_t)s * n2;
+    pdl_trigger();
     row_slot_factors<L2>(A, k1, bf, nullptr);
+    pdl_wait();  // pass A's columns of G
     row_load<L2, T>(sm, row);
     __syncthreads();
     row_level0_fwd<L2, T>(sm, A, k1, bf);
@@ -577,12 +580,17 @@ __global__ void __launch_bounds__(rowsplit_threads(L2), rowsplit_ctas(L2)) k_row
     u32* rowF = J.wa + (size_t)s * n2;
     const u32* rowG = J.wb + (size_t)s * n2;
     RowCtx ctx{A.pk, A.twr, A.twr_inv};
+    pdl_trigger();
+    // F's forward row pass depends only on pass A (complete before the
+    // previous kernel, G's row pass, started), so it runs while that kernel
+    // finishes; G's spectrum is read after pdl_wait
     row_slot_factors<L2>(A, k1, bf, bi);
     row_load<L2, T>(sm, rowF);
     __syncthreads();
     row_level0_fwd<L2, T>(sm, A, k1, bf);
     __syncthreads();
     fwd1_levels<L2, 1, T>(sm, A.pk, A.twr);
+    pdl_wait();
     for (int r = threadIdx.x; r < n2 / 32; r += T) {
         u32 x[32];
         load_row32(x, sm, r * 32);

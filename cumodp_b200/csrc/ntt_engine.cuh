@@ -104,6 +104,14 @@ __device__ __forceinline__ void dit_regs(u32 (&x)[R], const Tw* __restrict__ c, 
     }
 }
 
+// Programmatic dependent launch: pdl_trigger lets the next kernel of the
+// stream (launched with programmatic stream serialization) be scheduled as
+// this grid's CTAs retire, to run its independent prologue; pdl_wait blocks
+// until the previous kernel of the stream has completed and its writes are
+// visible.  Without the launch attribute both are no-ops.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 template <int R>
 __device__ __forceinline__ void load_tw(Tw (&t)[R], const Tw* __restrict__ src) {
     const uint4* s4 = reinterpret_cast<const uint4*>(src);

@@ -29,6 +29,24 @@ const SmallFn kSmall[15] = {nullptr, nullptr, nullptr, nullptr, nullptr,
                             launch_small_t<14>};
 
 
+// Launch with programmatic stream serialization: the kernel may start while
+// the previous kernel of the stream finishes (it calls pdl_wait before
+// reading that kernel's results).
+template <class K>
+void launch_pdl(K kernel, dim3 grid, int threads, size_t smem, cudaStream_t st, const LargeArgs& a) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, a);
+}
+
 template <int L1>
 void launch_col_fwd_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
     const size_t smem = col_smem_bytes(L1, false);
@@ -47,7 +65,7 @@ void launch_col_inv_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
         cudaFuncSetAttribute(k_col_inv<L1, col_warps(L1, true)>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    k_col_inv<L1, col_warps(L1, true)><<<grid, col_warps(L1, true) * 32, smem, st>>>(a);
+    launch_pdl(k_col_inv<L1, col_warps(L1, true)>, grid, col_warps(L1, true) * 32, smem, st, a);
 }
 template <int L2>
 void launch_row_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
@@ -62,11 +80,11 @@ void launch_row_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
 
 template <int L2>
 void launch_row_g_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
-    k_row_fwd_g<L2><<<grid, rowsplit_threads(L2), (size_t)(1 << L2) * sizeof(u32), st>>>(a);
+    launch_pdl(k_row_fwd_g<L2>, grid, rowsplit_threads(L2), (size_t)(1 << L2) * sizeof(u32), st, a);
 }
 template <int L2>
 void launch_row_f_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
-    k_row_mul_f<L2><<<grid, rowsplit_threads(L2), (size_t)(1 << L2) * sizeof(u32), st>>>(a);
+    launch_pdl(k_row_mul_f<L2>, grid, rowsplit_threads(L2), (size_t)(1 << L2) * sizeof(u32), st, a);
 }
 
 typedef void (*PassFn)(const LargeArgs&, dim3, cudaStream_t);
