@@ -27,7 +27,8 @@ __host__ __device__ constexpr LevelPlan row_plan(int logl) {
 }
 
 // Plan for a batch of interleaved columns (lane = column): bank conflicts do
-// not depend on the radix, so fewer, wider levels are used.
+// not depend on the radix, so fewer, wider levels are used (two levels up to
+// 2^10 rows: every element goes through shared memory twice).
 __host__ __device__ constexpr LevelPlan col_plan(int logl) {
     switch (logl) {
         case 1: return LevelPlan{1, {1}};
@@ -38,8 +39,8 @@ __host__ __device__ constexpr LevelPlan col_plan(int logl) {
         case 6: return LevelPlan{2, {3, 3}};
         case 7: return LevelPlan{2, {3, 4}};
         case 8: return LevelPlan{2, {4, 4}};
-        case 9: return LevelPlan{3, {3, 3, 3}};
-        case 10: return LevelPlan{3, {3, 3, 4}};
+        case 9: return LevelPlan{2, {4, 5}};
+        case 10: return LevelPlan{2, {5, 5}};
         case 11: return LevelPlan{3, {3, 4, 4}};
         case 12: return LevelPlan{3, {4, 4, 4}};
         default: return LevelPlan{0, {0}};
