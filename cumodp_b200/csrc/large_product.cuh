@@ -67,14 +67,14 @@ struct ColLevel {
 
 // Row slot -> frequency index k1 of the column transform (digit reversal of
 // the column plan).
-__device__ __forceinline__ u32 col_slot_to_k1(u32 s, const LevelPlan& PL, int L1) {
+__host__ __device__ __forceinline__ u32 col_slot_to_k1(u32 s, const LevelPlan& PL, int L1) {
     u32 k = 0, mul = 1;
     int lb = L1;
     for (int i = 0; i < PL.nlev; ++i) {
         const int r = PL.logr[i];
         lb -= r;
         const u32 j = (s >> lb) & ((1u << r) - 1);
-        k += (__brev(j) >> (32 - r)) * mul;
+        k += rev_bits(j, r) * mul;
         mul <<= r;
     }
     return k;
@@ -91,7 +91,7 @@ __device__ __forceinline__ u32 col_slot_to_k1(u32 s, const LevelPlan& PL, int L1
 
 // Word offset of tile row r.
 template <int L1, int INV>
-__device__ __forceinline__ int tile_row(int r) {
+__host__ __device__ __forceinline__ int tile_row(int r) {
     constexpr int TC = col_tile_cols(L1, INV);
     if constexpr (TC == 32) return r * 32;
     else return (r + (r >> col_pad_log(L1))) * TC;
@@ -103,7 +103,7 @@ __device__ __forceinline__ int tile_row(int r) {
 // a multiple of the padding period; the last level has TB = 1 and blocks of
 // exactly one period.
 template <int L1, int INV, int TB>
-__device__ __forceinline__ constexpr int tile_step(int m) {
+__host__ __device__ __forceinline__ constexpr int tile_step(int m) {
     constexpr int TC = col_tile_cols(L1, INV), PAD = 1 << col_pad_log(L1);
     if constexpr (TC == 32) return TB * m * 32;
     else if constexpr (TB % PAD == 0) return TB * m * TC + (TB / PAD) * m * TC;

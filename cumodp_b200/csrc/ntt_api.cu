@@ -39,22 +39,6 @@ __device__ __forceinline__ u32 seed_mont_at(const u32* __restrict__ seeds, int n
     return mul_mont(__ldg(seeds + (e & 4095u)), __ldg(seeds + nlo + (e >> 12)), p, pinv);
 }
 
-// Position in a row after the row plan's DIF levels -> frequency index.
-template <int L2>
-__device__ __forceinline__ u32 row_pos_to_freq(u32 P) {
-    constexpr LevelPlan PL = row_plan(L2);
-    u32 f = 0, mul = 1;
-    int lb = L2;
-#pragma unroll
-    for (int i = 0; i < PL.nlev; ++i) {
-        const int r = PL.logr[i];
-        lb -= r;
-        const u32 j = (P >> lb) & ((1u << r) - 1);
-        f += (__brev(j) >> (32 - r)) * mul;
-        mul <<= r;
-    }
-    return f;
-}
 
 // One row of the natural-order transform per CTA: the row (a column-pass
 // output row, or an independent row) is copied into shared memory with

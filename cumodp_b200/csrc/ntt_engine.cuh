@@ -41,7 +41,7 @@ struct PrimeK {
 // is XOR-ed with (row & 7).  Scalar accesses by 32 lanes to 32 consecutive
 // words and 16-byte accesses by lanes to consecutive 32-word rows (or to
 // consecutive 16/8/4-word groups) are both bank-conflict free.
-__device__ __forceinline__ int swz(int i) { return i ^ (((i >> 5) & 7) << 2); }
+__host__ __device__ __forceinline__ int swz(int i) { return i ^ (((i >> 5) & 7) << 2); }
 
 // swz(base + TB * m) for the m-th element of a level task, where base is a
 // multiple of the block size B plus the task index o < TB, and m is an
@@ -50,10 +50,21 @@ __device__ __forceinline__ int swz(int i) { return i ^ (((i >> 5) & 7) << 2); }
 // immediate offset).  With TB = 32 and B a multiple of 256, base lies in a
 // row that is a multiple of 8, so the XOR is the constant (m & 7) << 2.
 template <int TB, int B>
-__device__ __forceinline__ int swz_task(int base, int bswz, int m) {
+__host__ __device__ __forceinline__ int swz_task(int base, int bswz, int m) {
     if constexpr (TB % 256 == 0) return bswz + TB * m;
     else if constexpr (TB == 32 && B % 256 == 0) return (base ^ ((m & 7) << 2)) + 32 * m;
     else return swz(base + TB * m);
+}
+
+// The low r bits of j in reverse order.
+__host__ __device__ __forceinline__ u32 rev_bits(u32 j, int r) {
+#ifdef __CUDA_ARCH__
+    return __brev(j) >> (32 - r);
+#else
+    u32 v = 0;
+    for (int i = 0; i < r; ++i) v |= ((j >> i) & 1u) << (r - 1 - i);
+    return v;
+#endif
 }
 
 // Forward R-point DIF on registers; x[j] ends holding X[bitrev_r(j)].

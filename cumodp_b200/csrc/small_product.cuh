@@ -63,6 +63,23 @@ struct SmallLevel {
     }();
 };
 
+// Position in a row after the row plan's DIF levels -> frequency index.
+template <int L2>
+__host__ __device__ __forceinline__ u32 row_pos_to_freq(u32 P) {
+    constexpr LevelPlan PL = row_plan(L2);
+    u32 f = 0, mul = 1;
+    int lb = L2;
+#pragma unroll
+    for (int i = 0; i < PL.nlev; ++i) {
+        const int r = PL.logr[i];
+        lb -= r;
+        const u32 j = (P >> lb) & ((1u << r) - 1);
+        f += rev_bits(j, r) * mul;
+        mul <<= r;
+    }
+    return f;
+}
+
 // Forward non-last level on both operands of every product in the CTA.
 template <int LOGL, int LEV, int T, int PPC, class Ctx>
 __device__ __forceinline__ void small_fwd_level(u32* sm, const Ctx& A) {
