@@ -127,6 +127,8 @@ def _lib():
         L.cumodp_twoconv_big_plan.restype = C.c_int
         L.cumodp_twoconv_big_plan.argtypes = [C.c_int, C.c_longlong, C.c_longlong, C.POINTER(C.c_int),
                                               C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.cumodp_inject_alloc_failures.restype = None
+        L.cumodp_inject_alloc_failures.argtypes = [C.c_int]
         L.cumodp_select_device.restype = C.c_int
         L.cumodp_select_device.argtypes = [C.c_int]
         L.cumodp_trace_passes.restype = None
@@ -348,6 +350,11 @@ def subproduct_level_dev(l: int, npairs: int, in_ptr: int, out_ptr: int, p: int,
     """One subproduct-tree level on device arrays (``cumodp_subproduct_level_dev``)."""
     _check(_lib().cumodp_subproduct_level_dev(l, npairs, in_ptr, out_ptr, p, stream or None),
            "cumodp_subproduct_level_dev")
+
+
+def inject_alloc_failures(count: int) -> None:
+    """Host-side fault injection: the next `count` device allocations fail (0 cancels)."""
+    _lib().cumodp_inject_alloc_failures(count)
 
 
 def select_device(dev: int) -> None:

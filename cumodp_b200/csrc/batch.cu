@@ -96,8 +96,8 @@ int tune_row_log(const PrimeCtx& pc, int logn, int njobs, int dev, cudaStream_t 
     int err = OK;
     u32* buf = nullptr;
     LargeJob* djobs = nullptr;
-    if (cudaMalloc(&buf, (size_t)jobs * 4 * n * sizeof(u32)) != cudaSuccess ||
-        cudaMalloc(&djobs, jobs * sizeof(LargeJob)) != cudaSuccess) {
+    if (dev_malloc((void**)&buf, (size_t)jobs * 4 * n * sizeof(u32)) != cudaSuccess ||
+        dev_malloc((void**)&djobs, jobs * sizeof(LargeJob)) != cudaSuccess) {
         cudaGetLastError();
         if (buf) cudaFree(buf);
         return default_row_log(logn);
@@ -232,7 +232,7 @@ int build_plan(BatchPlan& P, const PrimeCtx& pc, cudaStream_t st) {
         P.classes.push_back(c);
     }
     P.jobs_bytes = std::max<size_t>(jb, 256);
-    if (cudaMalloc(&P.djobs, P.jobs_bytes) != cudaSuccess) {
+    if (dev_malloc(&P.djobs, P.jobs_bytes) != cudaSuccess) {
         cudaGetLastError();
         return OUT_OF_MEMORY;
     }
@@ -240,7 +240,7 @@ int build_plan(BatchPlan& P, const PrimeCtx& pc, cudaStream_t st) {
     P.hjobs.assign(P.jobs_bytes, 0);
     P.ws_words = ws;
     if (ws) {
-        if (cudaMalloc(&P.ws, ws * sizeof(u32)) != cudaSuccess) {
+        if (dev_malloc((void**)&P.ws, ws * sizeof(u32)) != cudaSuccess) {
             cudaGetLastError();
             return OUT_OF_MEMORY;
         }

@@ -26,6 +26,9 @@ bool have_device() {
 
 extern "C" {
 
+void cumodp_inject_alloc_failures(int count) { inject_alloc_failures(count); }
+
+
 int is_cuda_enabled(void) { return have_device() ? 1 : 0; }
 
 int num_of_cuda_devices(void) {

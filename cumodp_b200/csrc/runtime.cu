@@ -8,6 +8,7 @@
 // scratch buffers grow once and are reused.
 #include "runtime.cuh"
 
+#include <atomic>
 #include <cstdio>
 #include <map>
 #include <cstring>
@@ -206,6 +207,23 @@ u32 canonical_root(const PrimeCtx& pc, int logn) {
     return powmod_exact(pc.root_max, 1ull << (pc.info.two_adic - logn), pc.info.p);
 }
 
+// Host-side fault injection (cumodp_inject_alloc_failures): the next n
+// device allocations of the library fail as if the device were full.
+static std::atomic<int> g_alloc_failures{0};
+
+void inject_alloc_failures(int n) { g_alloc_failures.store(n < 0 ? 0 : n); }
+
+cudaError_t dev_malloc(void** p, size_t bytes) {
+    int left = g_alloc_failures.load();
+    while (left > 0) {
+        if (g_alloc_failures.compare_exchange_weak(left, left - 1)) {
+            *p = nullptr;
+            return cudaErrorMemoryAllocation;
+        }
+    }
+    return cudaMalloc(p, bytes);
+}
+
 static const Tw* level_tables(int dev, u32 p, u32 root, int logl, int kind, int* err) {
     Caches& C = caches();
     std::lock_guard<std::mutex> g(C.m);
@@ -215,7 +233,7 @@ static const Tw* level_tables(int dev, u32 p, u32 root, int logl, int kind, int*
     const LevelPlan pl = kind == 0 ? row_plan(logl) : col_plan(logl);
     std::vector<Tw> t = build_level_tables(pl, logl, root, p);
     Tw* d = nullptr;
-    if (cudaMalloc(&d, t.size() * sizeof(Tw)) != cudaSuccess) {
+    if (dev_malloc((void**)&d, t.size() * sizeof(Tw)) != cudaSuccess) {
         cudaGetLastError();
         *err = OUT_OF_MEMORY;
         return nullptr;
@@ -261,7 +279,7 @@ const u32* seed_tables(int dev, u32 p, u32 root, int logn, int* err) {
         wi = mulmod_exact(wi, stepi, p);
     }
     u32* d = nullptr;
-    if (cudaMalloc(&d, s.size() * sizeof(u32)) != cudaSuccess) {
+    if (dev_malloc((void**)&d, s.size() * sizeof(u32)) != cudaSuccess) {
         cudaGetLastError();
         *err = OUT_OF_MEMORY;
         return nullptr;
@@ -284,7 +302,7 @@ void* workspace(int dev, int slot, size_t bytes, int* err) {
     e.first = nullptr;
     e.second = 0;
     size_t sz = bytes < 4096 ? 4096 : bytes;
-    if (cudaMalloc(&e.first, sz) != cudaSuccess) {
+    if (dev_malloc(&e.first, sz) != cudaSuccess) {
         cudaGetLastError();
         *err = OUT_OF_MEMORY;
         e.first = nullptr;

@@ -77,6 +77,11 @@ cudaStream_t lib_stream(int dev);
 // Serialises host entry points that share workspace and caches.
 std::mutex& lib_mutex();
 
+// Every device allocation of the library goes through dev_malloc, which
+// honours the host-side fault injection of inject_alloc_failures.
+cudaError_t dev_malloc(void** p, size_t bytes);
+void inject_alloc_failures(int n);
+
 // Side streams of the library (per device) for independent pieces of one
 // call: aux_fork makes streams 0..n-1 wait for `st`'s work so far,
 // aux_stream(dev, i) is stream i, aux_join makes `st` wait for all of them.

@@ -155,7 +155,7 @@ struct DevBuf {
         p = nullptr;
         const size_t cap = grow_to(n, want);
         n = 0;
-        if (cudaMalloc(&p, cap * sizeof(T)) != cudaSuccess) {
+        if (dev_malloc((void**)&p, cap * sizeof(T)) != cudaSuccess) {
             cudaGetLastError();
             return OUT_OF_MEMORY;
         }

@@ -336,6 +336,13 @@ int cumodp_twoconv_big_out_words(long long na, long long nb, int bit_width);
 cumodp_err cumodp_twoconv_big_plan(int bit_width, long long na, long long nb, int *K, int *M, int *nprimes,
                                    int *log_transform);
 
+/* Addition (testing).  Host-side fault injection: the next `count` device
+ * allocations the library makes fail as if the device were out of memory
+ * (the calls that needed them return CUMODP_OUT_OF_MEMORY; nothing is left
+ * half-built, so the same call succeeds once the injection is used up).
+ * 0 cancels.  Nothing touches the GPU. */
+void cumodp_inject_alloc_failures(int count);
+
 /* Addition.  Makes `dev` the current device of the calling thread for the
  * library's own CUDA runtime (one process per GPU). */
 cumodp_err cumodp_select_device(int dev);
