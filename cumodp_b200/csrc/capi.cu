@@ -88,6 +88,7 @@ cumodp_err cumodp_fftmul_uni_dev(sfixn lh, sfixn* H, sfixn df, const sfixn* F, s
 cumodp_err cumodp_fftmul_uni(sfixn dh, sfixn* H, sfixn df, const sfixn* F, sfixn dg, const sfixn* G, sfixn p) {
     if (!have_device()) return CUMODP_NO_CUDA_DEVICE;
     if (df < 0 || dg < 0 || dh < 0 || !F || !G || !H) return CUMODP_ASSUMPTION_ERROR;
+    NvtxRange range("cumodp_fftmul_uni");
     std::lock_guard<std::mutex> g(lib_mutex());
     const int dev = current_device();
     cudaStream_t st = lib_stream(dev);

@@ -232,6 +232,7 @@ static const char* kRowName[15] = {"", "", "", "", "", "", "row_fused_6", "row_f
 
 void launch_small(int logn, const SmallArgs& a, int njobs, cudaStream_t st) {
     const int ppc = small_ppc(logn);
+    NvtxRange range(kSmallName[logn]);
     cudaEvent_t e0;
     const bool tr = pass_timing_begin(st, &e0);
     kSmall[logn](a, (njobs + ppc - 1) / ppc, st);
@@ -240,6 +241,7 @@ void launch_small(int logn, const SmallArgs& a, int njobs, cudaStream_t st) {
 
 void launch_large(const LargeArgs& a, int njobs, cudaStream_t st) {
     const int n1 = 1 << a.l1, n2 = 1 << a.l2;
+    NvtxRange range(kRowFName[a.l2]);  // the product's three passes, named by its dominant kernel
     cudaEvent_t e0;
     bool tr = pass_timing_begin(st, &e0);
     kColFwd[a.l1](a, dim3(n2 / col_tile_cols_rt(a.l1, false), 2, njobs), st);

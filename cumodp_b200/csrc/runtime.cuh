@@ -1,6 +1,7 @@
 // Host runtime shared by every entry point: prime set-up, resident twiddle
 // tables, per-device workspace and the error convention.
 #pragma once
+#include <nvtx3/nvToolsExt.h>
 #include <cuda_runtime.h>
 #include <cstddef>
 #include <cstdint>
@@ -76,6 +77,15 @@ cudaStream_t lib_stream(int dev);
 
 // Serialises host entry points that share workspace and caches.
 std::mutex& lib_mutex();
+
+// NVTX range (host timeline) around a library operation: visible in Nsight
+// Systems / ncu range filters, a few nanoseconds when no tool is attached.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Every device allocation of the library goes through dev_malloc, which
 // honours the host-side fault injection of inject_alloc_failures.
