@@ -62,11 +62,13 @@ __host__ __device__ constexpr int col_tw_entries(int logl) {
 // one column on each lane; 16-column tiles put two tasks on each warp (one
 // per half-warp) and insert a 16-word pad after every 2^col_pad_log rows (the
 // plan's last radix), so that the two half-warps always read opposite halves
-// of the banks.  Kinds 1 and 2 over 2^10-row tiles use 16 columns and two
+// of the banks.  Short tiles (2^5, 2^6 rows: the column side of products of
+// 2^15-2^17) run on one or two warps, so many CTAs share an SM.  Kinds 1 and
+// 2 over 2^10-row tiles use 16 columns and two
 // CTAs per SM (their load, compute and store phases overlap); kind 0 keeps
 // 32 columns (its loads skip the zero-padded half).
 __host__ __device__ constexpr int col_tile_cols(int logl, int kind) { return kind != 0 && logl == 10 ? 16 : 32; }
-__host__ __device__ constexpr int col_warps(int logl, int kind) { return logl == 10 && kind == 0 ? 32 : 16; }
+__host__ __device__ constexpr int col_warps(int logl, int kind) { return logl == 10 && kind == 0 ? 32 : (logl <= 5 ? 1 : (logl <= 6 ? 2 : 16)); }
 __host__ __device__ constexpr int col_ctas(int logl, int kind) { return kind != 0 && logl == 10 ? 2 : 1; }
 __host__ __device__ constexpr int col_pad_log(int logl) { return col_plan(logl).logr[col_plan(logl).nlev - 1]; }
 __host__ __device__ constexpr int col_tile_words(int logl, int kind) {
