@@ -201,10 +201,10 @@ void launch_colfwd1_t(const LargeArgs& a, int tiles, cudaStream_t st) {
     k_col_fwd<L1, col_warps(L1, 2), 2><<<dim3(tiles, 1, 1), col_warps(L1, 2) * 32, smem, st>>>(a);
 }
 typedef void (*ColFn)(const LargeArgs&, int, cudaStream_t);
-const ColFn kColFwd1[11] = {nullptr, launch_colfwd1_t<1>, launch_colfwd1_t<2>, launch_colfwd1_t<3>,
+const ColFn kColFwd1[12] = {nullptr, launch_colfwd1_t<1>, launch_colfwd1_t<2>, launch_colfwd1_t<3>,
                             launch_colfwd1_t<4>, launch_colfwd1_t<5>, launch_colfwd1_t<6>,
                             launch_colfwd1_t<7>, launch_colfwd1_t<8>, launch_colfwd1_t<9>,
-                            launch_colfwd1_t<10>};
+                            launch_colfwd1_t<10>, launch_colfwd1_t<11>};
 
 // w is a primitive 2^k-th root of unity mod p.
 bool root_has_order(u32 w, int k, u32 p) {

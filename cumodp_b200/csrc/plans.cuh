@@ -67,7 +67,7 @@ __host__ __device__ constexpr int col_tw_entries(int logl) {
 // 2 over 2^10-row tiles use 16 columns and two
 // CTAs per SM (their load, compute and store phases overlap); kind 0 keeps
 // 32 columns (its loads skip the zero-padded half).
-__host__ __device__ constexpr int col_tile_cols(int logl, int kind) { return kind != 0 && logl == 10 ? 16 : 32; }
+__host__ __device__ constexpr int col_tile_cols(int logl, int kind) { return (kind != 0 && logl == 10) || logl >= 11 ? 16 : 32; }
 __host__ __device__ constexpr int col_warps(int logl, int kind) { return logl == 10 && kind == 0 ? 32 : (logl <= 5 ? 1 : (logl <= 6 ? 2 : 16)); }
 __host__ __device__ constexpr int col_ctas(int logl, int kind) { return kind != 0 && logl == 10 ? 2 : 1; }
 __host__ __device__ constexpr int col_pad_log(int logl) { return col_plan(logl).logr[col_plan(logl).nlev - 1]; }

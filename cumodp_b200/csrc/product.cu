@@ -88,14 +88,14 @@ void launch_row_f_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
 }
 
 typedef void (*PassFn)(const LargeArgs&, dim3, cudaStream_t);
-const PassFn kColFwd[11] = {nullptr, launch_col_fwd_t<1>, launch_col_fwd_t<2>, launch_col_fwd_t<3>,
+const PassFn kColFwd[12] = {nullptr, launch_col_fwd_t<1>, launch_col_fwd_t<2>, launch_col_fwd_t<3>,
                             launch_col_fwd_t<4>, launch_col_fwd_t<5>, launch_col_fwd_t<6>,
                             launch_col_fwd_t<7>, launch_col_fwd_t<8>, launch_col_fwd_t<9>,
-                            launch_col_fwd_t<10>};
-const PassFn kColInv[11] = {nullptr, launch_col_inv_t<1>, launch_col_inv_t<2>, launch_col_inv_t<3>,
+                            launch_col_fwd_t<10>, launch_col_fwd_t<11>};
+const PassFn kColInv[12] = {nullptr, launch_col_inv_t<1>, launch_col_inv_t<2>, launch_col_inv_t<3>,
                             launch_col_inv_t<4>, launch_col_inv_t<5>, launch_col_inv_t<6>,
                             launch_col_inv_t<7>, launch_col_inv_t<8>, launch_col_inv_t<9>,
-                            launch_col_inv_t<10>};
+                            launch_col_inv_t<10>, launch_col_inv_t<11>};
 const PassFn kRow[15] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
                          launch_row_t<6>, launch_row_t<7>, launch_row_t<8>, launch_row_t<9>,
                          launch_row_t<10>, launch_row_t<11>, launch_row_t<12>, launch_row_t<13>,
@@ -149,7 +149,7 @@ void ensure_kernel_attrs() {
         attr_small<5>(); attr_small<6>(); attr_small<7>(); attr_small<8>(); attr_small<9>();
         attr_small<10>(); attr_small<11>(); attr_small<12>(); attr_small<13>(); attr_small<14>();
         attr_col<1>(); attr_col<2>(); attr_col<3>(); attr_col<4>(); attr_col<5>();
-        attr_col<6>(); attr_col<7>(); attr_col<8>(); attr_col<9>(); attr_col<10>();
+        attr_col<6>(); attr_col<7>(); attr_col<8>(); attr_col<9>(); attr_col<10>(); attr_col<11>();
         attr_row<6>(); attr_row<7>(); attr_row<8>(); attr_row<9>(); attr_row<10>();
         attr_row<11>(); attr_row<12>(); attr_row<13>(); attr_row<14>();
         attr_rowsplit<6>(); attr_rowsplit<7>(); attr_rowsplit<8>(); attr_rowsplit<9>(); attr_rowsplit<10>();
@@ -165,7 +165,7 @@ int default_row_log(int logn) {
     // rows of 2^l2 words, columns of 2^(logn-l2): columns as long as the
     // 32-column tile fits shared memory (n1 <= 2^10), rows as long as one
     // CTA can hold both operands (n2 <= 2^14)
-    int l2 = std::max(logn - kMaxColLog, 7);
+    int l2 = std::max(logn - kDefaultColLog, 7);
     return std::min(l2, kMaxRowLog);
 }
 
@@ -219,10 +219,10 @@ int large_args(const PrimeCtx& pc, u32 root_n, int logn, int l2, int dev, LargeA
 static const char* kSmallName[15] = {"", "", "", "", "", "small_product_5", "small_product_6",
     "small_product_7", "small_product_8", "small_product_9", "small_product_10", "small_product_11",
     "small_product_12", "small_product_13", "small_product_14"};
-static const char* kColFwdName[11] = {"", "col_fwd_1", "col_fwd_2", "col_fwd_3", "col_fwd_4", "col_fwd_5",
-    "col_fwd_6", "col_fwd_7", "col_fwd_8", "col_fwd_9", "col_fwd_10"};
-static const char* kColInvName[11] = {"", "col_inv_1", "col_inv_2", "col_inv_3", "col_inv_4", "col_inv_5",
-    "col_inv_6", "col_inv_7", "col_inv_8", "col_inv_9", "col_inv_10"};
+static const char* kColFwdName[12] = {"", "col_fwd_1", "col_fwd_2", "col_fwd_3", "col_fwd_4", "col_fwd_5",
+    "col_fwd_6", "col_fwd_7", "col_fwd_8", "col_fwd_9", "col_fwd_10", "col_fwd_11"};
+static const char* kColInvName[12] = {"", "col_inv_1", "col_inv_2", "col_inv_3", "col_inv_4", "col_inv_5",
+    "col_inv_6", "col_inv_7", "col_inv_8", "col_inv_9", "col_inv_10", "col_inv_11"};
 static const char* kRowGName[15] = {"", "", "", "", "", "", "row_fwd_g_6", "row_fwd_g_7", "row_fwd_g_8",
     "row_fwd_g_9", "row_fwd_g_10", "row_fwd_g_11", "row_fwd_g_12", "row_fwd_g_13", "row_fwd_g_14"};
 static const char* kRowFName[15] = {"", "", "", "", "", "", "row_mul_f_6", "row_mul_f_7", "row_mul_f_8",

@@ -7,10 +7,11 @@ namespace cmb {
 
 constexpr int kMinLog = 5;        // smallest transform: one radix-32 row
 constexpr int kMaxSmallLog = 14;  // largest single-CTA product (2 x 64 KiB of shared memory)
-constexpr int kMaxColLog = 10;    // 32-column tile of 2^10 rows = 128 KiB of shared memory
+constexpr int kMaxColLog = 11;    // 16-column tile of 2^11 rows = 136 KiB of shared memory
 constexpr int kMaxRowLog = 14;
 constexpr int kMinRowLog = 6;
-constexpr int kMaxLog = kMaxColLog + kMaxRowLog;  // 2^24
+constexpr int kMaxLog = 24;        // largest product transform (2^24)
+constexpr int kDefaultColLog = 10;  // column length of the default split (rows of 2^14)
 
 // workspace slots (runtime.cuh: workspace)
 enum WsSlot { kWsSingle = 0, kWsBatch = 1, kWsStage = 2, kWsNtt = 3, kWsTwoConv = 4, kWsServer = 5,

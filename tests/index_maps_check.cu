@@ -8,7 +8,7 @@
 //            each word of its buffer exactly once, swz_task equals the plain
 //            swizzle, the last level's 16-byte quads tile the buffer, and the
 //            twiddle reads stay inside the plan's table;
-//   columns: for every tile kind and 2^1..2^10 rows, tile_row is injective and
+//   columns: for every tile kind and 2^1..2^11 rows, tile_row is injective and
 //            in bounds, tile_step equals tile_row differences for every level
 //            task, and the two half-warps of a 16-column tile read opposite
 //            halves of the banks;
@@ -178,6 +178,7 @@ int main() {
     col_plan_check<8>();
     col_plan_check<9>();
     col_plan_check<10>();
+    col_plan_check<11>();
     std::printf("%s: %d failures\n", failures ? "FAILED" : "OK", failures);
     return failures ? 1 : 0;
 }
