@@ -162,9 +162,12 @@ int product_logn(long long la, long long lb) {
 }
 
 int default_row_log(int logn) {
-    // rows of 2^l2 words, columns of 2^(logn-l2): columns as long as the
-    // 32-column tile fits shared memory (n1 <= 2^10), rows as long as one
-    // CTA can hold both operands (n2 <= 2^14)
+    // rows of 2^l2 words, columns of 2^(logn-l2): the split with the shortest
+    // single-product time measured on B200 for each length 2^15..2^24 (a
+    // batch's own splits come from the autotuner)
+    static const int kBest[25] = {7, 7, 7, 7, 7, 7, 7, 7, 7, 7, 7, 7, 7, 7, 7,
+                                  7, 11, 12, 13, 14, 10, 11, 12, 14, 14};
+    if (logn >= 0 && logn <= 24) return kBest[logn];
     int l2 = std::max(logn - kDefaultColLog, 7);
     return std::min(l2, kMaxRowLog);
 }
