@@ -19,8 +19,8 @@ __host__ __device__ constexpr LevelPlan row_plan(int logl) {
         case 9: return LevelPlan{2, {4, 5}};
         case 10: return LevelPlan{3, {2, 3, 5}};
         case 11: return LevelPlan{3, {3, 3, 5}};
-        case 12: return LevelPlan{3, {3, 4, 5}};
-        case 13: return LevelPlan{3, {4, 4, 5}};
+        case 12: return LevelPlan{4, {2, 2, 3, 5}};
+        case 13: return LevelPlan{4, {2, 3, 3, 5}};
         case 14: return LevelPlan{4, {3, 3, 3, 5}};
         default: return LevelPlan{0, {0}};
     }
