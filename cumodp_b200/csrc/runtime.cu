@@ -224,6 +224,17 @@ cudaError_t dev_malloc(void** p, size_t bytes) {
     return cudaMalloc(p, bytes);
 }
 
+cudaError_t dev_malloc_async(void** p, size_t bytes, cudaStream_t st) {
+    int left = g_alloc_failures.load();
+    while (left > 0) {
+        if (g_alloc_failures.compare_exchange_weak(left, left - 1)) {
+            *p = nullptr;
+            return cudaErrorMemoryAllocation;
+        }
+    }
+    return cudaMallocAsync(p, bytes, st);
+}
+
 static const Tw* level_tables(int dev, u32 p, u32 root, int logl, int kind, int* err) {
     Caches& C = caches();
     std::lock_guard<std::mutex> g(C.m);

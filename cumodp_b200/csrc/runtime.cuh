@@ -90,6 +90,8 @@ struct NvtxRange {
 // Every device allocation of the library goes through dev_malloc, which
 // honours the host-side fault injection of inject_alloc_failures.
 cudaError_t dev_malloc(void** p, size_t bytes);
+// Stream-ordered allocation (cudaMallocAsync) with the same fault injection.
+cudaError_t dev_malloc_async(void** p, size_t bytes, cudaStream_t st);
 void inject_alloc_failures(int n);
 
 // Side streams of the library (per device) for independent pieces of one

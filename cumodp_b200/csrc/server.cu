@@ -24,6 +24,8 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <thread>
@@ -146,24 +148,27 @@ struct Req {
 size_t grow_to(size_t have, size_t want) { return std::max<size_t>({want, have + have / 2, 1024}); }
 
 template <class T>
+// A lane's device buffer, allocated and freed in the order of the lane's
+// stream (cudaMallocAsync / cudaFreeAsync): growing it neither waits for the
+// device nor stalls the other lanes.
 struct DevBuf {
     T* p = nullptr;
     size_t n = 0;
-    int ensure(size_t want) {
+    int ensure(size_t want, cudaStream_t st) {
         if (want <= n) return OK;
-        if (p) cudaFree(p);  // synchronises the device: grow rarely
+        if (p) cudaFreeAsync(p, st);  // after the stream's earlier work, which used it
         p = nullptr;
         const size_t cap = grow_to(n, want);
         n = 0;
-        if (dev_malloc((void**)&p, cap * sizeof(T)) != cudaSuccess) {
+        if (dev_malloc_async((void**)&p, cap * sizeof(T), st) != cudaSuccess) {
             cudaGetLastError();
             return OUT_OF_MEMORY;
         }
         n = cap;
         return OK;
     }
-    void release() {
-        if (p) cudaFree(p);
+    void release(cudaStream_t st) {
+        if (p) cudaFreeAsync(p, st);
         p = nullptr;
         n = 0;
     }
@@ -203,6 +208,8 @@ struct Lane {
     int status = OK;
     bool busy = false;
     long long seq = 0;
+    double t_start = 0, t_launched = 0;  // batch timing for the trace log
+    double t_alloc = 0, t_copies = 0;    // after the buffer checks, after the operand copies
 };
 
 }  // namespace
@@ -221,6 +228,7 @@ struct Server {
     long long next_id = 1, lane_seq = 0;
     bool stop = false;
     std::thread batcher, completer;
+    FILE* trace = nullptr;  // CUMODP_SERVER_TRACE: per-batch timing log
     // statistics
     std::vector<double> lat;
     long long completed = 0, failed = 0, batches = 0;
@@ -277,10 +285,12 @@ int run_batch(Server& S, Lane& L) {
             nin += la[i] + lb[i];
             nout += lh[i];
         }
-        if ((err = L.din.ensure(nin)) || (err = L.dout.ensure(nout))) return err;
+        if ((err = L.din.ensure(nin, L.st)) || (err = L.dout.ensure(nout, L.st))) return err;
         const size_t wsw = direct_ws_words(cnt, la.data(), lb.data());
         const size_t jb = direct_job_bytes(cnt);
-        if ((err = L.ws.ensure(wsw + 1)) || (err = L.djobs.ensure(jb)) || (err = L.hjobs.ensure(jb))) return err;
+        if ((err = L.ws.ensure(wsw + 1, L.st)) || (err = L.djobs.ensure(jb, L.st)) || (err = L.hjobs.ensure(jb)))
+            return err;
+        L.t_alloc = now_us();
         std::vector<const u32*> pa(cnt), pb(cnt);
         std::vector<u32*> ph(cnt);
         size_t o = 0, q = 0;
@@ -294,6 +304,7 @@ int run_batch(Server& S, Lane& L) {
             ph[i] = L.dout.p + q;
             q += lh[i];
         }
+        L.t_copies = now_us();
         // no autotuning on the serving path: cached or default splits only
         err = direct_batch(cnt, pa.data(), la.data(), pb.data(), lb.data(), ph.data(), lh.data(), p, L.ws.p,
                            L.djobs.p, L.hjobs.p, L.st, false);
@@ -315,8 +326,8 @@ int run_batch(Server& S, Lane& L) {
             jbb += j;
         }
         // int64 data travels through the u32 buffers (two words per value)
-        if ((err = L.din.ensure(2 * nin)) || (err = L.dout.ensure(2 * nout + evw)) || (err = L.ws.ensure(wsw + 1)) ||
-            (err = L.djobs.ensure(jbb)) || (err = L.hjobs.ensure(jbb)))
+        if ((err = L.din.ensure(2 * nin, L.st)) || (err = L.dout.ensure(2 * nout + evw, L.st)) ||
+            (err = L.ws.ensure(wsw + 1, L.st)) || (err = L.djobs.ensure(jbb, L.st)) || (err = L.hjobs.ensure(jbb)))
             return err;
         size_t o = 0, q = 0, jo = 0;
         u32* eval = L.dout.p + 2 * nout;
@@ -398,7 +409,10 @@ void batcher_loop(Server* Sp) {
         L.seq = ++S.lane_seq;
         S.batches++;
         lk.unlock();
+        L.t_start = now_us();
+        L.t_alloc = L.t_copies = 0;
         L.status = run_batch(S, L);
+        L.t_launched = now_us();
         if (L.status != OK) cudaEventRecord(L.ev, L.st);  // completer still waits on the lane
         lk.lock();
         S.dispatched.push_back(li);
@@ -426,6 +440,16 @@ void completer_loop(Server* Sp) {
             cudaStreamSynchronize(L.st);
             cudaGetLastError();
             recreate_lane(L);
+        }
+        if (S.trace) {
+            // one line per batch: start, host launch time, completion seen,
+            // kind, prime, requests, operand words, status
+            long long words = 0;
+            for (Req* r : L.reqs) words += r->la + r->lb;
+            std::fprintf(S.trace, "%.1f %.1f %.1f %d %u %zu %lld %d %.1f %.1f\n", L.t_start, L.t_launched - L.t_start,
+                         now_us() - L.t_start, L.reqs.empty() ? -1 : L.reqs[0]->kind,
+                         L.reqs.empty() ? 0u : L.reqs[0]->p, L.reqs.size(), words, st,
+                         L.t_alloc ? L.t_alloc - L.t_start : -1.0, L.t_copies ? L.t_copies - L.t_start : -1.0);
         }
         lk.lock();
         size_t freed = 0;
@@ -636,10 +660,30 @@ cumodp_server* cumodp_server_create(const cumodp_server_config* cfg) {
     Server* S = new Server(c);
     S->lanes.resize(c.lanes);
     for (Lane& L : S->lanes) recreate_lane(L);
+    // lane buffers come from the device's default memory pool (stream-ordered
+    // allocation); keep what they free cached in this process instead of
+    // returning it at every synchronisation
+    cudaMemPool_t mp;
+    if (cudaDeviceGetDefaultMemPool(&mp, c.device) == cudaSuccess) {
+        uint64_t keep = ~0ull;
+        cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &keep);
+        // back the pool with physical memory now (growing it later maps new
+        // memory inside a batch's launch, which took up to a second)
+        const size_t reserve = std::min<size_t>(c.memory_budget, 8ull << 30);
+        void* tmp = nullptr;
+        cudaStream_t s0 = S->lanes[0].st;
+        if (cudaMallocAsync(&tmp, reserve, s0) == cudaSuccess) cudaFreeAsync(tmp, s0);
+        cudaStreamSynchronize(s0);
+    }
+    cudaGetLastError();
+    // job tables for a full batch, so that pinned memory is not reallocated
+    // (cudaFreeHost waits for the device) while serving
+    for (Lane& L : S->lanes) L.hjobs.ensure(direct_job_bytes(c.max_batch));
     // pinned slabs: the whole host budget is pinned now, so that serving never
     // calls cudaHostAlloc (slow, and it stalls other CUDA calls)
     S->pool.set_limit(c.host_budget ? c.host_budget : (2ull << 30));
     S->pool.reserve(S->pool.limit);
+    if (const char* tf = getenv("CUMODP_SERVER_TRACE")) S->trace = fopen(tf, "a");
     S->batcher = std::thread(batcher_loop, S);
     S->completer = std::thread(completer_loop, S);
     return (cumodp_server*)S;
@@ -798,11 +842,12 @@ void cumodp_server_destroy(cumodp_server* h) {
     cudaSetDevice(S->dev);
     for (Lane& L : S->lanes) {
         if (L.st) cudaStreamSynchronize(L.st);
-        L.din.release(); L.dout.release(); L.ws.release(); L.djobs.release();
+        L.din.release(L.st); L.dout.release(L.st); L.ws.release(L.st); L.djobs.release(L.st);
         L.hjobs.release();
         if (L.st) cudaStreamDestroy(L.st);
         if (L.ev) cudaEventDestroy(L.ev);
     }
+    if (S->trace) fclose(S->trace);
     for (auto& kv : S->reqs) {
         S->pool.put(kv.second->in, kv.second->in_bytes);
         S->pool.put(kv.second->res, kv.second->res_bytes);
