@@ -93,7 +93,6 @@ int tune_row_log(const PrimeCtx& pc, int logn, int njobs, int dev, cudaStream_t 
     // synthetic class: `jobs` products of two length-n/2 operands
     const int jobs = std::min(key.bucket, 32);
     const long long n = 1ll << logn;
-    int err = OK;
     u32* buf = nullptr;
     LargeJob* djobs = nullptr;
     if (dev_malloc((void**)&buf, (size_t)jobs * 4 * n * sizeof(u32)) != cudaSuccess ||
@@ -137,7 +136,6 @@ int tune_row_log(const PrimeCtx& pc, int logn, int njobs, int dev, cudaStream_t 
     cudaEventDestroy(e1);
     cudaFree(buf);
     cudaFree(djobs);
-    (void)err;
     std::lock_guard<std::mutex> g(g_tune_m);
     g_tune[key] = best;
     if (const char* f = getenv("CUMODP_TUNE_FILE")) {

@@ -42,6 +42,8 @@ struct LargeArgs {
     int njobs;
     LevelPlan colpl;             // column plan (row slot -> k1 map)
     int row_fused;               // 1: one fused row kernel; 0: the split pair
+    double r32p;                 // 2^32 / p (estimate for Shoup quotients on the device)
+    const Tw* __restrict__ rowtab;  // per-slot level-0 factor tables (RowTab), or nullptr
     LargeJob job0;
 };
 
@@ -319,6 +321,136 @@ __global__ void __launch_bounds__(NW * 32, col_ctas(L1, KIND)) k_col_fwd(const _
     tile_store<L1, KIND, NW * 32>(tile, dst, 1ll << (L1 + A.l2), c0, n2, false, A.pkc);
 }
 
+// Pass A as a persistent, software-pipelined kernel for the two-level
+// column plans with 32-column tiles (n1 = 2^9, 2^10).  Each CTA walks the
+// tiles gridDim.x apart; while it transforms one tile, rows [0, n1/2) of its
+// next tile are already on their way into a staging buffer (cp.async,
+// zero-filled past the operand's end), so the SM does not wait for HBM
+// between tiles.  A product's operands are usually at most n/2 words long:
+// their rows [n1/2, n1) are zero and the first level skips that half.
+// Level 0 reads the stage and writes the tile; the last level reads the tile
+// and stores its outputs straight to HBM (each warp store is one 128-byte
+// row segment).  A longer operand also has rows [n1/2, n1) copied into the
+// tile before level 0, which then reads them there.  Sources that are not
+// 16-byte aligned are copied word by word.  Results are those of k_col_fwd
+// (same levels, same output layout).
+template <int L1, int NW>
+__global__ void __launch_bounds__(NW * 32, col_pipe_ctas(L1)) k_col_fwd_pipe(const __grid_constant__ LargeArgs A) {
+    constexpr LevelPlan PL = col_plan(L1);
+    static_assert(PL.nlev == 2, "two-level column plans only");
+    constexpr int n1 = 1 << L1, HALF = n1 / 2, T = NW * 32;
+    constexpr int R0 = 1 << PL.logr[0], R1 = 1 << PL.logr[1];  // n1 = R0 * R1; level-0 tasks: R1
+    extern __shared__ __align__(16) u32 smem[];
+    u32* tile = smem;                                     // n1 rows x 32 words
+    u32* stage = smem + n1 * 32;                          // rows [0, HALF) x 32 words
+    Tw* tws = reinterpret_cast<Tw*>(stage + HALF * 32);   // level-0 twiddles (n1 entries)
+    const int n2 = 1 << A.l2, ct = n2 / 32;
+    const int ntiles = ct * 2 * A.njobs;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const u32 p = A.pkc.p, p2 = A.pkc.p2, oneq = A.pkc.one_q;
+    for (int i = threadIdx.x; i < n1; i += T) tws[i] = A.twc[i];
+
+    // tile t -> job, operand, first column
+    auto decode = [&](int t, const u32*& src, long long& len, u32*& dst, int& c0) {
+        const LargeJob& J = A.jobs ? A.jobs[t / (2 * ct)] : A.job0;
+        const int op = (t / ct) & 1;
+        src = op ? J.b : J.a;
+        len = op ? J.lb : J.la;
+        dst = op ? J.wb : J.wa;
+        c0 = (t % ct) * 32;
+    };
+    // rows [r0, r1) x 32 columns of the operand into buf + r * 32 (one
+    // commit group); words at or past len read as 0
+    auto rows_issue = [&](u32* buf, const u32* src, long long len, int c0, int r0, int r1) {
+        if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+#pragma unroll 4
+            for (int idx = r0 * 8 + threadIdx.x; idx < r1 * 8; idx += T) {
+                const int r = idx >> 3, q = idx & 7;
+                const long long gi = (long long)r * n2 + c0 + 4 * q;
+                const long long rem = len - gi;
+                const int bytes = rem >= 4 ? 16 : (rem > 0 ? (int)rem * 4 : 0);
+                const u32* g = bytes ? src + gi : src;
+                const unsigned d = (unsigned)__cvta_generic_to_shared(buf + r * 32 + 4 * q);
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(g), "r"(bytes) : "memory");
+            }
+        } else {
+            for (int idx = r0 * 32 + threadIdx.x; idx < r1 * 32; idx += T) {
+                const int r = idx >> 5, c = idx & 31;
+                const long long gi = (long long)r * n2 + c0 + c;
+                const int bytes = gi < len ? 4 : 0;
+                const u32* g = bytes ? src + gi : src;
+                const unsigned d = (unsigned)__cvta_generic_to_shared(buf + r * 32 + c);
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(g), "r"(bytes) : "memory");
+            }
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+
+    int t = blockIdx.x;
+    if (t < ntiles) {
+        const u32* src; long long len; u32* dst; int c0;
+        decode(t, src, len, dst, c0);
+        rows_issue(stage, src, len, c0, 0, HALF);
+    }
+    for (; t < ntiles; t += gridDim.x) {
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        __syncthreads();  // stage and twiddles visible; the previous tile's last level is done with `tile`
+        bool full;
+        {
+            const u32* src; long long len; u32* dst; int c0;
+            decode(t, src, len, dst, c0);
+            full = len > (long long)HALF * n2;
+            if (full) {  // the upper rows of a long operand, into the tile
+                rows_issue(tile, src, len, c0, HALF, n1);
+                asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+                __syncthreads();
+            }
+        }
+
+        // level 0: task o (rows o + R1 m), lane = column
+        for (int o = warp; o < R1; o += NW) {
+            u32 x[R0];
+#pragma unroll
+            for (int m = 0; m < R0 / 2; ++m) x[m] = stage[(o + R1 * m) * 32 + lane];
+            if (!full) {
+                dif_regs_halfzero<R0, true>(x, A.pkc.rc.f, p, p2, oneq);
+            } else {
+#pragma unroll
+                for (int m = 0; m < R0; ++m)
+                    x[m] = mul_shoup(m < R0 / 2 ? x[m] : tile[(o + R1 * m) * 32 + lane], 1u, oneq, p);
+                dif_regs<R0, true>(x, A.pkc.rc.f, p, p2);
+            }
+#pragma unroll
+            for (int j = 1; j < R0; ++j) {
+                const Tw w = tws[o * R0 + j];  // broadcast
+                x[j] = mul_shoup(x[j], w.w, w.wq, p);
+            }
+#pragma unroll
+            for (int m = 0; m < R0; ++m) tile[(o + R1 * m) * 32 + lane] = x[m];
+        }
+        __syncthreads();  // tile complete; the stage is free
+
+        if (t + (int)gridDim.x < ntiles) {
+            const u32* src; long long len; u32* dst; int c0;
+            decode(t + gridDim.x, src, len, dst, c0);
+            rows_issue(stage, src, len, c0, 0, HALF);
+        }
+
+        // level 1 (last): block blk = rows blk * R1 + m, straight to HBM
+        const u32* src; long long len; u32* dst; int c0;
+        decode(t, src, len, dst, c0);
+        for (int blk = warp; blk < R0; blk += NW) {
+            u32 x[R1];
+#pragma unroll
+            for (int m = 0; m < R1; ++m) x[m] = tile[(blk * R1 + m) * 32 + lane];
+            dif_regs<R1>(x, A.pkc.rc.f, p, p2);
+            u32* out = dst + (size_t)(blk * R1) * n2 + c0 + lane;
+#pragma unroll
+            for (int m = 0; m < R1; ++m) out[(size_t)m * n2] = x[m];
+        }
+    }
+}
+
 // pass C, grid: (n2/TC column tiles, 1, jobs)
 template <int L1, int NW>
 __global__ void __launch_bounds__(NW * 32, col_ctas(L1, true)) k_col_inv(const __grid_constant__ LargeArgs A) {
@@ -495,19 +627,154 @@ __device__ __forceinline__ void row_slot_factors(const LargeArgs& A, u32 k1, Tw*
 // a thread's copies in flight at once); the caller's __syncthreads follows
 // the wait.
 template <int L2, int T>
-__device__ __forceinline__ void row_load(u32* sm, const u32* __restrict__ row) {
+__device__ __forceinline__ void row_load_issue(u32* sm, const u32* __restrict__ row) {
     constexpr int n2 = 1 << L2;
 #pragma unroll 8
     for (int i = threadIdx.x * 4; i < n2; i += T * 4) {
         const unsigned dst = (unsigned)__cvta_generic_to_shared(sm + swz(i));
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(row + i) : "memory");
     }
-    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void row_load_wait() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+template <int L2, int T>
+__device__ __forceinline__ void row_load(u32* sm, const u32* __restrict__ row) {
+    row_load_issue<L2, T>(sm, row);
+    row_load_wait();
 }
 
-// Level 0 forward of one operand with the inter-pass twiddle w_n^(k1 c).
+// floor(w * 2^32 / p) for w < p < 2^30 (the Shoup quotient of w): a
+// double-precision estimate, off by at most one, corrected with exact
+// 64-bit integer arithmetic.
+__host__ __device__ __forceinline__ u32 shoup_quot_dev(u32 w, u32 p, double r32p) {
+    u32 q = (u32)((double)w * r32p);
+    const long long r = (long long)(((u64)w << 32) - (u64)q * p);
+    if (r < 0) --q;
+    else if (r >= (long long)p) ++q;
+    return q;
+}
+
+// Per-row factor tables of the split row kernels' level 0.
+//
+// Level 0 of the row DFT of slot s (column frequency k1, W = w_n^k1) takes
+// task o's inputs c = o + TB0 m times the inter-pass twiddle W^c, runs a
+// radix-R0 DIF and multiplies output j by the level twiddle w_n2^(o rev(j)).
+// W^c = W^o * W^(TB0 m), and the common factor W^o of a task commutes with
+// the DIF, so the level is: inputs times V_m = W^(TB0 m) (the slot factors),
+// DIF, outputs times U_j^o with U_j = W w_n2^rev(j).  U_j^o is the product
+// of two table entries, U_j^(o mod NA) and U_j^(NA (o div NA)), so no
+// twiddle of level 0 is read from L2 inside the level.  An entry
+// U_j^e = W^e * w_n2^(e rev(j)) is a power of W (from the seed tables) times
+// the level-0 twiddle table entry (e, j).  The inverse level uses the
+// inverse factors: inputs times U_j^-o, DIT, outputs times W^-(TB0 m) with
+// the 2^32/n scale.  A slot's table (one direction: the U entries, then the
+// R0 slot factors) depends only on the prime and the transform shape: it is
+// built once into HBM (k_rowtab_build) and copied into shared memory next to
+// the row; without it (rowtab == nullptr) each CTA builds its own.  Rows
+// shorter than 2^11 words keep computing W^c from the seeds per task: there
+// the table would cost more than it saves.
+template <int L2>
+struct RowTab {
+    using LV0 = SmallLevel<L2, 0>;
+    static constexpr bool USE = L2 >= 11;
+    static constexpr int R0 = LV0::R, TB0 = LV0::TB;
+    static constexpr int LOGTB = LV0::LOGB - LV0::PL.logr[0];
+    static constexpr int LA = (LOGTB + 1) / 2;
+    static constexpr int NA = 1 << LA, NB = TB0 >> LA;
+    static constexpr int ENTRIES = USE ? R0 * (NA + NB) : 0;  // [j][NA] then [j][NB]
+    static constexpr int TABW = USE ? ENTRIES + R0 : 0;        // + the slot factors
+    static constexpr int NPOW = USE ? NA + NB : 0;             // W^e: e < NA, then e = NA k
+};
+
+// Slot factors of one direction into f[0, R0): W^(TB0 m), or W^-(TB0 m)
+// times 2^32/n (the inverse's output factors).
+template <int L2>
+__device__ __forceinline__ void row_slot_entries(Tw* f, const LargeArgs& A, u32 k1, bool inv) {
+    using LV0 = SmallLevel<L2, 0>;
+    const u32 nmask = (1u << (A.l1 + L2)) - 1;
+    const u32 p = A.pk.p, pinv = A.pk.pinv_neg;
+    if (threadIdx.x < LV0::R) {
+        const u32 m = threadIdx.x;
+        u32 v = red1(mul_mont(seed_mont(A, (k1 * (u32)LV0::TB * m) & nmask, inv), 1u, p, pinv), p);
+        if (inv) v = (u32)(((u64)v * A.scale_rn) % p);
+        f[m] = Tw{v, shoup_quot_dev(v, p, A.r32p)};
+    }
+}
+
+// W^(+-e) * 2^32 for the table's exponents (e < NA, then e = NA k).
 template <int L2, int T>
-__device__ __forceinline__ void row_level0_fwd(u32* sm, const LargeArgs& A, u32 k1, const Tw* bf) {
+__device__ __forceinline__ void row_wpow_build(u32* wp, const LargeArgs& A, u32 k1, bool inv) {
+    using RT = RowTab<L2>;
+    const u32 nmask = (1u << (A.l1 + L2)) - 1;
+    for (int i = threadIdx.x; i < RT::NPOW; i += T) {
+        const u32 e = i < RT::NA ? (u32)i : (u32)(i - RT::NA) * RT::NA;
+        wp[i] = seed_mont(A, (k1 * e) & nmask, inv);
+    }
+}
+
+// The U entries of one direction from the powers wp and that direction's
+// level-0 twiddles twl (entry e R0 + j = w_n2^(+-e rev(j))).  The loop runs
+// j fastest so the twiddle reads are coalesced.
+template <int L2, int T>
+__device__ __forceinline__ void row_tab_build(Tw* tab, const u32* wp, const Tw* __restrict__ twl, const LargeArgs& A) {
+    using RT = RowTab<L2>;
+    const u32 p = A.pk.p, pinv = A.pk.pinv_neg;
+    for (int q = threadIdx.x; q < RT::ENTRIES; q += T) {
+        const int j = q % RT::R0;
+        int e, w, at;
+        if (q < RT::R0 * RT::NA) {
+            const int a = q / RT::R0;
+            e = a; w = a; at = j * RT::NA + a;
+        } else {
+            const int k = (q - RT::R0 * RT::NA) / RT::R0;
+            e = k * RT::NA; w = RT::NA + k; at = RT::R0 * RT::NA + j * RT::NB + k;
+        }
+        const u32 v = red1(mul_mont(wp[w], __ldg(&twl[e * RT::R0 + j].w), p, pinv), p);
+        tab[at] = Tw{v, shoup_quot_dev(v, p, A.r32p)};
+    }
+}
+
+// One slot's table of one direction into tab (shared or global memory):
+// from HBM when the prebuilt tables exist (cp.async, one commit group; the
+// caller waits), else built here (wp: NPOW words of shared scratch; the
+// caller's barrier must separate this from the table's first read).
+template <int L2, int T>
+__device__ __forceinline__ void row_tab_fetch(Tw* tab, u32* wp, const LargeArgs& A, u32 s, u32 k1, bool inv) {
+    using RT = RowTab<L2>;
+    if (A.rowtab) {
+        const Tw* src = A.rowtab + ((size_t)(inv ? 1 : 0) * (1u << A.l1) + s) * RT::TABW;
+        for (int i = threadIdx.x; i < RT::TABW / 2; i += T) {
+            const unsigned d = (unsigned)__cvta_generic_to_shared(tab + 2 * i);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + 2 * i) : "memory");
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    } else {
+        row_slot_entries<L2>(tab + RT::ENTRIES, A, k1, inv);
+        row_wpow_build<L2, T>(wp, A, k1, inv);
+        __syncthreads();
+        row_tab_build<L2, T>(tab, wp, inv ? A.twr + A.twr_inv : A.twr, A);
+    }
+}
+
+// Builds every slot's tables into HBM: grid (n1 slots, 2 directions).
+template <int L2>
+__global__ void __launch_bounds__(rowsplit_threads(L2)) k_rowtab_build(const __grid_constant__ LargeArgs A, Tw* out) {
+    using RT = RowTab<L2>;
+    __shared__ u32 wp[RT::NPOW > 0 ? RT::NPOW : 1];
+    const u32 s = blockIdx.x;
+    const bool inv = blockIdx.y != 0;
+    const u32 k1 = col_slot_to_k1(s, A.colpl, A.l1);
+    Tw* dst = out + ((size_t)blockIdx.y * gridDim.x + s) * RT::TABW;
+    row_slot_entries<L2>(dst + RT::ENTRIES, A, k1, inv);
+    row_wpow_build<L2, rowsplit_threads(L2)>(wp, A, k1, inv);
+    __syncthreads();
+    row_tab_build<L2, rowsplit_threads(L2)>(dst, wp, inv ? A.twr + A.twr_inv : A.twr, A);
+}
+
+// Level 0 forward of one operand computing the inter-pass twiddle W^c per
+// task from the seeds (short rows).
+template <int L2, int T>
+__device__ __forceinline__ void row_level0_fwd_seeds(u32* sm, const LargeArgs& A, u32 k1, const Tw* bf) {
     using LV0 = SmallLevel<L2, 0>;
     constexpr int R0 = LV0::R, TB0 = LV0::TB;
     const u32 nmask = (1u << (A.l1 + L2)) - 1;
@@ -528,6 +795,34 @@ __device__ __forceinline__ void row_level0_fwd(u32* sm, const LargeArgs& A, u32 
     }
 }
 
+// Level 0 forward of one operand: slot factors on the inputs, DIF, the
+// per-row factors U_j^o on the outputs.
+template <int L2, int T>
+__device__ __forceinline__ void row_level0_fwd(u32* sm, const LargeArgs& A, const Tw* tab) {
+    using RT = RowTab<L2>;
+    constexpr int R0 = RT::R0, TB0 = RT::TB0;
+    const u32 p = A.pk.p, p2 = A.pk.p2;
+    const Tw* bf = tab + RT::ENTRIES;
+    for (int o = threadIdx.x; o < TB0; o += T) {
+        u32 x[R0];
+#pragma unroll
+        for (int m = 0; m < R0; ++m) {
+            const u32 v = sm[swz_task<TB0, (1 << L2)>(o, swz(o), m)];
+            x[m] = m == 0 ? v : mul_shoup(v, bf[m].w, bf[m].wq, p);
+        }
+        dif_regs<R0, true>(x, A.pk.rc.f, p, p2);
+        const Tw* ta = tab + (o % RT::NA);
+        const Tw* tb = tab + RT::R0 * RT::NA + o / RT::NA;
+#pragma unroll
+        for (int j = 0; j < R0; ++j) {
+            const Tw a = ta[j * RT::NA], b = tb[j * RT::NB];
+            x[j] = mul_shoup(mul_shoup(x[j], a.w, a.wq, p), b.w, b.wq, p);
+        }
+#pragma unroll
+        for (int m = 0; m < R0; ++m) sm[swz_task<TB0, (1 << L2)>(o, swz(o), m)] = x[m];
+    }
+}
+
 template <int L2>
 __global__ void __launch_bounds__(rowsplit_threads(L2), rowsplit_ctas(L2)) k_row_fwd_g(const __grid_constant__ LargeArgs A) {
     constexpr int n2 = 1 << L2;
@@ -535,19 +830,25 @@ __global__ void __launch_bounds__(rowsplit_threads(L2), rowsplit_ctas(L2)) k_row
     constexpr LevelPlan PL = row_plan(L2);
     static_assert(PL.nlev >= 2, "row pass needs at least two levels");
     constexpr int R0 = SmallLevel<L2, 0>::R;
+    // the row, then the level-0 factor table (and scratch to build it)
     extern __shared__ __align__(16) u32 sm[];
     __shared__ Tw bf[R0];
+    Tw* tab = reinterpret_cast<Tw*>(sm + n2);
+    u32* wp = reinterpret_cast<u32*>(tab + RowTab<L2>::TABW);
     const LargeJob& J = A.jobs ? A.jobs[blockIdx.y] : A.job0;
     const u32 s = blockIdx.x;
     const u32 k1 = col_slot_to_k1(s, A.colpl, A.l1);
     const u32 p = A.pk.p, p2 = A.pk.p2;
     u32* row = J.wb + (size_t)s * n2;
     pdl_trigger();
-    row_slot_factors<L2>(A, k1, bf, nullptr);
+    if constexpr (RowTab<L2>::USE) row_tab_fetch<L2, T>(tab, wp, A, s, k1, false);
+    else row_slot_factors<L2>(A, k1, bf, nullptr);
     pdl_wait();  // pass A's columns of G
-    row_load<L2, T>(sm, row);
+    row_load_issue<L2, T>(sm, row);
+    row_load_wait();
     __syncthreads();
-    row_level0_fwd<L2, T>(sm, A, k1, bf);
+    if constexpr (RowTab<L2>::USE) row_level0_fwd<L2, T>(sm, A, tab);
+    else row_level0_fwd_seeds<L2, T>(sm, A, k1, bf);
     __syncthreads();
     fwd1_levels<L2, 1, T>(sm, A.pk, A.twr);
     for (int r = threadIdx.x; r < n2 / 32; r += T) {
@@ -570,12 +871,14 @@ __global__ void __launch_bounds__(rowsplit_threads(L2), rowsplit_ctas(L2)) k_row
     static_assert(PL.nlev >= 2, "row pass needs at least two levels");
     using LV0 = SmallLevel<L2, 0>;
     constexpr int R0 = LV0::R, TB0 = LV0::TB;
+    // the row, then the level-0 factor table (and scratch to build it)
     extern __shared__ __align__(16) u32 sm[];
     __shared__ Tw bf[R0], bi[R0];
+    Tw* tab = reinterpret_cast<Tw*>(sm + n2);
+    u32* wp = reinterpret_cast<u32*>(tab + RowTab<L2>::TABW);
     const LargeJob& J = A.jobs ? A.jobs[blockIdx.y] : A.job0;
     const u32 s = blockIdx.x;
     const u32 k1 = col_slot_to_k1(s, A.colpl, A.l1);
-    const u32 nmask = (1u << (A.l1 + L2)) - 1;
     const u32 p = A.pk.p, p2 = A.pk.p2, pinv = A.pk.pinv_neg;
     u32* rowF = J.wa + (size_t)s * n2;
     const u32* rowG = J.wb + (size_t)s * n2;
@@ -584,11 +887,17 @@ __global__ void __launch_bounds__(rowsplit_threads(L2), rowsplit_ctas(L2)) k_row
     // F's forward row pass depends only on pass A (complete before the
     // previous kernel, G's row pass, started), so it runs while that kernel
     // finishes; G's spectrum is read after pdl_wait
-    row_slot_factors<L2>(A, k1, bf, bi);
-    row_load<L2, T>(sm, rowF);
+    row_load_issue<L2, T>(sm, rowF);
+    if constexpr (RowTab<L2>::USE) row_tab_fetch<L2, T>(tab, wp, A, s, k1, false);
+    else row_slot_factors<L2>(A, k1, bf, bi);
+    row_load_wait();
     __syncthreads();
-    row_level0_fwd<L2, T>(sm, A, k1, bf);
+    if constexpr (RowTab<L2>::USE) row_level0_fwd<L2, T>(sm, A, tab);
+    else row_level0_fwd_seeds<L2, T>(sm, A, k1, bf);
     __syncthreads();
+    // level 0's inverse factors replace the forward ones; they are waited
+    // for (prebuilt) or visible (built here) after the barriers below
+    if constexpr (RowTab<L2>::USE) row_tab_fetch<L2, T>(tab, wp, A, s, k1, true);
     fwd1_levels<L2, 1, T>(sm, A.pk, A.twr);
     pdl_wait();
     for (int r = threadIdx.x; r < n2 / 32; r += T) {
@@ -606,22 +915,43 @@ __global__ void __launch_bounds__(rowsplit_threads(L2), rowsplit_ctas(L2)) k_row
         dit_regs<32>(x, A.pk.rc.i, p, p2);
         store_row32(sm, r * 32, x);
     }
+    row_load_wait();  // the inverse factor table
     __syncthreads();
     small_inv_levels<L2, PL.nlev - 2, T, 1, 1>(sm, ctx);
-    for (int o = threadIdx.x; o < TB0; o += T) {
-        u32 x[R0];
+    // level 0 inverse: inputs times U_j^-o, DIT, outputs times W^-(TB0 m) 2^32/n
+    using RT = RowTab<L2>;
+    if constexpr (RT::USE) {
+        const Tw* bo = tab + RT::ENTRIES;
+        for (int o = threadIdx.x; o < TB0; o += T) {
+            u32 x[R0];
+            const Tw* ta = tab + (o % RT::NA);
+            const Tw* tb = tab + RT::R0 * RT::NA + o / RT::NA;
 #pragma unroll
-        for (int m = 0; m < R0; ++m) x[m] = sm[swz_task<TB0, n2>(o, swz(o), m)];
-        Tw t[R0];
-        load_tw<R0>(t, A.twr + A.twr_inv + o * R0);
+            for (int j = 0; j < R0; ++j) {
+                const Tw a = ta[j * RT::NA], b = tb[j * RT::NB];
+                x[j] = mul_shoup(mul_shoup(sm[swz_task<TB0, n2>(o, swz(o), j)], a.w, a.wq, p), b.w, b.wq, p);
+            }
+            dit_regs<R0, true>(x, A.pk.rc.i, p, p2);
 #pragma unroll
-        for (int j = 1; j < R0; ++j) x[j] = mul_shoup(x[j], t[j].w, t[j].wq, p);
-        dit_regs<R0, true>(x, A.pk.rc.i, p, p2);
-        const u32 mo = seed_mont(A, (k1 * (u32)o) & nmask, true);  // w^-(k1 o) * 2^32
+            for (int m = 0; m < R0; ++m) rowF[o + TB0 * m] = mul_shoup(x[m], bo[m].w, bo[m].wq, p);
+        }
+    } else {  // short rows: level twiddles from the table, W^-c from the seeds
+        const u32 nmask = (1u << (A.l1 + L2)) - 1;
+        for (int o = threadIdx.x; o < TB0; o += T) {
+            u32 x[R0];
 #pragma unroll
-        for (int m = 0; m < R0; ++m) {
-            const u32 d = mul_shoup(mo, bi[m].w, bi[m].wq, p);  // w^-(k1 c) * 2^64 / n
-            rowF[o + TB0 * m] = mul_mont(red2(x[m], p2), d, p, pinv);
+            for (int m = 0; m < R0; ++m) x[m] = sm[swz_task<TB0, n2>(o, swz(o), m)];
+            Tw t[R0];
+            load_tw<R0>(t, A.twr + A.twr_inv + o * R0);
+#pragma unroll
+            for (int j = 1; j < R0; ++j) x[j] = mul_shoup(x[j], t[j].w, t[j].wq, p);
+            dit_regs<R0, true>(x, A.pk.rc.i, p, p2);
+            const u32 mo = seed_mont(A, (k1 * (u32)o) & nmask, true);  // w^-(k1 o) * 2^32
+#pragma unroll
+            for (int m = 0; m < R0; ++m) {
+                const u32 d = mul_shoup(mo, bi[m].w, bi[m].wq, p);  // w^-(k1 c) * 2^64 / n
+                rowF[o + TB0 * m] = mul_mont(red2(x[m], p2), d, p, pinv);
+            }
         }
     }
 }

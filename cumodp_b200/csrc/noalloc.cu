@@ -147,6 +147,7 @@ int mul_dev_noalloc(const u32* a, long long la, const u32* b, long long lb, u32*
         A.l1 = l1;
         A.l2 = l2;
         A.colpl = col_plan(l1);
+        A.r32p = 4294967296.0 / (double)p;
         u32* ws = D.base;  // workspace: the first 2n words of the array
         A.job0 = LargeJob{a, b, h, (int)la, (int)lb, (int)lh, 0, ws, ws + n};
         A.njobs = 1;

@@ -70,11 +70,13 @@ __host__ __device__ __forceinline__ u32 rev_bits(u32 j, int r) {
 // Forward R-point DIF on registers; x[j] ends holding X[bitrev_r(j)].
 // Inputs in [0, 2p).  Outputs in [0, 2p), except that with TW (the caller
 // multiplies every output j >= 1 by a Shoup twiddle next, which accepts any
-// 32-bit input) the last stage leaves outputs j >= 1 in [0, 4p).
-template <int R, bool TW = false>
+// 32-bit input) the last stage leaves outputs j >= 1 in [0, 4p).  H0 < R/2
+// runs only the stages of butterfly span H0, H0/2, ..., 1 (the caller did
+// the earlier ones).
+template <int R, bool TW = false, int H0 = R / 2>
 __device__ __forceinline__ void dif_regs(u32 (&x)[R], const Tw* __restrict__ c, u32 p, u32 p2) {
 #pragma unroll
-    for (int half = R / 2; half >= 1; half >>= 1) {
+    for (int half = H0; half >= 1; half >>= 1) {
 #pragma unroll
         for (int g = 0; g < R; g += 2 * half) {
 #pragma unroll
@@ -89,6 +91,24 @@ __device__ __forceinline__ void dif_regs(u32 (&x)[R], const Tw* __restrict__ c, 
             }
         }
     }
+}
+
+// Forward R-point DIF whose inputs R/2 .. R-1 are zero: x[0 .. R/2) hold
+// raw words (any 32-bit value, reduced here) and x[R/2 .. R) are ignored.
+// The first stage reduces to x[j] = v, x[j + R/2] = v * w_R^j; the rest is
+// dif_regs.  Same output ranges as dif_regs<R, TW>.
+template <int R, bool TW = false>
+__device__ __forceinline__ void dif_regs_halfzero(u32 (&x)[R], const Tw* __restrict__ c, u32 p, u32 p2,
+                                                  u32 one_q) {
+#pragma unroll
+    for (int j = 0; j < R / 2; ++j) {
+        const int e = j * (32 / R);
+        const u32 v = x[j];
+        const u32 r = mul_shoup(v, 1u, one_q, p);
+        x[j] = r;
+        x[j + R / 2] = e == 0 ? r : mul_shoup(v, c[e].w, c[e].wq, p);
+    }
+    dif_regs<R, TW, R / 4>(x, c, p, p2);
 }
 
 // Inverse R-point DIT on registers (roots c = w_32^-j); x[j] holds Y[bitrev(j)]

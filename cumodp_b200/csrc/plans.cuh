@@ -98,6 +98,19 @@ __host__ __device__ constexpr int col_smem_bytes(int logl, int kind) {
     return col_tile_words(logl, kind) * 4 + (col_tw_smem(logl, kind) ? col_tw_entries(logl) * 8 : 0);
 }
 
+// Persistent pass A (k_col_fwd_pipe) for the two-level column plans with
+// 32-column tiles: one CTA per SM of 512 threads with up to 128 registers
+// each (a warp holds two level tasks at once; 1024 threads at 64 registers
+// spill, and for n1 = 2^9 two 512-thread CTAs per SM measured slower).
+// Shared memory: the tile, a stage of its first n1/2 rows and the level-0
+// twiddles.
+__host__ __device__ constexpr bool col_pipe_ok(int logl) { return logl == 9 || logl == 10; }
+__host__ __device__ constexpr int col_pipe_warps(int logl) { return 16; }
+__host__ __device__ constexpr int col_pipe_ctas(int logl) { return 1; }
+__host__ __device__ constexpr int col_pipe_smem_bytes(int logl) {
+    return (32 << logl) * 4 + (16 << logl) * 4 + (1 << logl) * 8;
+}
+
 // A single product (no batch) of transform length 2^logn uses the three-pass
 // kernels from this length on, even where one CTA could hold it: spread over
 // many CTAs it finishes sooner than on one SM.

@@ -2,6 +2,9 @@
 #include "product.cuh"
 
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <cstdlib>
 #include <cstring>
 
@@ -57,6 +60,35 @@ void launch_col_fwd_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
     }
     k_col_fwd<L1, col_warps(L1, false)><<<grid, col_warps(L1, false) * 32, smem, st>>>(a);
 }
+// SMs of the current device (cached per device).
+int sm_count(int dev) {
+    static int cache[64] = {0};
+    if (dev < 0 || dev >= 64) return 148;
+    if (!cache[dev]) {
+        int v = 0;
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        cache[dev] = v > 0 ? v : 148;
+    }
+    return cache[dev];
+}
+
+// Whether pass A uses the persistent pipelined kernel where it applies
+// (CUMODP_COL_PIPE=0 selects the one-tile-per-CTA kernel, for comparison).
+bool col_pipe_enabled() {
+    static const bool on = [] {
+        const char* e = getenv("CUMODP_COL_PIPE");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+template <int L1>
+void launch_col_fwd_pipe_t(const LargeArgs& a, int ntiles, cudaStream_t st) {
+    constexpr int smem = col_pipe_smem_bytes(L1);
+    const int grid = std::min(ntiles, sm_count(current_device()) * col_pipe_ctas(L1));
+    k_col_fwd_pipe<L1, col_pipe_warps(L1)><<<grid, col_pipe_warps(L1) * 32, smem, st>>>(a);
+}
+
 template <int L1>
 void launch_col_inv_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
     const size_t smem = col_smem_bytes(L1, true);
@@ -78,13 +110,79 @@ void launch_row_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
     k_row_fused<L2><<<grid, row_threads(L2), smem, st>>>(a);
 }
 
+// Dynamic shared memory of the split row kernels: the row, its level-0
+// factor table and the scratch to build the table in place.
+template <int L2>
+constexpr size_t rowsplit_smem() {
+    return (size_t)(1 << L2) * sizeof(u32) + (size_t)RowTab<L2>::TABW * sizeof(Tw) +
+           (size_t)RowTab<L2>::NPOW * sizeof(u32);
+}
+
+template <int L2>
+void launch_rowtab_t(const LargeArgs& a, Tw* out, cudaStream_t st) {
+    k_rowtab_build<L2><<<dim3(1u << a.l1, 2), rowsplit_threads(L2), 0, st>>>(a, out);
+}
+typedef void (*RowTabFn)(const LargeArgs&, Tw*, cudaStream_t);
+RowTabFn rowtab_fn(int l2) {
+    switch (l2) {
+        case 11: return launch_rowtab_t<11>;
+        case 12: return launch_rowtab_t<12>;
+        case 13: return launch_rowtab_t<13>;
+        case 14: return launch_rowtab_t<14>;
+        default: return nullptr;
+    }
+}
+size_t rowtab_words(int l2) {
+    switch (l2) {
+        case 11: return RowTab<11>::TABW;
+        case 12: return RowTab<12>::TABW;
+        case 13: return RowTab<13>::TABW;
+        case 14: return RowTab<14>::TABW;
+        default: return 0;
+    }
+}
+
+// Every slot's level-0 factor tables (both directions) for the transform
+// shape of `a`, built once on the device and kept for the process; nullptr
+// (the row kernels then build each table themselves) for rows without
+// tables or when the memory is not there.
+const Tw* row_factor_tables(const LargeArgs& a, int dev, u32 p, u32 root_n, int logn) {
+    const RowTabFn fn = rowtab_fn(a.l2);
+    if (!fn) return nullptr;
+    static const bool off = [] {  // CUMODP_ROWTAB=0: kernels build their tables (for comparison)
+        const char* e = getenv("CUMODP_ROWTAB");
+        return e && e[0] == '0';
+    }();
+    if (off) return nullptr;
+    static std::mutex m;
+    static std::map<std::tuple<int, u32, u32, int, int>, Tw*> cache;
+    std::lock_guard<std::mutex> g(m);
+    const auto key = std::make_tuple(dev, p, root_n, logn, a.l2);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    const size_t bytes = (size_t)2 * ((size_t)1 << a.l1) * rowtab_words(a.l2) * sizeof(Tw);
+    Tw* d = nullptr;
+    if (dev_malloc((void**)&d, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    const cudaStream_t st = lib_stream(dev);
+    fn(a, d, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+        cudaFree(d);
+        return nullptr;
+    }
+    account_bytes((long long)bytes);
+    cache[key] = d;
+    return d;
+}
 template <int L2>
 void launch_row_g_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
-    launch_pdl(k_row_fwd_g<L2>, grid, rowsplit_threads(L2), (size_t)(1 << L2) * sizeof(u32), st, a);
+    launch_pdl(k_row_fwd_g<L2>, grid, rowsplit_threads(L2), rowsplit_smem<L2>(), st, a);
 }
 template <int L2>
 void launch_row_f_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
-    launch_pdl(k_row_mul_f<L2>, grid, rowsplit_threads(L2), (size_t)(1 << L2) * sizeof(u32), st, a);
+    launch_pdl(k_row_mul_f<L2>, grid, rowsplit_threads(L2), rowsplit_smem<L2>(), st, a);
 }
 
 typedef void (*PassFn)(const LargeArgs&, dim3, cudaStream_t);
@@ -113,6 +211,11 @@ void attr_col() {
     cudaFuncSetAttribute(k_col_inv<L1, col_warps(L1, true)>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          col_smem_bytes(L1, true));
 }
+template <int L1>
+void attr_col_pipe() {
+    cudaFuncSetAttribute(k_col_fwd_pipe<L1, col_pipe_warps(L1)>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         col_pipe_smem_bytes(L1));
+}
 template <int L2>
 void attr_row() {
     cudaFuncSetAttribute(k_row_fused<L2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -121,7 +224,7 @@ void attr_row() {
 
 template <int L2>
 void attr_rowsplit() {
-    const int smem = (1 << L2) * (int)sizeof(u32);
+    const int smem = (int)rowsplit_smem<L2>();
     cudaFuncSetAttribute(k_row_fwd_g<L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     cudaFuncSetAttribute(k_row_mul_f<L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
@@ -150,6 +253,7 @@ void ensure_kernel_attrs() {
         attr_small<10>(); attr_small<11>(); attr_small<12>(); attr_small<13>(); attr_small<14>();
         attr_col<1>(); attr_col<2>(); attr_col<3>(); attr_col<4>(); attr_col<5>();
         attr_col<6>(); attr_col<7>(); attr_col<8>(); attr_col<9>(); attr_col<10>(); attr_col<11>();
+        attr_col_pipe<9>(); attr_col_pipe<10>();
         attr_row<6>(); attr_row<7>(); attr_row<8>(); attr_row<9>(); attr_row<10>();
         attr_row<11>(); attr_row<12>(); attr_row<13>(); attr_row<14>();
         attr_rowsplit<6>(); attr_rowsplit<7>(); attr_rowsplit<8>(); attr_rowsplit<9>(); attr_rowsplit<10>();
@@ -213,8 +317,10 @@ int large_args(const PrimeCtx& pc, u32 root_n, int logn, int l2, int dev, LargeA
     a->l1 = l1;
     a->l2 = l2;
     a->colpl = col_plan(l1);
+    a->r32p = 4294967296.0 / (double)p;
     const char* rf = getenv("CUMODP_ROW_FUSED");
     a->row_fused = rf && rf[0] == '1';
+    a->rowtab = row_factor_tables(*a, dev, p, root_n, logn);
     return OK;
 }
 
@@ -247,7 +353,13 @@ void launch_large(const LargeArgs& a, int njobs, cudaStream_t st) {
     NvtxRange range(kRowFName[a.l2]);  // the product's three passes, named by its dominant kernel
     cudaEvent_t e0;
     bool tr = pass_timing_begin(st, &e0);
-    kColFwd[a.l1](a, dim3(n2 / col_tile_cols_rt(a.l1, false), 2, njobs), st);
+    if (col_pipe_ok(a.l1) && col_pipe_enabled()) {
+        const int ntiles = (n2 / 32) * 2 * njobs;
+        if (a.l1 == 10) launch_col_fwd_pipe_t<10>(a, ntiles, st);
+        else launch_col_fwd_pipe_t<9>(a, ntiles, st);
+    } else {
+        kColFwd[a.l1](a, dim3(n2 / col_tile_cols_rt(a.l1, false), 2, njobs), st);
+    }
     if (tr) pass_timing_end(st, kColFwdName[a.l1], e0);
     if (a.row_fused) {
         tr = pass_timing_begin(st, &e0);

@@ -156,8 +156,6 @@ __global__ void k_crt_recombine(const __grid_constant__ CrtArgs A) {
 
 namespace {
 
-int bit_width_u64(unsigned long long m) { return m ? 64 - __builtin_clzll(m) : 1; }
-
 // log2 of prod of the first k primes (floor)
 double log2_prime_product(int k) {
     double s = 0;

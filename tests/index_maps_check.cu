@@ -12,7 +12,12 @@
 //            in bounds, tile_step equals tile_row differences for every level
 //            task, and the two half-warps of a 16-column tile read opposite
 //            halves of the banks;
-//   orders:  col_slot_to_k1 and row_pos_to_freq are permutations.
+//   orders:  col_slot_to_k1 and row_pos_to_freq are permutations;
+//   row factor tables (rows of 2^11..2^14 words): every level-0 task reads
+//            its two entries inside the table, the two digits recompose the
+//            task index, and the row kernels' shared memory fits the SM;
+//   pipelined column pass: stage, tile and twiddle indexes in bounds;
+//   Shoup quotients from the double estimate equal floor(w 2^32 / p).
 #include <cstdio>
 #include <set>
 #include <vector>
@@ -157,6 +162,77 @@ void col_plan_check() {
     for (int i = 0; i < (1 << L1); ++i) CHECK(k[i] == 1, "col_slot_to_k1 L1=%d not a permutation", L1);
 }
 
+template <int L2>
+void row_tab_check() {
+    using RT = RowTab<L2>;
+    CHECK(RT::NA * RT::NB == RT::TB0, "rowtab L2=%d digits", L2);
+    for (int o = 0; o < RT::TB0; ++o) {
+        CHECK((o % RT::NA) + RT::NA * (o / RT::NA) == o, "rowtab L2=%d recompose", L2);
+        for (int j = 0; j < RT::R0; ++j) {
+            const int ia = (o % RT::NA) + j * RT::NA;
+            const int ib = RT::R0 * RT::NA + o / RT::NA + j * RT::NB;
+            CHECK(ia >= 0 && ia < RT::R0 * RT::NA, "rowtab L2=%d A index", L2);
+            CHECK(ib >= RT::R0 * RT::NA && ib < RT::ENTRIES, "rowtab L2=%d B index", L2);
+        }
+    }
+    // build loop (row_tab_build's decode): every table slot written once, the
+    // power and twiddle read for it in bounds and of the slot's exponent
+    std::vector<int> hit(RT::ENTRIES, 0);
+    for (int q = 0; q < RT::ENTRIES; ++q) {
+        const int j = q % RT::R0;
+        int e, w, at;
+        if (q < RT::R0 * RT::NA) { const int a = q / RT::R0; e = a; w = a; at = j * RT::NA + a; }
+        else { const int k = (q - RT::R0 * RT::NA) / RT::R0; e = k * RT::NA; w = RT::NA + k; at = RT::R0 * RT::NA + j * RT::NB + k; }
+        CHECK(at >= 0 && at < RT::ENTRIES, "rowtab L2=%d build slot", L2);
+        if (at >= 0 && at < RT::ENTRIES) hit[at]++;
+        CHECK(w >= 0 && w < RT::NPOW, "rowtab L2=%d build power", L2);
+        CHECK(e * RT::R0 + j < plan_tw_entries(row_plan(L2), L2), "rowtab L2=%d build twiddle", L2);
+        // the slot the level reads for (o, j) has exponent o mod NA, resp. NA (o div NA)
+        if (q < RT::R0 * RT::NA) CHECK(at % RT::NA == e && at / RT::NA == j, "rowtab L2=%d A exponent", L2);
+        else CHECK((at - RT::R0 * RT::NA) % RT::NB * RT::NA == e, "rowtab L2=%d B exponent", L2);
+    }
+    for (int i = 0; i < RT::ENTRIES; ++i) CHECK(hit[i] == 1, "rowtab L2=%d slot %d written %d times", L2, i, hit[i]);
+    // shared memory of the split row kernels (+1 KiB reserved per CTA)
+    const long long smem = (long long)(1 << L2) * 4 + (long long)RT::TABW * 8 + (long long)RT::NPOW * 4 + 2 * RT::R0 * 8;
+    CHECK((RT::TABW * 8) % 16 == 0, "rowtab L2=%d table not a whole number of 16-byte copies", L2);
+    CHECK((smem + 1024) * rowsplit_ctas(L2) <= 228 * 1024, "rowsplit L2=%d shared memory", L2);
+}
+
+template <int L1>
+void col_pipe_check() {
+    constexpr LevelPlan PL = col_plan(L1);
+    constexpr int n1 = 1 << L1, HALF = n1 / 2, R0 = 1 << PL.logr[0], R1 = 1 << PL.logr[1];
+    CHECK(PL.nlev == 2 && R0 * R1 == n1, "colpipe L1=%d plan", L1);
+    for (int o = 0; o < R1; ++o)
+        for (int m = 0; m < R0; ++m) {
+            const int row = o + R1 * m;
+            CHECK(row < n1, "colpipe L1=%d level-0 row", L1);
+            if (m < R0 / 2) CHECK(row < HALF, "colpipe L1=%d stage row", L1);
+            else CHECK(row >= HALF, "colpipe L1=%d upper row", L1);
+            CHECK(o * R0 + m < col_tw_entries(L1), "colpipe L1=%d twiddle", L1);
+        }
+    for (int blk = 0; blk < R0; ++blk)
+        for (int m = 0; m < R1; ++m) CHECK(blk * R1 + m < n1, "colpipe L1=%d level-1 row", L1);
+    CHECK(col_pipe_smem_bytes(L1) == n1 * 128 + HALF * 128 + col_tw_entries(L1) * 8, "colpipe L1=%d layout", L1);
+    CHECK((col_pipe_smem_bytes(L1) + 1024) * col_pipe_ctas(L1) <= 228 * 1024, "colpipe L1=%d shared memory", L1);
+}
+
+void shoup_quot_check() {
+    const u32 primes[] = {469762049u, 754974721u, 962592769u, 950009857u, 940572673u, 998244353u,
+                          257u, 7681u, 12289u, 40961u, 1073479681u};
+    unsigned long long st = 0x9E3779B97F4A7C15ull;
+    for (u32 p : primes) {
+        const double r = 4294967296.0 / (double)p;
+        for (int k = 0; k < 200000; ++k) {
+            st ^= st << 13; st ^= st >> 7; st ^= st << 17;
+            u32 w = (u32)(st % p);
+            if (k < 4) w = k < 2 ? (u32)k : p - (u32)(k - 1);
+            const u32 want = (u32)(((unsigned long long)w << 32) / p);
+            CHECK(shoup_quot_dev(w, p, r) == want, "shoup quotient p=%u w=%u", p, w);
+        }
+    }
+}
+
 int main() {
     row_plan_check<5>();
     row_plan_check<6>();
@@ -179,6 +255,13 @@ int main() {
     col_plan_check<9>();
     col_plan_check<10>();
     col_plan_check<11>();
+    row_tab_check<11>();
+    row_tab_check<12>();
+    row_tab_check<13>();
+    row_tab_check<14>();
+    col_pipe_check<9>();
+    col_pipe_check<10>();
+    shoup_quot_check();
     std::printf("%s: %d failures\n", failures ? "FAILED" : "OK", failures);
     return failures ? 1 : 0;
 }

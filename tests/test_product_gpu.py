@@ -42,6 +42,36 @@ def test_three_pass_products(cm, oracle_mod, p, da, db):
     assert np.array_equal(got, want)
 
 
+@pytest.mark.parametrize("da,db", [(600000, 100), (100, 600000), (5000000, 10), (3000000, 3000000)])
+def test_column_pass_long_operands(cm, oracle_mod, da, db):
+    """Transforms of 2^20 and 2^23 words (1024- and 512-row columns) where an
+    operand is longer than half the transform, so its columns have no zero
+    half, and a balanced 2^23 case."""
+    r = SplitMix64(hash((da, db, 5)) & 0xFFFFFFFF)
+    a, b = _rand(r, da + 1, P0), _rand(r, db + 1, P0)
+    assert np.array_equal(cm.fftmul_uni(a, b, P0), oracle_mod.polymul(a, b, P0))
+
+
+@pytest.mark.parametrize("da,db,off", [(2**19 - 1, 2**19 - 1, 1), (2**19 - 1, 2**19 - 1, 3), (700000, 2**19 - 10, 2),
+                                       (2**22 - 1, 2**22 - 1, 1)])
+def test_column_pass_unaligned_device_operands(cm, oracle_mod, da, db, off):
+    """Device operands that start off a 16-byte boundary (offsets of 4-12
+    bytes), through cumodp_fftmul_uni_dev."""
+    import torch
+    r = SplitMix64(hash((da, db, off)) & 0xFFFFFFFF)
+    a, b = _rand(r, da + 1, P0), _rand(r, db + 1, P0)
+    ta = torch.zeros(da + 1 + off, dtype=torch.int32, device="cuda")
+    tb = torch.zeros(db + 1 + off, dtype=torch.int32, device="cuda")
+    ta[off:] = torch.from_numpy(a.view(np.int32)).cuda()
+    tb[off:] = torch.from_numpy(b.view(np.int32)).cuda()
+    lh = da + db + 1
+    th = torch.zeros(lh + off, dtype=torch.int32, device="cuda")
+    cm.fftmul_uni_dev(th.data_ptr() + 4 * off, lh, ta.data_ptr() + 4 * off, da, tb.data_ptr() + 4 * off, db, P0)
+    torch.cuda.synchronize()
+    got = th[off:].cpu().numpy().view(np.uint32)
+    assert np.array_equal(got, oracle_mod.polymul(a, b, P0))
+
+
 def test_c1_config_vs_modpn(cm, oracle_mod):
     """4095 x 4095 mod 469762049 (transform 8192) against modpn's own product."""
     r = SplitMix64(0xC0DA0000)
