@@ -451,6 +451,90 @@ __global__ void __launch_bounds__(NW * 32, col_pipe_ctas(L1)) k_col_fwd_pipe(con
     }
 }
 
+// Pass C as a persistent, software-pipelined kernel for the two-level
+// column plans (n1 = 2^9: 32-column tiles, n1 = 2^10: 16-column tiles, the
+// inverse pass's layouts).  Each CTA walks the tiles gridDim.x apart; the
+// whole next tile is copied into a stage buffer (cp.async) while the current
+// one is transformed.  The deepest level reads the stage and writes the
+// tile; level 0 reads the tile and stores the canonical residues straight to
+// the output, truncated at lh.  Results are those of k_col_inv.
+template <int L1, int NW>
+__global__ void __launch_bounds__(NW * 32, 1) k_col_inv_pipe(const __grid_constant__ LargeArgs A) {
+    constexpr LevelPlan PL = col_plan(L1);
+    static_assert(PL.nlev == 2, "two-level column plans only");
+    constexpr int INV = 1, T = NW * 32;
+    constexpr int TC = col_tile_cols(L1, INV), SUB = 32 / TC, QR = TC / 4;
+    constexpr int n1 = 1 << L1, R0 = 1 << PL.logr[0], R1 = 1 << PL.logr[1];  // n1 = R0 * R1
+    constexpr int TW = col_tile_words(L1, INV);
+    extern __shared__ __align__(16) u32 smem[];
+    u32* tile = smem;
+    u32* stage = smem + TW;
+    Tw* tws = reinterpret_cast<Tw*>(stage + TW);  // inverse level-0 twiddles (n1 entries)
+    const int n2 = 1 << A.l2, ct = n2 / TC;
+    const int ntiles = ct * A.njobs;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int col = lane % TC;
+    const u32 p = A.pkc.p, p2 = A.pkc.p2;
+    for (int i = threadIdx.x; i < n1; i += T) tws[i] = A.twc[A.twc_inv + i];
+
+    // the whole tile t (all n1 rows of the row pass's output) into the stage
+    auto stage_issue = [&](int t) {
+        const LargeJob& J = A.jobs ? A.jobs[t / ct] : A.job0;
+        const u32* src = J.wa + (t % ct) * TC;
+#pragma unroll 4
+        for (int idx = threadIdx.x; idx < n1 * QR; idx += T) {
+            const int r = idx / QR, q = idx % QR;
+            const unsigned d = (unsigned)__cvta_generic_to_shared(stage + tile_row<L1, INV>(r) + 4 * q);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + (size_t)r * n2 + 4 * q)
+                         : "memory");
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+
+    pdl_wait();  // pass B's output
+    int t = blockIdx.x;
+    if (t < ntiles) stage_issue(t);
+    for (; t < ntiles; t += gridDim.x) {
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        __syncthreads();  // stage and twiddles visible; the previous tile's level 0 is done with `tile`
+
+        // deepest level: blocks of R1 consecutive rows, DIT, stage -> tile
+        for (int id = warp * SUB + lane / TC; id < R0; id += NW * SUB) {
+            u32 x[R1];
+            const int off = tile_row<L1, INV>(id * R1) + col;
+#pragma unroll
+            for (int m = 0; m < R1; ++m) x[m] = stage[off + tile_step<L1, INV, 1>(m)];
+            dit_regs<R1, false>(x, A.pkc.rc.i, p, p2);
+#pragma unroll
+            for (int m = 0; m < R1; ++m) tile[off + tile_step<L1, INV, 1>(m)] = x[m];
+        }
+        __syncthreads();  // tile complete; the stage is free
+        if (t + (int)gridDim.x < ntiles) stage_issue(t + gridDim.x);
+
+        // level 0: task o (rows o + R1 m), pre-twiddle, DIT, canonical residues out
+        const LargeJob& J = A.jobs ? A.jobs[t / ct] : A.job0;
+        const long long lh = J.lh;
+        const int c0 = (t % ct) * TC;
+        for (int o = warp * SUB + lane / TC; o < R1; o += NW * SUB) {
+            u32 x[R0];
+            const int off = tile_row<L1, INV>(o) + col;
+#pragma unroll
+            for (int m = 0; m < R0; ++m) x[m] = tile[off + tile_step<L1, INV, R1>(m)];
+#pragma unroll
+            for (int j = 1; j < R0; ++j) {
+                const Tw w = tws[o * R0 + j];
+                x[j] = mul_shoup(x[j], w.w, w.wq, p);
+            }
+            dit_regs<R0, true>(x, A.pkc.rc.i, p, p2);
+#pragma unroll
+            for (int m = 0; m < R0; ++m) {
+                const long long gi = (long long)(o + R1 * m) * n2 + c0 + col;
+                if (gi < lh) J.h[gi] = red1(red2(x[m], p2), p);
+            }
+        }
+    }
+}
+
 // pass C, grid: (n2/TC column tiles, 1, jobs)
 template <int L1, int NW>
 __global__ void __launch_bounds__(NW * 32, col_ctas(L1, true)) k_col_inv(const __grid_constant__ LargeArgs A) {

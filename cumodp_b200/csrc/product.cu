@@ -90,6 +90,13 @@ void launch_col_fwd_pipe_t(const LargeArgs& a, int ntiles, cudaStream_t st) {
 }
 
 template <int L1>
+void launch_col_inv_pipe_t(const LargeArgs& a, int ntiles, cudaStream_t st) {
+    const int grid = std::min(ntiles, sm_count(current_device()));
+    launch_pdl(k_col_inv_pipe<L1, col_pipe_warps(L1)>, dim3(grid), col_pipe_warps(L1) * 32,
+               (size_t)col_inv_pipe_smem_bytes(L1), st, a);
+}
+
+template <int L1>
 void launch_col_inv_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
     const size_t smem = col_smem_bytes(L1, true);
     static bool attr = false;
@@ -215,6 +222,8 @@ template <int L1>
 void attr_col_pipe() {
     cudaFuncSetAttribute(k_col_fwd_pipe<L1, col_pipe_warps(L1)>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          col_pipe_smem_bytes(L1));
+    cudaFuncSetAttribute(k_col_inv_pipe<L1, col_pipe_warps(L1)>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         col_inv_pipe_smem_bytes(L1));
 }
 template <int L2>
 void attr_row() {
@@ -374,7 +383,13 @@ void launch_large(const LargeArgs& a, int njobs, cudaStream_t st) {
         if (tr) pass_timing_end(st, kRowFName[a.l2], e0);
     }
     tr = pass_timing_begin(st, &e0);
-    kColInv[a.l1](a, dim3(n2 / col_tile_cols_rt(a.l1, true), 1, njobs), st);
+    if (col_pipe_ok(a.l1) && col_pipe_enabled()) {
+        const int ntiles = (n2 / col_tile_cols_rt(a.l1, true)) * njobs;
+        if (a.l1 == 10) launch_col_inv_pipe_t<10>(a, ntiles, st);
+        else launch_col_inv_pipe_t<9>(a, ntiles, st);
+    } else {
+        kColInv[a.l1](a, dim3(n2 / col_tile_cols_rt(a.l1, true), 1, njobs), st);
+    }
     if (tr) pass_timing_end(st, kColInvName[a.l1], e0);
 }
 

@@ -217,6 +217,29 @@ void col_pipe_check() {
     CHECK((col_pipe_smem_bytes(L1) + 1024) * col_pipe_ctas(L1) <= 228 * 1024, "colpipe L1=%d shared memory", L1);
 }
 
+template <int L1>
+void col_inv_pipe_check() {
+    constexpr LevelPlan PL = col_plan(L1);
+    constexpr int n1 = 1 << L1, R0 = 1 << PL.logr[0], R1 = 1 << PL.logr[1];
+    constexpr int TC = col_tile_cols(L1, 1), QR = TC / 4, TW = col_tile_words(L1, 1);
+    // stage copies: every 16-byte quad of every row inside the stage, aligned
+    for (int idx = 0; idx < n1 * QR; ++idx) {
+        const int r = idx / QR, q = idx % QR;
+        const int a = tile_row<L1, 1>(r) + 4 * q;
+        CHECK((a % 4 == 0 && a + 3 < TW), "colinvpipe L1=%d stage quad", L1);
+    }
+    // deepest level (blocks of R1 rows) and level 0 (rows o + R1 m): in the tile
+    for (int id = 0; id < R0; ++id)
+        for (int m = 0; m < R1; ++m)
+            CHECK((tile_row<L1, 1>(id * R1) + tile_step<L1, 1, 1>(m) == tile_row<L1, 1>(id * R1 + m)), "colinvpipe L1=%d deep", L1);
+    for (int o = 0; o < R1; ++o)
+        for (int m = 0; m < R0; ++m) {
+            CHECK((tile_row<L1, 1>(o) + tile_step<L1, 1, R1>(m) == tile_row<L1, 1>(o + R1 * m)), "colinvpipe L1=%d lvl0", L1);
+            CHECK(o * R0 + m < n1, "colinvpipe L1=%d twiddle", L1);
+        }
+    CHECK(col_inv_pipe_smem_bytes(L1) + 1024 <= 228 * 1024, "colinvpipe L1=%d shared memory", L1);
+}
+
 void shoup_quot_check() {
     const u32 primes[] = {469762049u, 754974721u, 962592769u, 950009857u, 940572673u, 998244353u,
                           257u, 7681u, 12289u, 40961u, 1073479681u};
@@ -261,6 +284,8 @@ int main() {
     row_tab_check<14>();
     col_pipe_check<9>();
     col_pipe_check<10>();
+    col_inv_pipe_check<9>();
+    col_inv_pipe_check<10>();
     shoup_quot_check();
     std::printf("%s: %d failures\n", failures ? "FAILED" : "OK", failures);
     return failures ? 1 : 0;
