@@ -322,31 +322,34 @@ __global__ void __launch_bounds__(NW * 32, col_ctas(L1, KIND)) k_col_fwd(const _
 }
 
 // Pass A as a persistent, software-pipelined kernel for the two-level
-// column plans with 32-column tiles (n1 = 2^9, 2^10).  Each CTA walks the
-// tiles gridDim.x apart; while it transforms one tile, rows [0, n1/2) of its
-// next tile are already on their way into a staging buffer (cp.async,
-// zero-filled past the operand's end), so the SM does not wait for HBM
-// between tiles.  A product's operands are usually at most n/2 words long:
-// their rows [n1/2, n1) are zero and the first level skips that half.
-// Level 0 reads the stage and writes the tile; the last level reads the tile
-// and stores its outputs straight to HBM (each warp store is one 128-byte
-// row segment).  A longer operand also has rows [n1/2, n1) copied into the
-// tile before level 0, which then reads them there.  Sources that are not
-// 16-byte aligned are copied word by word.  Results are those of k_col_fwd
-// (same levels, same output layout).
-template <int L1, int NW>
+// column plans (n1 = 2^9, 2^10), on tiles of the layout `KIND` (0: 32
+// columns, one per lane; 2: 16 columns, one task per half-warp, padded rows).
+// Each CTA walks the tiles gridDim.x apart; while it transforms one tile,
+// rows [0, n1/2) of its next tile are already on their way into a staging
+// buffer (cp.async, zero-filled past the operand's end), so the SM does not
+// wait for HBM between tiles.  A product's operands are usually at most n/2
+// words long: their rows [n1/2, n1) are zero and the first level skips that
+// half.  Level 0 reads the stage and writes the tile; the last level reads
+// the tile and stores its outputs straight to HBM (each warp store covers
+// whole row segments).  A longer operand also has rows [n1/2, n1) copied
+// into the tile before level 0, which then reads them there.  Sources that
+// are not 16-byte aligned are copied word by word.  Results are those of
+// k_col_fwd (same levels, same output layout).
+template <int L1, int KIND, int NW>
 __global__ void __launch_bounds__(NW * 32, col_pipe_ctas(L1)) k_col_fwd_pipe(const __grid_constant__ LargeArgs A) {
     constexpr LevelPlan PL = col_plan(L1);
     static_assert(PL.nlev == 2, "two-level column plans only");
     constexpr int n1 = 1 << L1, HALF = n1 / 2, T = NW * 32;
     constexpr int R0 = 1 << PL.logr[0], R1 = 1 << PL.logr[1];  // n1 = R0 * R1; level-0 tasks: R1
+    constexpr int TC = col_tile_cols(L1, KIND), SUB = 32 / TC, QR = TC / 4;
     extern __shared__ __align__(16) u32 smem[];
-    u32* tile = smem;                                     // n1 rows x 32 words
-    u32* stage = smem + n1 * 32;                          // rows [0, HALF) x 32 words
-    Tw* tws = reinterpret_cast<Tw*>(stage + HALF * 32);   // level-0 twiddles (n1 entries)
-    const int n2 = 1 << A.l2, ct = n2 / 32;
+    u32* tile = smem;                                                   // n1 rows
+    u32* stage = smem + col_tile_words(L1, KIND);                       // rows [0, HALF)
+    Tw* tws = reinterpret_cast<Tw*>(stage + tile_row<L1, KIND>(HALF));  // level-0 twiddles (n1 entries)
+    const int n2 = 1 << A.l2, ct = n2 / TC;
     const int ntiles = ct * 2 * A.njobs;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int col = lane % TC;
     const u32 p = A.pkc.p, p2 = A.pkc.p2, oneq = A.pkc.one_q;
     for (int i = threadIdx.x; i < n1; i += T) tws[i] = A.twc[i];
 
@@ -357,29 +360,29 @@ __global__ void __launch_bounds__(NW * 32, col_pipe_ctas(L1)) k_col_fwd_pipe(con
         src = op ? J.b : J.a;
         len = op ? J.lb : J.la;
         dst = op ? J.wb : J.wa;
-        c0 = (t % ct) * 32;
+        c0 = (t % ct) * TC;
     };
-    // rows [r0, r1) x 32 columns of the operand into buf + r * 32 (one
-    // commit group); words at or past len read as 0
+    // rows [r0, r1) x TC columns of the operand into buf at the tile layout
+    // (one commit group); words at or past len read as 0
     auto rows_issue = [&](u32* buf, const u32* src, long long len, int c0, int r0, int r1) {
         if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
 #pragma unroll 4
-            for (int idx = r0 * 8 + threadIdx.x; idx < r1 * 8; idx += T) {
-                const int r = idx >> 3, q = idx & 7;
+            for (int idx = r0 * QR + threadIdx.x; idx < r1 * QR; idx += T) {
+                const int r = idx / QR, q = idx % QR;
                 const long long gi = (long long)r * n2 + c0 + 4 * q;
                 const long long rem = len - gi;
                 const int bytes = rem >= 4 ? 16 : (rem > 0 ? (int)rem * 4 : 0);
                 const u32* g = bytes ? src + gi : src;
-                const unsigned d = (unsigned)__cvta_generic_to_shared(buf + r * 32 + 4 * q);
+                const unsigned d = (unsigned)__cvta_generic_to_shared(buf + tile_row<L1, KIND>(r) + 4 * q);
                 asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(g), "r"(bytes) : "memory");
             }
         } else {
-            for (int idx = r0 * 32 + threadIdx.x; idx < r1 * 32; idx += T) {
-                const int r = idx >> 5, c = idx & 31;
+            for (int idx = r0 * TC + threadIdx.x; idx < r1 * TC; idx += T) {
+                const int r = idx / TC, c = idx % TC;
                 const long long gi = (long long)r * n2 + c0 + c;
                 const int bytes = gi < len ? 4 : 0;
                 const u32* g = bytes ? src + gi : src;
-                const unsigned d = (unsigned)__cvta_generic_to_shared(buf + r * 32 + c);
+                const unsigned d = (unsigned)__cvta_generic_to_shared(buf + tile_row<L1, KIND>(r) + c);
                 asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(g), "r"(bytes) : "memory");
             }
         }
@@ -407,26 +410,27 @@ __global__ void __launch_bounds__(NW * 32, col_pipe_ctas(L1)) k_col_fwd_pipe(con
             }
         }
 
-        // level 0: task o (rows o + R1 m), lane = column
-        for (int o = warp; o < R1; o += NW) {
+        // level 0: task o (rows o + R1 m)
+        for (int o = warp * SUB + lane / TC; o < R1; o += NW * SUB) {
             u32 x[R0];
+            const int off = tile_row<L1, KIND>(o) + col;
 #pragma unroll
-            for (int m = 0; m < R0 / 2; ++m) x[m] = stage[(o + R1 * m) * 32 + lane];
+            for (int m = 0; m < R0 / 2; ++m) x[m] = stage[off + tile_step<L1, KIND, R1>(m)];
             if (!full) {
                 dif_regs_halfzero<R0, true>(x, A.pkc.rc.f, p, p2, oneq);
             } else {
 #pragma unroll
                 for (int m = 0; m < R0; ++m)
-                    x[m] = mul_shoup(m < R0 / 2 ? x[m] : tile[(o + R1 * m) * 32 + lane], 1u, oneq, p);
+                    x[m] = mul_shoup(m < R0 / 2 ? x[m] : tile[off + tile_step<L1, KIND, R1>(m)], 1u, oneq, p);
                 dif_regs<R0, true>(x, A.pkc.rc.f, p, p2);
             }
 #pragma unroll
             for (int j = 1; j < R0; ++j) {
-                const Tw w = tws[o * R0 + j];  // broadcast
+                const Tw w = tws[o * R0 + j];  // broadcast to the (half-)warp
                 x[j] = mul_shoup(x[j], w.w, w.wq, p);
             }
 #pragma unroll
-            for (int m = 0; m < R0; ++m) tile[(o + R1 * m) * 32 + lane] = x[m];
+            for (int m = 0; m < R0; ++m) tile[off + tile_step<L1, KIND, R1>(m)] = x[m];
         }
         __syncthreads();  // tile complete; the stage is free
 
@@ -439,12 +443,13 @@ __global__ void __launch_bounds__(NW * 32, col_pipe_ctas(L1)) k_col_fwd_pipe(con
         // level 1 (last): block blk = rows blk * R1 + m, straight to HBM
         const u32* src; long long len; u32* dst; int c0;
         decode(t, src, len, dst, c0);
-        for (int blk = warp; blk < R0; blk += NW) {
+        for (int blk = warp * SUB + lane / TC; blk < R0; blk += NW * SUB) {
             u32 x[R1];
+            const int off = tile_row<L1, KIND>(blk * R1) + col;
 #pragma unroll
-            for (int m = 0; m < R1; ++m) x[m] = tile[(blk * R1 + m) * 32 + lane];
+            for (int m = 0; m < R1; ++m) x[m] = tile[off + tile_step<L1, KIND, 1>(m)];
             dif_regs<R1>(x, A.pkc.rc.f, p, p2);
-            u32* out = dst + (size_t)(blk * R1) * n2 + c0 + lane;
+            u32* out = dst + (size_t)(blk * R1) * n2 + c0 + col;
 #pragma unroll
             for (int m = 0; m < R1; ++m) out[(size_t)m * n2] = x[m];
         }

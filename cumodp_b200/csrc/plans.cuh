@@ -98,22 +98,31 @@ __host__ __device__ constexpr int col_smem_bytes(int logl, int kind) {
     return col_tile_words(logl, kind) * 4 + (col_tw_smem(logl, kind) ? col_tw_entries(logl) * 8 : 0);
 }
 
-// Persistent pass A (k_col_fwd_pipe) for the two-level column plans with
-// 32-column tiles: one CTA per SM of 512 threads with up to 128 registers
-// each (a warp holds two level tasks at once; 1024 threads at 64 registers
-// spill, and for n1 = 2^9 two 512-thread CTAs per SM measured slower).
-// Shared memory: the tile, a stage of its first n1/2 rows and the level-0
-// twiddles.
+// Persistent pass A (k_col_fwd_pipe) for the two-level column plans, up to
+// 128 registers a thread (1024 threads at 64 registers spill): 2^10-row
+// columns in 16-column tiles (the layout of kind 2), two 256-thread CTAs per
+// SM, whose barriers and phases then overlap (measured 8 % faster than one
+// 512-thread CTA on 32-column tiles); 2^9-row columns in 32-column tiles,
+// one 512-thread CTA per SM (two per SM measured slower).  Shared memory:
+// the tile, a stage of its first n1/2 rows and the level-0 twiddles.
 __host__ __device__ constexpr bool col_pipe_ok(int logl) { return logl == 9 || logl == 10; }
-__host__ __device__ constexpr int col_pipe_warps(int logl) { return 16; }
-__host__ __device__ constexpr int col_pipe_ctas(int logl) { return 1; }
+__host__ __device__ constexpr int col_pipe_kind(int logl) { return logl == 10 ? 2 : 0; }  // tile layout (col_tile_cols)
+__host__ __device__ constexpr int col_pipe_warps(int logl) { return logl == 10 ? 8 : 16; }
+__host__ __device__ constexpr int col_pipe_ctas(int logl) { return logl == 10 ? 2 : 1; }
 __host__ __device__ constexpr int col_pipe_smem_bytes(int logl) {
-    return (32 << logl) * 4 + (16 << logl) * 4 + (1 << logl) * 8;
+    // tile, stage (the tile layout's first n1/2 rows), level-0 twiddles
+    return col_tile_words(logl, col_pipe_kind(logl)) * 4 +
+           (col_tile_cols(logl, col_pipe_kind(logl)) == 32
+                ? (16 << logl)
+                : ((1 << logl) / 2 + ((1 << logl) / 2 >> col_pad_log(logl))) * col_tile_cols(logl, col_pipe_kind(logl))) * 4 +
+           (1 << logl) * 8;
 }
 
 // Persistent pass C (k_col_inv_pipe) for the same column lengths: one
 // 512-thread CTA per SM holding the tile, a stage for the whole next tile
-// and the level-0 twiddles.
+// and the level-0 twiddles (two 256-thread CTAs per SM with a half-tile
+// stage measured 9 % slower: the unstaged half's load is exposed).
+__host__ __device__ constexpr int col_inv_pipe_warps(int logl) { return 16; }
 __host__ __device__ constexpr int col_inv_pipe_smem_bytes(int logl) {
     return 2 * col_tile_words(logl, 1) * 4 + (1 << logl) * 8;
 }

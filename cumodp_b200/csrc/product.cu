@@ -86,13 +86,13 @@ template <int L1>
 void launch_col_fwd_pipe_t(const LargeArgs& a, int ntiles, cudaStream_t st) {
     constexpr int smem = col_pipe_smem_bytes(L1);
     const int grid = std::min(ntiles, sm_count(current_device()) * col_pipe_ctas(L1));
-    k_col_fwd_pipe<L1, col_pipe_warps(L1)><<<grid, col_pipe_warps(L1) * 32, smem, st>>>(a);
+    k_col_fwd_pipe<L1, col_pipe_kind(L1), col_pipe_warps(L1)><<<grid, col_pipe_warps(L1) * 32, smem, st>>>(a);
 }
 
 template <int L1>
 void launch_col_inv_pipe_t(const LargeArgs& a, int ntiles, cudaStream_t st) {
     const int grid = std::min(ntiles, sm_count(current_device()));
-    launch_pdl(k_col_inv_pipe<L1, col_pipe_warps(L1)>, dim3(grid), col_pipe_warps(L1) * 32,
+    launch_pdl(k_col_inv_pipe<L1, col_inv_pipe_warps(L1)>, dim3(grid), col_inv_pipe_warps(L1) * 32,
                (size_t)col_inv_pipe_smem_bytes(L1), st, a);
 }
 
@@ -220,9 +220,9 @@ void attr_col() {
 }
 template <int L1>
 void attr_col_pipe() {
-    cudaFuncSetAttribute(k_col_fwd_pipe<L1, col_pipe_warps(L1)>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_col_fwd_pipe<L1, col_pipe_kind(L1), col_pipe_warps(L1)>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          col_pipe_smem_bytes(L1));
-    cudaFuncSetAttribute(k_col_inv_pipe<L1, col_pipe_warps(L1)>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_col_inv_pipe<L1, col_inv_pipe_warps(L1)>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          col_inv_pipe_smem_bytes(L1));
 }
 template <int L2>
@@ -363,7 +363,7 @@ void launch_large(const LargeArgs& a, int njobs, cudaStream_t st) {
     cudaEvent_t e0;
     bool tr = pass_timing_begin(st, &e0);
     if (col_pipe_ok(a.l1) && col_pipe_enabled()) {
-        const int ntiles = (n2 / 32) * 2 * njobs;
+        const int ntiles = (n2 / col_tile_cols_rt(a.l1, col_pipe_kind(a.l1))) * 2 * njobs;
         if (a.l1 == 10) launch_col_fwd_pipe_t<10>(a, ntiles, st);
         else launch_col_fwd_pipe_t<9>(a, ntiles, st);
     } else {

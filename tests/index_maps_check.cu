@@ -198,23 +198,35 @@ void row_tab_check() {
     CHECK((smem + 1024) * rowsplit_ctas(L2) <= 228 * 1024, "rowsplit L2=%d shared memory", L2);
 }
 
-template <int L1>
+template <int L1, int KIND>
 void col_pipe_check() {
     constexpr LevelPlan PL = col_plan(L1);
     constexpr int n1 = 1 << L1, HALF = n1 / 2, R0 = 1 << PL.logr[0], R1 = 1 << PL.logr[1];
+    constexpr int TC = col_tile_cols(L1, KIND), QR = TC / 4;
+    constexpr int TW = col_tile_words(L1, KIND);
+    const int SW = tile_row<L1, KIND>(HALF);
     CHECK(PL.nlev == 2 && R0 * R1 == n1, "colpipe L1=%d plan", L1);
+    // stage copies of rows [0, HALF) and tile copies of rows [HALF, n1)
+    for (int idx = 0; idx < n1 * QR; ++idx) {
+        const int r = idx / QR, q = idx % QR;
+        const int a = tile_row<L1, KIND>(r) + 4 * q;
+        CHECK((a % 4 == 0 && a + 3 < (r < HALF ? SW : TW)), "colpipe L1=%d kind=%d copy", L1, KIND);
+    }
     for (int o = 0; o < R1; ++o)
         for (int m = 0; m < R0; ++m) {
             const int row = o + R1 * m;
-            CHECK(row < n1, "colpipe L1=%d level-0 row", L1);
-            if (m < R0 / 2) CHECK(row < HALF, "colpipe L1=%d stage row", L1);
+            CHECK((tile_row<L1, KIND>(o) + tile_step<L1, KIND, R1>(m) == tile_row<L1, KIND>(row)), "colpipe L1=%d level-0 step", L1);
+            if (m < R0 / 2) CHECK((row < HALF && tile_row<L1, KIND>(row) + TC <= SW), "colpipe L1=%d stage row", L1);
             else CHECK(row >= HALF, "colpipe L1=%d upper row", L1);
             CHECK(o * R0 + m < col_tw_entries(L1), "colpipe L1=%d twiddle", L1);
         }
     for (int blk = 0; blk < R0; ++blk)
-        for (int m = 0; m < R1; ++m) CHECK(blk * R1 + m < n1, "colpipe L1=%d level-1 row", L1);
-    CHECK(col_pipe_smem_bytes(L1) == n1 * 128 + HALF * 128 + col_tw_entries(L1) * 8, "colpipe L1=%d layout", L1);
-    CHECK((col_pipe_smem_bytes(L1) + 1024) * col_pipe_ctas(L1) <= 228 * 1024, "colpipe L1=%d shared memory", L1);
+        for (int m = 0; m < R1; ++m)
+            CHECK((tile_row<L1, KIND>(blk * R1) + tile_step<L1, KIND, 1>(m) == tile_row<L1, KIND>(blk * R1 + m)), "colpipe L1=%d level-1 step", L1);
+    if (KIND == col_pipe_kind(L1)) {
+        CHECK(col_pipe_smem_bytes(L1) == TW * 4 + SW * 4 + col_tw_entries(L1) * 8, "colpipe L1=%d layout", L1);
+        CHECK((col_pipe_smem_bytes(L1) + 1024) * col_pipe_ctas(L1) <= 228 * 1024, "colpipe L1=%d shared memory", L1);
+    }
 }
 
 template <int L1>
@@ -282,8 +294,9 @@ int main() {
     row_tab_check<12>();
     row_tab_check<13>();
     row_tab_check<14>();
-    col_pipe_check<9>();
-    col_pipe_check<10>();
+    col_pipe_check<9, 0>();
+    col_pipe_check<10, 0>();
+    col_pipe_check<10, 2>();
     col_inv_pipe_check<9>();
     col_inv_pipe_check<10>();
     shoup_quot_check();
