@@ -33,6 +33,7 @@ struct RowNttArgs {
     u32* dst;                       // natural row k1 at dst + k1 * n2
     Tw scale;                       // applied to every output
     int rows_in_place;              // 1: independent rows, row s written to dst row s
+    const Tw* __restrict__ rowtab;  // per-slot level-0 factor tables (RowTab, forward direction), or nullptr
 };
 
 __device__ __forceinline__ u32 seed_mont_at(const u32* __restrict__ seeds, int nlo, u32 e, u32 p, u32 pinv) {
@@ -46,7 +47,10 @@ __device__ __forceinline__ u32 seed_mont_at(const u32* __restrict__ seeds, int n
 // the input), the remaining levels run as in the product kernels, and the
 // last level leaves each thread one 32-word group in registers; after a
 // barrier the groups are written back at their natural positions in the same
-// buffer, and the row is stored with 16-byte accesses.
+// buffer, and the row is stored with 16-byte accesses.  With the prebuilt
+// per-slot factor tables (rows of 2^11-2^14 words) level 0 is that of the
+// product's row kernels: inputs times W^(TB0 m), DIF, outputs times the two
+// shared-memory factors of U_j^o.
 template <int L2>
 __global__ void __launch_bounds__(ntt_row_threads(L2), ntt_row_ctas(L2)) k_row_ntt(const __grid_constant__ RowNttArgs A) {
     constexpr int n2 = 1 << L2;
@@ -65,15 +69,50 @@ __global__ void __launch_bounds__(ntt_row_threads(L2), ntt_row_ctas(L2)) k_row_n
     const bool twid = A.seeds != nullptr;
     const u32 nmask = (1u << (A.l1 + L2)) - 1;
     const u32 p = A.pk.p, p2 = A.pk.p2, pinv = A.pk.pinv_neg;
-    if (twid && threadIdx.x < R0) {
+    using RT = RowTab<L2>;
+    const bool tabbed = RT::USE && twid && A.rowtab;
+    Tw* tab = reinterpret_cast<Tw*>(sm + n2);
+    row_load_issue<L2, T>(sm, A.src + (size_t)s * n2);
+    if (tabbed) {
+        const Tw* src = A.rowtab + (size_t)s * RT::TABW;  // forward direction
+        for (int i = threadIdx.x; i < RT::TABW / 2; i += T) {
+            const unsigned d = (unsigned)__cvta_generic_to_shared(tab + 2 * i);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + 2 * i) : "memory");
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    } else if (twid && threadIdx.x < R0) {
         const u32 e = (k1 * (u32)TB0 * threadIdx.x) & nmask;
         const u32 v = red1(mul_mont(seed_mont_at(A.seeds, A.nlo, e, p, pinv), 1u, p, pinv), p);
         bf[threadIdx.x] = Tw{v, (u32)(((u64)v << 32) / p)};
     }
-    row_load<L2, T>(sm, A.src + (size_t)s * n2);
+    row_load_wait();
     __syncthreads();
 
-    for (int o = threadIdx.x; o < TB0; o += T) {
+    if constexpr (RT::USE) {
+        if (tabbed) {
+            const Tw* vf = tab + RT::ENTRIES;
+            for (int o = threadIdx.x; o < TB0; o += T) {
+                u32 x[R0];
+                const int bs = swz(o);
+#pragma unroll
+                for (int m = 0; m < R0; ++m) {
+                    const u32 v = sm[swz_task<TB0, n2>(o, bs, m)];
+                    x[m] = m == 0 ? v : mul_shoup(v, vf[m].w, vf[m].wq, p);
+                }
+                dif_regs<R0, true>(x, A.pk.rc.f, p, p2);
+                const Tw* ta = tab + (o % RT::NA);
+                const Tw* tb = tab + RT::R0 * RT::NA + o / RT::NA;
+#pragma unroll
+                for (int j = 0; j < R0; ++j) {
+                    const Tw a = ta[j * RT::NA], b = tb[j * RT::NB];
+                    x[j] = mul_shoup(mul_shoup(x[j], a.w, a.wq, p), b.w, b.wq, p);
+                }
+#pragma unroll
+                for (int m = 0; m < R0; ++m) sm[swz_task<TB0, n2>(o, bs, m)] = x[m];
+            }
+        }
+    }
+    for (int o = threadIdx.x; o < (tabbed ? 0 : TB0); o += T) {
         u32 x[R0];
         const u32 mo = twid ? seed_mont_at(A.seeds, A.nlo, (k1 * (u32)o) & nmask, p, pinv) : 0u;
         const int bs = swz(o);
@@ -174,7 +213,7 @@ namespace {
 
 template <int L2>
 void launch_row_ntt_t(const RowNttArgs& a, int rows, cudaStream_t st) {
-    const size_t smem = (size_t)(1 << L2) * sizeof(u32);
+    const size_t smem = (size_t)(1 << L2) * sizeof(u32) + (size_t)RowTab<L2>::TABW * sizeof(Tw);
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_row_ntt<L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -232,6 +271,8 @@ int column_pass(const PrimeCtx& pc, u32 root_c, int l1, int l2, const u32* src, 
     A.colpl = col_plan(l1);
     A.job0 = LargeJob{src, nullptr, nullptr, (int)std::min<long long>(len, 1ll << 30), 0, 0, 0, dst, nullptr};
     A.njobs = 1;
+    // (the pipelined pass-A kernel measured slower here: a full-length input
+    // has no zero half, so half of every tile's load is exposed)
     kColFwd1[l1](A, (1 << l2) / col_tile_cols_rt(l1, 2), st);
     return OK;
 }
@@ -296,6 +337,10 @@ int ntt_natural_dev(const u32* x_in, u32* x_out, int k, u32 w, u32 p, bool inver
     A.src = w1;
     A.dst = w2;
     A.scale = tw_of(sc, p);
+    {
+        LargeArgs LA;  // the level-0 factor tables of this root and shape (built once, cached)
+        if (large_args(*pc, root, k, l2, dev, &LA) == OK) A.rowtab = LA.rowtab;
+    }
     tr = pass_timing_begin(st, &e0);
     kRowNtt[l2](A, 1 << l1, st);
     if (tr) pass_timing_end(st, "ntt_row", e0);

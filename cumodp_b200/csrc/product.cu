@@ -357,18 +357,20 @@ void launch_small(int logn, const SmallArgs& a, int njobs, cudaStream_t st) {
     if (tr) pass_timing_end(st, kSmallName[logn], e0);
 }
 
+bool launch_col_fwd_pipe(const LargeArgs& a, int njobs, cudaStream_t st) {
+    if (!col_pipe_ok(a.l1) || !col_pipe_enabled()) return false;
+    const int ntiles = ((1 << a.l2) / col_tile_cols_rt(a.l1, col_pipe_kind(a.l1))) * 2 * njobs;
+    if (a.l1 == 10) launch_col_fwd_pipe_t<10>(a, ntiles, st);
+    else launch_col_fwd_pipe_t<9>(a, ntiles, st);
+    return true;
+}
+
 void launch_large(const LargeArgs& a, int njobs, cudaStream_t st) {
     const int n1 = 1 << a.l1, n2 = 1 << a.l2;
     NvtxRange range(kRowFName[a.l2]);  // the product's three passes, named by its dominant kernel
     cudaEvent_t e0;
     bool tr = pass_timing_begin(st, &e0);
-    if (col_pipe_ok(a.l1) && col_pipe_enabled()) {
-        const int ntiles = (n2 / col_tile_cols_rt(a.l1, col_pipe_kind(a.l1))) * 2 * njobs;
-        if (a.l1 == 10) launch_col_fwd_pipe_t<10>(a, ntiles, st);
-        else launch_col_fwd_pipe_t<9>(a, ntiles, st);
-    } else {
-        kColFwd[a.l1](a, dim3(n2 / col_tile_cols_rt(a.l1, false), 2, njobs), st);
-    }
+    if (!launch_col_fwd_pipe(a, njobs, st)) kColFwd[a.l1](a, dim3(n2 / col_tile_cols_rt(a.l1, false), 2, njobs), st);
     if (tr) pass_timing_end(st, kColFwdName[a.l1], e0);
     if (a.row_fused) {
         tr = pass_timing_begin(st, &e0);

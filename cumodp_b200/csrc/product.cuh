@@ -24,6 +24,9 @@ int default_row_log(int logn);
 
 int small_args(const PrimeCtx& pc, u32 root, int logn, int dev, SmallArgs* a);
 int large_args(const PrimeCtx& pc, u32 root_n, int logn, int l2, int dev, LargeArgs* a);
+// A product's pass A through the persistent pipelined kernel when the column
+// length has one (2^9, 2^10 rows); false when the caller must launch k_col_fwd.
+bool launch_col_fwd_pipe(const LargeArgs& a, int njobs, cudaStream_t st);
 void launch_small(int logn, const SmallArgs& a, int njobs, cudaStream_t st);
 void launch_large(const LargeArgs& a, int njobs, cudaStream_t st);
 

@@ -195,6 +195,9 @@ void row_tab_check() {
     // shared memory of the split row kernels (+1 KiB reserved per CTA)
     const long long smem = (long long)(1 << L2) * 4 + (long long)RT::TABW * 8 + (long long)RT::NPOW * 4 + 2 * RT::R0 * 8;
     CHECK((RT::TABW * 8) % 16 == 0, "rowtab L2=%d table not a whole number of 16-byte copies", L2);
+    // the natural-order row kernel holds the row and the forward table
+    CHECK(((long long)(1 << L2) * 4 + (long long)RT::TABW * 8 + RT::R0 * 8 + 1024) * ntt_row_ctas(L2) <= 228 * 1024,
+          "ntt row L2=%d shared memory", L2);
     CHECK((smem + 1024) * rowsplit_ctas(L2) <= 228 * 1024, "rowsplit L2=%d shared memory", L2);
 }
 
