@@ -366,10 +366,14 @@ __global__ void __launch_bounds__(NW * 32, col_pipe_ctas(L1)) k_col_fwd_pipe(con
     // (one commit group); words at or past len read as 0
     auto rows_issue = [&](u32* buf, const u32* src, long long len, int c0, int r0, int r1) {
         if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+            // a thread keeps one quad column q and walks rows T / QR apart
+            // (running index: 64-bit adds, no multiply per copy)
+            static_assert(T % QR == 0, "whole rows per thread round");
+            const int q = threadIdx.x % QR;
+            const long long step = (long long)(T / QR) * n2;
+            long long gi = (long long)(r0 + threadIdx.x / QR) * n2 + c0 + 4 * q;
 #pragma unroll 4
-            for (int idx = r0 * QR + threadIdx.x; idx < r1 * QR; idx += T) {
-                const int r = idx / QR, q = idx % QR;
-                const long long gi = (long long)r * n2 + c0 + 4 * q;
+            for (int r = r0 + threadIdx.x / QR; r < r1; r += T / QR, gi += step) {
                 const long long rem = len - gi;
                 const int bytes = rem >= 4 ? 16 : (rem > 0 ? (int)rem * 4 : 0);
                 const u32* g = bytes ? src + gi : src;
@@ -449,9 +453,10 @@ __global__ void __launch_bounds__(NW * 32, col_pipe_ctas(L1)) k_col_fwd_pipe(con
 #pragma unroll
             for (int m = 0; m < R1; ++m) x[m] = tile[off + tile_step<L1, KIND, 1>(m)];
             dif_regs<R1>(x, A.pkc.rc.f, p, p2);
+            // running pointer: 64-bit adds on the ALU pipe, not a multiply per store
             u32* out = dst + (size_t)(blk * R1) * n2 + c0 + col;
 #pragma unroll
-            for (int m = 0; m < R1; ++m) out[(size_t)m * n2] = x[m];
+            for (int m = 0; m < R1; ++m, out += n2) *out = x[m];
         }
     }
 }
@@ -485,13 +490,15 @@ __global__ void __launch_bounds__(NW * 32, 1) k_col_inv_pipe(const __grid_consta
     // the whole tile t (all n1 rows of the row pass's output) into the stage
     auto stage_issue = [&](int t) {
         const LargeJob& J = A.jobs ? A.jobs[t / ct] : A.job0;
-        const u32* src = J.wa + (t % ct) * TC;
+        // a thread keeps one quad column q and walks rows T / QR apart
+        static_assert(T % QR == 0, "whole rows per thread round");
+        const int q = threadIdx.x % QR;
+        const u32* src = J.wa + (t % ct) * TC + (size_t)(threadIdx.x / QR) * n2 + 4 * q;
+        const size_t step = (size_t)(T / QR) * n2;
 #pragma unroll 4
-        for (int idx = threadIdx.x; idx < n1 * QR; idx += T) {
-            const int r = idx / QR, q = idx % QR;
+        for (int r = threadIdx.x / QR; r < n1; r += T / QR, src += step) {
             const unsigned d = (unsigned)__cvta_generic_to_shared(stage + tile_row<L1, INV>(r) + 4 * q);
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + (size_t)r * n2 + 4 * q)
-                         : "memory");
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     };
@@ -531,11 +538,13 @@ __global__ void __launch_bounds__(NW * 32, 1) k_col_inv_pipe(const __grid_consta
                 x[j] = mul_shoup(x[j], w.w, w.wq, p);
             }
             dit_regs<R0, true>(x, A.pkc.rc.i, p, p2);
+            // running index and pointer (64-bit adds on the ALU pipe)
+            long long gi = (long long)o * n2 + c0 + col;
+            u32* out = J.h + gi;
+            const long long step = (long long)R1 * n2;
 #pragma unroll
-            for (int m = 0; m < R0; ++m) {
-                const long long gi = (long long)(o + R1 * m) * n2 + c0 + col;
-                if (gi < lh) J.h[gi] = red1(red2(x[m], p2), p);
-            }
+            for (int m = 0; m < R0; ++m, gi += step, out += step)
+                if (gi < lh) *out = red1(red2(x[m], p2), p);
         }
     }
 }
