@@ -165,6 +165,37 @@ def product_check(a, b, h) -> bool:
     return eval_mod(h, pw) == eval_mod(a, pw[:len(a)]) * eval_mod(b, pw[:len(b)]) % P
 
 
+def host_link_bound(torch, dev, h2d_bytes: int, d2h_bytes: int, reps: int = 5) -> dict:
+    """The host link's ceiling for a step that moves h2d_bytes in and d2h_bytes
+    out: one step's copies, both directions at once from pinned buffers on two
+    streams, timed with CUDA events (best of reps); e2e can at most reach
+    1 / that time per GPU."""
+    hi = torch.empty(h2d_bytes // 4, dtype=torch.int32).pin_memory()
+    ho = torch.empty(d2h_bytes // 4, dtype=torch.int32).pin_memory()
+    di = torch.empty(h2d_bytes // 4, dtype=torch.int32, device=dev)
+    do = torch.empty(d2h_bytes // 4, dtype=torch.int32, device=dev)
+    s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    best = None
+    for _ in range(reps + 1):
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s_in)
+        s_out.wait_event(e0)
+        with torch.cuda.stream(s_in):
+            di.copy_(hi, non_blocking=True)
+        with torch.cuda.stream(s_out):
+            ho.copy_(do, non_blocking=True)
+        e1.record(s_in)
+        e2.record(s_out)
+        torch.cuda.synchronize(dev)
+        ms = max(e0.elapsed_time(e1), e0.elapsed_time(e2))
+        best = ms if best is None else min(best, ms)
+    return {"ms_per_step_copies": round(best, 4), "bound_per_s": round(1000.0 / best, 1),
+            "gbs_per_direction": round(max(h2d_bytes, d2h_bytes) / (best / 1000.0) / 1e9, 1),
+            "how": "one step's H2D and D2H copies at once (pinned, two streams), CUDA events, best of %d" % reps}
+
+
 def host_threads() -> int:
     try:
         return len(os.sched_getaffinity(0))
@@ -375,7 +406,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
            "d2h_bytes_per_step": (n - 1) * 4, "steps": e2e_steps, "eval_point_identity": e2e_ok,
            "api": "cumodp_fftmul_batch (host arrays, pinned)",
            "single_call": {"value": replica_throughput(world, e2e_steps, single_s), "api": "cumodp_fftmul_uni",
-                           "eval_point_identity": single_ok}}
+                           "eval_point_identity": single_ok},
+           "host_link": host_link_bound(torch, dev, 2 * (DEG + 1) * 4, (n - 1) * 4)}
 
     extras = {}
     if rank == 0 and not args.no_extras:
