@@ -80,3 +80,36 @@ def test_large_host_batch_is_pipelined_and_exact(cm, oracle_mod):
     for (a, b), h in zip(pairs, outs):
         assert np.array_equal(h, cm.fftmul_uni(a, b, P0))
     assert np.array_equal(outs[1], oracle_mod.polymul(pairs[1][0], pairs[1][1], P0))
+
+
+def test_device_batch_of_large_classes(cm):
+    """Device-resident batch with several products per large size class
+    (2^20-2^22 transforms: one launch of each pass kernel per class covers
+    every job, including operands longer than half the transform and
+    operands starting off a 16-byte boundary); each product equals its
+    single call."""
+    import torch
+    r = SplitMix64(0xC0DA0502)
+    degs = [(2**19 - 1, 2**19 - 1), (2**19 - 1, 2**19 - 1), (600000, 100), (100, 600000), (2**19 - 1, 3),
+            (2**20 - 1, 2**20 - 1), (2**20 - 1, 2**20 - 2), (2**21 - 1, 2**21 - 1), (2**21 - 1, 2**21 - 7)]
+    df = np.array([a for a, _ in degs], np.int32)
+    dg = np.array([b for _, b in degs], np.int32)
+    # odd gaps between operands: most of them start off a 16-byte boundary
+    f_off = np.zeros(len(degs), np.int64)
+    g_off = np.zeros(len(degs), np.int64)
+    h_off = np.zeros(len(degs), np.int64)
+    f_off[1:] = np.cumsum(df.astype(np.int64) + 2)[:-1]
+    g_off[1:] = np.cumsum(dg.astype(np.int64) + 3)[:-1]
+    h_off[1:] = np.cumsum(df.astype(np.int64) + dg + 1)[:-1]
+    F = r.residues(int(f_off[-1] + df[-1] + 1), P0)
+    G = r.residues(int(g_off[-1] + dg[-1] + 1), P0)
+    tF = torch.from_numpy(F.view(np.int32)).cuda()
+    tG = torch.from_numpy(G.view(np.int32)).cuda()
+    tH = torch.zeros(int(h_off[-1] + df[-1] + dg[-1] + 1), dtype=torch.int32, device="cuda")
+    cm.fftmul_batch_dev(df, f_off, tF.data_ptr(), dg, g_off, tG.data_ptr(), h_off, tH.data_ptr(), P0)
+    torch.cuda.synchronize()
+    H = tH.cpu().numpy().view(np.uint32)
+    for i, (a, b) in enumerate(degs):
+        fa = F[f_off[i]:f_off[i] + a + 1]
+        gb = G[g_off[i]:g_off[i] + b + 1]
+        assert np.array_equal(H[h_off[i]:h_off[i] + a + b + 1], cm.fftmul_uni(fa, gb, P0)), i
