@@ -696,7 +696,8 @@ __global__ void __launch_bounds__(row_threads(L2), 1) k_row_fused(const __grid_c
 // The row pass as two kernels of one operand each, so a CTA needs half the
 // shared memory (one 2^14-word row = 64 KiB) and two CTAs share an SM:
 //   k_row_fwd_g   row DFT of G' (inter-pass twiddle, all forward levels),
-//                 result written over G' in digit-reversed row order;
+//                 result written over G' in digit-reversed row order, its
+//                 32-word groups quad-interleaved (coalesced both ways);
 //   k_row_mul_f   row DFT of F', pointwise product with that row of G^
 //                 read from global memory in the same order, inverse row
 //                 DFT, inverse twiddle with 2^64/n, result over F'.
@@ -953,10 +954,13 @@ __global__ void __launch_bounds__(rowsplit_threads(L2), rowsplit_ctas(L2)) k_row
         u32 x[32];
         load_row32(x, sm, r * 32);
         dif_regs<32>(x, A.pk.rc.f, p, p2);
-        // store this 32-word row of the spectrum straight to global memory
+        // store this 32-word group of the spectrum straight to global memory,
+        // quad-interleaved (quad c of group r at c * n2/8 + 4 r): the lanes of
+        // a warp write one contiguous 512-byte run per store, and k_row_mul_f
+        // reads it back the same way
 #pragma unroll
         for (int c = 0; c < 8; ++c)
-            *reinterpret_cast<uint4*>(row + r * 32 + 4 * c) =
+            *reinterpret_cast<uint4*>(row + c * (n2 / 8) + 4 * r) =
                 make_uint4(x[4 * c], x[4 * c + 1], x[4 * c + 2], x[4 * c + 3]);
     }
 }
@@ -1004,7 +1008,7 @@ __global__ void __launch_bounds__(rowsplit_threads(L2), rowsplit_ctas(L2)) k_row
         dif_regs<32>(x, A.pk.rc.f, p, p2);
 #pragma unroll
         for (int c = 0; c < 8; ++c) {
-            const uint4 g = __ldg(reinterpret_cast<const uint4*>(rowG + r * 32 + 4 * c));
+            const uint4 g = __ldg(reinterpret_cast<const uint4*>(rowG + c * (n2 / 8) + 4 * r));  // quad-interleaved
             x[4 * c] = mul_mont(x[4 * c], g.x, p, pinv);
             x[4 * c + 1] = mul_mont(x[4 * c + 1], g.y, p, pinv);
             x[4 * c + 2] = mul_mont(x[4 * c + 2], g.z, p, pinv);
