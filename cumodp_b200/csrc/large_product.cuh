@@ -900,22 +900,29 @@ template <int L2, int T>
 __device__ __forceinline__ void row_level0_fwd(u32* sm, const LargeArgs& A, const Tw* tab) {
     using RT = RowTab<L2>;
     constexpr int R0 = RT::R0, TB0 = RT::TB0;
+    static_assert(T % RT::NA == 0, "the tasks of a thread share o mod NA");
     const u32 p = A.pk.p, p2 = A.pk.p2;
-    const Tw* bf = tab + RT::ENTRIES;
+    // the slot factors and this thread's U_j^(o mod NA) are the same for all
+    // of its tasks: kept in registers
+    Tw vf[R0], af[R0];
+#pragma unroll
+    for (int j = 0; j < R0; ++j) {
+        vf[j] = tab[RT::ENTRIES + j];
+        af[j] = tab[j * RT::NA + threadIdx.x % RT::NA];
+    }
     for (int o = threadIdx.x; o < TB0; o += T) {
         u32 x[R0];
 #pragma unroll
         for (int m = 0; m < R0; ++m) {
             const u32 v = sm[swz_task<TB0, (1 << L2)>(o, swz(o), m)];
-            x[m] = m == 0 ? v : mul_shoup(v, bf[m].w, bf[m].wq, p);
+            x[m] = m == 0 ? v : mul_shoup(v, vf[m].w, vf[m].wq, p);
         }
         dif_regs<R0, true>(x, A.pk.rc.f, p, p2);
-        const Tw* ta = tab + (o % RT::NA);
         const Tw* tb = tab + RT::R0 * RT::NA + o / RT::NA;
 #pragma unroll
         for (int j = 0; j < R0; ++j) {
-            const Tw a = ta[j * RT::NA], b = tb[j * RT::NB];
-            x[j] = mul_shoup(mul_shoup(x[j], a.w, a.wq, p), b.w, b.wq, p);
+            const Tw b = tb[j * RT::NB];
+            x[j] = mul_shoup(mul_shoup(x[j], af[j].w, af[j].wq, p), b.w, b.wq, p);
         }
 #pragma unroll
         for (int m = 0; m < R0; ++m) sm[swz_task<TB0, (1 << L2)>(o, swz(o), m)] = x[m];
@@ -1024,14 +1031,16 @@ __global__ void __launch_bounds__(rowsplit_threads(L2), rowsplit_ctas(L2)) k_row
     using RT = RowTab<L2>;
     if constexpr (RT::USE) {
         const Tw* bo = tab + RT::ENTRIES;
+        Tw af[R0];  // this thread's U_j^-(o mod NA), the same for all of its tasks
+#pragma unroll
+        for (int j = 0; j < R0; ++j) af[j] = tab[j * RT::NA + threadIdx.x % RT::NA];
         for (int o = threadIdx.x; o < TB0; o += T) {
             u32 x[R0];
-            const Tw* ta = tab + (o % RT::NA);
             const Tw* tb = tab + RT::R0 * RT::NA + o / RT::NA;
 #pragma unroll
             for (int j = 0; j < R0; ++j) {
-                const Tw a = ta[j * RT::NA], b = tb[j * RT::NB];
-                x[j] = mul_shoup(mul_shoup(sm[swz_task<TB0, n2>(o, swz(o), j)], a.w, a.wq, p), b.w, b.wq, p);
+                const Tw b = tb[j * RT::NB];
+                x[j] = mul_shoup(mul_shoup(sm[swz_task<TB0, n2>(o, swz(o), j)], af[j].w, af[j].wq, p), b.w, b.wq, p);
             }
             dit_regs<R0, true>(x, A.pk.rc.i, p, p2);
 #pragma unroll
