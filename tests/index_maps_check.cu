@@ -17,7 +17,8 @@
 //            its two entries inside the table, the two digits recompose the
 //            task index, and the row kernels' shared memory fits the SM;
 //   pipelined column pass: stage, tile and twiddle indexes in bounds;
-//   Shoup quotients from the double estimate equal floor(w 2^32 / p).
+//   Shoup quotients from the double estimate equal floor(w 2^32 / p);
+//   the quad-interleaved row spectrum is a permutation with warp-contiguous runs.
 #include <cstdio>
 #include <set>
 #include <vector>
@@ -162,6 +163,23 @@ void col_plan_check() {
     for (int i = 0; i < (1 << L1); ++i) CHECK(k[i] == 1, "col_slot_to_k1 L1=%d not a permutation", L1);
 }
 
+// G's row spectrum between the row kernels: quad c of 32-word group r at
+// c * n2/8 + 4 r, a permutation of the row's quads; the lanes of a warp
+// (consecutive r) cover one contiguous 512-byte run per quad index.
+template <int L2>
+void spectrum_layout_check() {
+    constexpr int n2 = 1 << L2, G = n2 / 32;
+    std::vector<int> hit(n2 / 4, 0);
+    for (int r = 0; r < G; ++r)
+        for (int c = 0; c < 8; ++c) {
+            const int w = c * (n2 / 8) + 4 * r;
+            CHECK((w % 4 == 0 && w + 3 < n2), "spectrum L2=%d quad in row", L2);
+            if (w % 4 == 0 && w + 3 < n2) hit[w / 4]++;
+            if (r % 32 != 0) CHECK(w == c * (n2 / 8) + 4 * (r - 1) + 4, "spectrum L2=%d warp run", L2);
+        }
+    for (int q = 0; q < n2 / 4; ++q) CHECK(hit[q] == 1, "spectrum L2=%d quad %d hit %d", L2, q, hit[q]);
+}
+
 template <int L2>
 void row_tab_check() {
     using RT = RowTab<L2>;
@@ -293,6 +311,9 @@ int main() {
     col_plan_check<9>();
     col_plan_check<10>();
     col_plan_check<11>();
+    spectrum_layout_check<6>();
+    spectrum_layout_check<10>();
+    spectrum_layout_check<14>();
     row_tab_check<11>();
     row_tab_check<12>();
     row_tab_check<13>();
