@@ -5,12 +5,17 @@
 // four-step split x[r*n2 + c]: a length-n1 DFT down every column, a twiddle
 // w_n^(c*k1), and a length-n2 DFT along every row.  The whole product needs
 // three passes over HBM:
-//   A  k_col_fwd    column DFTs of both operands (tile of 32 columns x n1
-//                   rows in shared memory; the zero pad is never read);
-//   B  k_row_fused  per row: twiddle, row DFT of both operands, pointwise
-//                   product, inverse row DFT, inverse twiddle with the 1/n
-//                   scale folded in;
-//   C  k_col_inv    inverse column DFTs, truncation, canonical residues.
+//   A  column DFTs of both operands: k_col_fwd_pipe (persistent, the next
+//      tile staged while the current one is transformed) for 2^9- and
+//      2^10-row columns, k_col_fwd (one tile per CTA) otherwise; the zero
+//      pad is never read;
+//   B  per row: twiddle, row DFT of both operands, pointwise product,
+//      inverse row DFT, inverse twiddle with the 1/n scale folded in: the
+//      split pair k_row_fwd_g + k_row_mul_f (one operand row per CTA; level
+//      0 reads per-slot factor tables built once by k_rowtab_build), or
+//      k_row_fused (both rows in one CTA, for comparison);
+//   C  inverse column DFTs, truncation, canonical residues: k_col_inv_pipe
+//      or k_col_inv, as for pass A.
 // Rows leave pass A in digit-reversed order of k1 and are consumed in that
 // order by passes B and C, so nothing is ever permuted.
 #pragma once
