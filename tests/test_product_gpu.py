@@ -72,6 +72,21 @@ def test_column_pass_unaligned_device_operands(cm, oracle_mod, da, db, off):
     assert np.array_equal(got, oracle_mod.polymul(a, b, P0))
 
 
+@pytest.mark.parametrize("da,db,dh", [(2**19 - 1, 2**19 - 1, 100000), (2**20 - 1, 2**20 - 1, 2**20 + 12345),
+                                      (2**19 - 1, 2**19 - 1, 2**20 + 40)])
+def test_output_length_contract_large(cm, oracle_mod, da, db, dh):
+    """Truncated and zero-extended outputs of 2^20 and 2^21 transforms (the
+    pipelined inverse column pass stops at lh)."""
+    r = SplitMix64(da + 3 * dh)
+    a, b = _rand(r, da + 1, P0), _rand(r, db + 1, P0)
+    full = oracle_mod.polymul(a, b, P0)
+    got = cm.fftmul_uni(a, b, P0, dh=dh)
+    want = np.zeros(dh + 1, dtype=np.uint32)
+    k = min(dh + 1, len(full))
+    want[:k] = full[:k]
+    assert np.array_equal(got, want)
+
+
 def test_c1_config_vs_modpn(cm, oracle_mod):
     """4095 x 4095 mod 469762049 (transform 8192) against modpn's own product."""
     r = SplitMix64(0xC0DA0000)
@@ -132,3 +147,30 @@ def test_inputs_above_p_are_reduced(cm, oracle_mod):
     b = r.next_u64(200).astype(np.uint32)
     want = oracle_mod.polymul_school(a % P0, b % P0, P0)
     assert np.array_equal(cm.fftmul_uni(a, b, P0), want)
+
+
+def test_comparison_switches_give_the_same_products(cm):
+    """CUMODP_COL_PIPE=0 (one-tile-per-CTA column passes) and CUMODP_ROWTAB=0
+    (factor tables built inside every row CTA) select other kernels for the
+    same products: a 2^21 and a 2^23 product must come out identical."""
+    import os
+    import subprocess
+    import sys
+    code = (
+        "import numpy as np, cumodp_b200 as cm\n"
+        "from cumodp_b200.workloads import SplitMix64\n"
+        "r = SplitMix64(99); p = 469762049\n"
+        "out = []\n"
+        "for d in (2**20 - 1, 2**22 - 1):\n"
+        "    a, b = r.residues(d + 1, p), r.residues(d + 1, p)\n"
+        "    h = cm.fftmul_uni(a, b, p)\n"
+        "    out.append(int((h.astype(np.uint64) * np.arange(1, len(h) + 1, dtype=np.uint64)).sum() % (2**61 - 1)))\n"
+        "print(out)\n")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    res = []
+    for extra in ({}, {"CUMODP_COL_PIPE": "0", "CUMODP_ROWTAB": "0"}):
+        env = dict(os.environ, PYTHONPATH=root, **extra)
+        out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=300)
+        assert out.returncode == 0, out.stderr[-2000:]
+        res.append(out.stdout.strip().splitlines()[-1])
+    assert res[0] == res[1]
