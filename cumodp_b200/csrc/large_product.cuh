@@ -470,9 +470,11 @@ __global__ void __launch_bounds__(NW * 32, col_pipe_ctas(L1)) k_col_fwd_pipe(con
 // column plans (n1 = 2^9: 32-column tiles, n1 = 2^10: 16-column tiles, the
 // inverse pass's layouts).  Each CTA walks the tiles gridDim.x apart; the
 // whole next tile is copied into a stage buffer (cp.async) while the current
-// one is transformed.  The deepest level reads the stage and writes the
-// tile; level 0 reads the tile and stores the canonical residues straight to
-// the output, truncated at lh.  Results are those of k_col_inv.
+// one is transformed: each warp refills the stage rows of its own blocks as
+// soon as its deepest-level tasks have consumed them.  The deepest level
+// reads the stage and writes the tile; level 0 reads the tile and stores the
+// canonical residues straight to the output, truncated at lh.  Results are
+// those of k_col_inv.
 template <int L1, int NW>
 __global__ void __launch_bounds__(NW * 32, 1) k_col_inv_pipe(const __grid_constant__ LargeArgs A) {
     constexpr LevelPlan PL = col_plan(L1);
@@ -493,6 +495,7 @@ __global__ void __launch_bounds__(NW * 32, 1) k_col_inv_pipe(const __grid_consta
     for (int i = threadIdx.x; i < n1; i += T) tws[i] = A.twc[A.twc_inv + i];
 
     // the whole tile t (all n1 rows of the row pass's output) into the stage
+    // (the first tile; later ones are refilled per warp)
     auto stage_issue = [&](int t) {
         const LargeJob& J = A.jobs ? A.jobs[t / ct] : A.job0;
         // a thread keeps one quad column q and walks rows T / QR apart
@@ -525,8 +528,27 @@ __global__ void __launch_bounds__(NW * 32, 1) k_col_inv_pipe(const __grid_consta
 #pragma unroll
             for (int m = 0; m < R1; ++m) tile[off + tile_step<L1, INV, 1>(m)] = x[m];
         }
-        __syncthreads();  // tile complete; the stage is free
-        if (t + (int)gridDim.x < ntiles) stage_issue(t + gridDim.x);
+        // this warp's blocks (rows [warp SUB R1, (warp + 1) SUB R1)) have been
+        // read (their words reached the tile), so the warp refills those stage
+        // rows with the next tile's at once, half a tile earlier than a
+        // CTA-wide refill after the barrier
+        static_assert(NW * SUB == R0, "one block set per warp");
+        __syncwarp();
+        if (t + (int)gridDim.x < ntiles) {
+            const int tn = t + gridDim.x;
+            const LargeJob& Jn = A.jobs ? A.jobs[tn / ct] : A.job0;
+            const int q = lane % QR;
+            const int r0 = warp * SUB * R1 + lane / QR;
+            const u32* src = Jn.wa + (tn % ct) * TC + (size_t)r0 * n2 + 4 * q;
+            const size_t step = (size_t)(32 / QR) * n2;
+#pragma unroll 4
+            for (int r = r0; r < (warp + 1) * SUB * R1; r += 32 / QR, src += step) {
+                const unsigned d = (unsigned)__cvta_generic_to_shared(stage + tile_row<L1, INV>(r) + 4 * q);
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+            }
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        __syncthreads();  // tile complete
 
         // level 0: task o (rows o + R1 m), pre-twiddle, DIT, canonical residues out
         const LargeJob& J = A.jobs ? A.jobs[t / ct] : A.job0;

@@ -271,6 +271,19 @@ void col_inv_pipe_check() {
             CHECK(o * R0 + m < n1, "colinvpipe L1=%d twiddle", L1);
         }
     CHECK(col_inv_pipe_smem_bytes(L1) + 1024 <= 228 * 1024, "colinvpipe L1=%d shared memory", L1);
+    // per-warp refill: warp w's deepest-level blocks are exactly the rows it
+    // copies, [w SUB R1, (w + 1) SUB R1), and the warps cover all n1 rows once
+    constexpr int NW = col_inv_pipe_warps(L1), SUB = 32 / TC;
+    CHECK(NW * SUB == R0, "colinvpipe L1=%d one block set per warp", L1);
+    std::vector<int> rows(n1, 0);
+    for (int w = 0; w < NW; ++w)
+        for (int l = 0; l < 32; ++l) {
+            const int blk = w * SUB + l / TC;
+            CHECK((blk * R1 >= w * SUB * R1 && (blk + 1) * R1 <= (w + 1) * SUB * R1), "colinvpipe L1=%d warp blocks", L1);
+            for (int r = w * SUB * R1 + l / QR; r < (w + 1) * SUB * R1; r += 32 / QR)
+                if (l % QR == 0) rows[r]++;
+        }
+    for (int r = 0; r < n1; ++r) CHECK(rows[r] == 1, "colinvpipe L1=%d refill row %d copied %d times", L1, r, rows[r]);
 }
 
 void shoup_quot_check() {
