@@ -143,14 +143,17 @@ __global__ void __launch_bounds__(ntt_row_threads(L2), ntt_row_ctas(L2)) k_row_n
         for (int j = 0; j < 32; ++j) x[j] = red1(mul_shoup(x[j], A.scale.w, A.scale.wq, p), p);
     }
     __syncthreads();
+    // natural order through shared memory (swz_nat layout: the reorder's
+    // stores are conflict-free), read out word by word, consecutive lanes on
+    // consecutive words
     if (has) {
 #pragma unroll
-        for (int j = 0; j < 32; ++j) sm[swz((int)row_pos_to_freq<L2>((u32)(r * 32 + j)))] = x[j];
+        for (int j = 0; j < 32; ++j) sm[swz_nat((int)row_pos_to_freq<L2>((u32)(r * 32 + j)))] = x[j];
     }
     __syncthreads();
     u32* out = A.dst + (size_t)out_row * n2;
-    for (int i = threadIdx.x * 4; i < n2; i += T * 4)
-        *reinterpret_cast<uint4*>(out + i) = *reinterpret_cast<const uint4*>(sm + swz(i));
+#pragma unroll 4
+    for (int i = threadIdx.x; i < n2; i += T) out[i] = sm[swz_nat(i)];
 }
 
 // out[c * rows + r] = in[r * cols + c] for rows and cols multiples of 64:

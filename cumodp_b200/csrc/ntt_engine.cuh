@@ -57,6 +57,14 @@ __host__ __device__ __forceinline__ int swz_task(int base, int bswz, int m) {
 }
 
 // The low r bits of j in reverse order.
+// Word index swizzle of the natural-order reorder buffer: bits 0-3 XOR bits
+// 5-8.  When the lanes of a warp each store one last-level output at its
+// frequency, those frequencies share their low bits; the XOR spreads them
+// over all 32 banks (for every row plan of 2^10-2^14 words).  A bijection
+// on each 512-word block, and a permutation of every 32-word row, so a
+// read-out of consecutive words by consecutive lanes is conflict-free too.
+__host__ __device__ __forceinline__ int swz_nat(int f) { return f ^ ((f >> 5) & 15); }
+
 __host__ __device__ __forceinline__ u32 rev_bits(u32 j, int r) {
 #ifdef __CUDA_ARCH__
     return __brev(j) >> (32 - r);

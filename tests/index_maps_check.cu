@@ -18,7 +18,8 @@
 //            task index, and the row kernels' shared memory fits the SM;
 //   pipelined column pass: stage, tile and twiddle indexes in bounds;
 //   Shoup quotients from the double estimate equal floor(w 2^32 / p);
-//   the quad-interleaved row spectrum is a permutation with warp-contiguous runs.
+//   the quad-interleaved row spectrum is a permutation with warp-contiguous runs;
+//   the natural-order reorder buffer's swizzle is a bijection without store conflicts.
 #include <cstdio>
 #include <set>
 #include <vector>
@@ -161,6 +162,27 @@ void col_plan_check() {
         if (v < (1u << L1)) k[v]++;
     }
     for (int i = 0; i < (1 << L1); ++i) CHECK(k[i] == 1, "col_slot_to_k1 L1=%d not a permutation", L1);
+}
+
+// Natural-order reorder of k_row_ntt: swz_nat is a bijection, and the
+// stores of one step (lanes r = 32 w + lane, output j) hit distinct banks.
+template <int L2>
+void ntt_reorder_check() {
+    constexpr int n2 = 1 << L2;
+    std::vector<int> hit(n2, 0);
+    for (int f = 0; f < n2; ++f) {
+        const int a = swz_nat(f);
+        CHECK((a >= 0 && a < n2), "reorder L2=%d range", L2);
+        if (a >= 0 && a < n2) hit[a]++;
+    }
+    for (int i = 0; i < n2; ++i) CHECK(hit[i] == 1, "reorder L2=%d bijection", L2);
+    for (int w = 0; w * 32 < n2 / 32; ++w)
+        for (int j = 0; j < 32; ++j) {
+            int banks[32] = {0};
+            for (int l = 0; l < 32 && w * 32 + l < n2 / 32; ++l)
+                banks[swz_nat((int)row_pos_to_freq<L2>((u32)((w * 32 + l) * 32 + j))) % 32]++;
+            for (int b = 0; b < 32; ++b) CHECK(banks[b] <= 1, "reorder L2=%d bank conflict", L2);
+        }
 }
 
 // G's row spectrum between the row kernels: quad c of 32-word group r at
@@ -324,6 +346,11 @@ int main() {
     col_plan_check<9>();
     col_plan_check<10>();
     col_plan_check<11>();
+    ntt_reorder_check<10>();
+    ntt_reorder_check<11>();
+    ntt_reorder_check<12>();
+    ntt_reorder_check<13>();
+    ntt_reorder_check<14>();
     spectrum_layout_check<6>();
     spectrum_layout_check<10>();
     spectrum_layout_check<14>();
