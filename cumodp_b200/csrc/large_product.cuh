@@ -466,6 +466,105 @@ __global__ void __launch_bounds__(NW * 32, col_pipe_ctas(L1)) k_col_fwd_pipe(con
     }
 }
 
+// Pass A of a natural-order transform (one full-length operand per job,
+// written over wa) as a persistent, software-pipelined kernel for 2^10-row
+// columns on 16-column tiles: the whole next tile is staged by cp.async
+// (zero-filled past the operand's end; word by word for an unaligned
+// source) while the current one is transformed.  Level 0 reads and reduces
+// the stage and writes the tile; level 1 stores straight to HBM.  Results
+// are those of k_col_fwd<L1, NW, 2>.
+template <int L1, int NW>
+__global__ void __launch_bounds__(NW * 32, 1) k_col_fwd_pipe1(const __grid_constant__ LargeArgs A) {
+    constexpr LevelPlan PL = col_plan(L1);
+    static_assert(PL.nlev == 2, "two-level column plans only");
+    constexpr int KIND = 2, n1 = 1 << L1, T = NW * 32;
+    constexpr int R0 = 1 << PL.logr[0], R1 = 1 << PL.logr[1];  // n1 = R0 * R1
+    constexpr int TC = col_tile_cols(L1, KIND), SUB = 32 / TC, QR = TC / 4;
+    constexpr int TW = col_tile_words(L1, KIND);
+    extern __shared__ __align__(16) u32 smem[];
+    u32* tile = smem;
+    u32* stage = smem + TW;
+    Tw* tws = reinterpret_cast<Tw*>(stage + TW);  // level-0 twiddles (n1 entries)
+    const int n2 = 1 << A.l2, ct = n2 / TC;
+    const int ntiles = ct * A.njobs;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int col = lane % TC;
+    const u32 p = A.pkc.p, p2 = A.pkc.p2, oneq = A.pkc.one_q;
+    for (int i = threadIdx.x; i < n1; i += T) tws[i] = A.twc[i];
+
+    // all n1 rows x TC columns of tile t into the stage (one commit group);
+    // words at or past the operand's length read as 0
+    auto stage_issue = [&](int t) {
+        const LargeJob& J = A.jobs ? A.jobs[t / ct] : A.job0;
+        const u32* src = J.a;
+        const long long len = J.la;
+        const int c0 = (t % ct) * TC;
+        if ((reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+            static_assert(T % QR == 0, "whole rows per thread round");
+            const int q = threadIdx.x % QR;
+            const long long step = (long long)(T / QR) * n2;
+            long long gi = (long long)(threadIdx.x / QR) * n2 + c0 + 4 * q;
+#pragma unroll 4
+            for (int r = threadIdx.x / QR; r < n1; r += T / QR, gi += step) {
+                const long long rem = len - gi;
+                const int bytes = rem >= 4 ? 16 : (rem > 0 ? (int)rem * 4 : 0);
+                const u32* g = bytes ? src + gi : src;
+                const unsigned d = (unsigned)__cvta_generic_to_shared(stage + tile_row<L1, KIND>(r) + 4 * q);
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(g), "r"(bytes) : "memory");
+            }
+        } else {
+            for (int idx = threadIdx.x; idx < n1 * TC; idx += T) {
+                const int r = idx / TC, c = idx % TC;
+                const long long gi = (long long)r * n2 + c0 + c;
+                const int bytes = gi < len ? 4 : 0;
+                const u32* g = bytes ? src + gi : src;
+                const unsigned d = (unsigned)__cvta_generic_to_shared(stage + tile_row<L1, KIND>(r) + c);
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(g), "r"(bytes) : "memory");
+            }
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+
+    int t = blockIdx.x;
+    if (t < ntiles) stage_issue(t);
+    for (; t < ntiles; t += gridDim.x) {
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        __syncthreads();  // stage and twiddles visible; the previous tile's level 1 is done with `tile`
+
+        // level 0: task o (rows o + R1 m), inputs reduced, DIF, twiddles, stage -> tile
+        for (int o = warp * SUB + lane / TC; o < R1; o += NW * SUB) {
+            u32 x[R0];
+            const int off = tile_row<L1, KIND>(o) + col;
+#pragma unroll
+            for (int m = 0; m < R0; ++m) x[m] = mul_shoup(stage[off + tile_step<L1, KIND, R1>(m)], 1u, oneq, p);
+            dif_regs<R0, true>(x, A.pkc.rc.f, p, p2);
+#pragma unroll
+            for (int j = 1; j < R0; ++j) {
+                const Tw w = tws[o * R0 + j];
+                x[j] = mul_shoup(x[j], w.w, w.wq, p);
+            }
+#pragma unroll
+            for (int m = 0; m < R0; ++m) tile[off + tile_step<L1, KIND, R1>(m)] = x[m];
+        }
+        __syncthreads();  // tile complete; the stage is free
+        if (t + (int)gridDim.x < ntiles) stage_issue(t + gridDim.x);
+
+        // level 1 (last): block blk = rows blk * R1 + m, straight to HBM
+        const LargeJob& J = A.jobs ? A.jobs[t / ct] : A.job0;
+        const int c0 = (t % ct) * TC;
+        for (int blk = warp * SUB + lane / TC; blk < R0; blk += NW * SUB) {
+            u32 x[R1];
+            const int off = tile_row<L1, KIND>(blk * R1) + col;
+#pragma unroll
+            for (int m = 0; m < R1; ++m) x[m] = tile[off + tile_step<L1, KIND, 1>(m)];
+            dif_regs<R1>(x, A.pkc.rc.f, p, p2);
+            u32* out = J.wa + (size_t)(blk * R1) * n2 + c0 + col;
+#pragma unroll
+            for (int m = 0; m < R1; ++m, out += n2) *out = x[m];
+        }
+    }
+}
+
 // Pass C as a persistent, software-pipelined kernel for the two-level
 // column plans (n1 = 2^9: 32-column tiles, n1 = 2^10: 16-column tiles, the
 // inverse pass's layouts).  Each CTA walks the tiles gridDim.x apart; the

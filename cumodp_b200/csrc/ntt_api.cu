@@ -274,9 +274,7 @@ int column_pass(const PrimeCtx& pc, u32 root_c, int l1, int l2, const u32* src, 
     A.colpl = col_plan(l1);
     A.job0 = LargeJob{src, nullptr, nullptr, (int)std::min<long long>(len, 1ll << 30), 0, 0, 0, dst, nullptr};
     A.njobs = 1;
-    // (the pipelined pass-A kernel measured slower here: a full-length input
-    // has no zero half, so half of every tile's load is exposed)
-    kColFwd1[l1](A, (1 << l2) / col_tile_cols_rt(l1, 2), st);
+    if (!launch_col_fwd_pipe1(A, 1, st)) kColFwd1[l1](A, (1 << l2) / col_tile_cols_rt(l1, 2), st);
     return OK;
 }
 

@@ -127,6 +127,13 @@ __host__ __device__ constexpr int col_inv_pipe_smem_bytes(int logl) {
     return 2 * col_tile_words(logl, 1) * 4 + (1 << logl) * 8;
 }
 
+// Persistent pass A of a natural-order transform (k_col_fwd_pipe1): 2^10-row
+// columns, one 512-thread CTA per SM holding the tile, a stage for the whole
+// next tile and the level-0 twiddles.
+__host__ __device__ constexpr int col_pipe1_smem_bytes(int logl) {
+    return 2 * col_tile_words(logl, 2) * 4 + (1 << logl) * 8;
+}
+
 // A single product (no batch) of transform length 2^logn uses the three-pass
 // kernels from this length on, even where one CTA could hold it: spread over
 // many CTAs it finishes sooner than on one SM.

@@ -218,6 +218,10 @@ void attr_col() {
     cudaFuncSetAttribute(k_col_inv<L1, col_warps(L1, true)>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          col_smem_bytes(L1, true));
 }
+void attr_col_pipe1() {
+    cudaFuncSetAttribute(k_col_fwd_pipe1<10, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         col_pipe1_smem_bytes(10));
+}
 template <int L1>
 void attr_col_pipe() {
     cudaFuncSetAttribute(k_col_fwd_pipe<L1, col_pipe_kind(L1), col_pipe_warps(L1)>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -262,7 +266,7 @@ void ensure_kernel_attrs() {
         attr_small<10>(); attr_small<11>(); attr_small<12>(); attr_small<13>(); attr_small<14>();
         attr_col<1>(); attr_col<2>(); attr_col<3>(); attr_col<4>(); attr_col<5>();
         attr_col<6>(); attr_col<7>(); attr_col<8>(); attr_col<9>(); attr_col<10>(); attr_col<11>();
-        attr_col_pipe<9>(); attr_col_pipe<10>();
+        attr_col_pipe<9>(); attr_col_pipe<10>(); attr_col_pipe1();
         attr_row<6>(); attr_row<7>(); attr_row<8>(); attr_row<9>(); attr_row<10>();
         attr_row<11>(); attr_row<12>(); attr_row<13>(); attr_row<14>();
         attr_rowsplit<6>(); attr_rowsplit<7>(); attr_rowsplit<8>(); attr_rowsplit<9>(); attr_rowsplit<10>();
@@ -362,6 +366,15 @@ bool launch_col_fwd_pipe(const LargeArgs& a, int njobs, cudaStream_t st) {
     const int ntiles = ((1 << a.l2) / col_tile_cols_rt(a.l1, col_pipe_kind(a.l1))) * 2 * njobs;
     if (a.l1 == 10) launch_col_fwd_pipe_t<10>(a, ntiles, st);
     else launch_col_fwd_pipe_t<9>(a, ntiles, st);
+    return true;
+}
+
+bool launch_col_fwd_pipe1(const LargeArgs& a, int njobs, cudaStream_t st) {
+    if (a.l1 != 10 || !col_pipe_enabled()) return false;
+    ensure_kernel_attrs();
+    const int ntiles = ((1 << a.l2) / col_tile_cols_rt(10, 2)) * njobs;
+    const int grid = std::min(ntiles, sm_count(current_device()));
+    k_col_fwd_pipe1<10, 16><<<grid, 16 * 32, col_pipe1_smem_bytes(10), st>>>(a);
     return true;
 }
 

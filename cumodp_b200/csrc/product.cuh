@@ -27,6 +27,9 @@ int large_args(const PrimeCtx& pc, u32 root_n, int logn, int l2, int dev, LargeA
 // A product's pass A through the persistent pipelined kernel when the column
 // length has one (2^9, 2^10 rows); false when the caller must launch k_col_fwd.
 bool launch_col_fwd_pipe(const LargeArgs& a, int njobs, cudaStream_t st);
+// A natural-order transform's column pass (operand a of each job, over wa)
+// through k_col_fwd_pipe1 when the columns have 2^10 rows; false otherwise.
+bool launch_col_fwd_pipe1(const LargeArgs& a, int njobs, cudaStream_t st);
 void launch_small(int logn, const SmallArgs& a, int njobs, cudaStream_t st);
 void launch_large(const LargeArgs& a, int njobs, cudaStream_t st);
 

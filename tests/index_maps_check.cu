@@ -361,6 +361,8 @@ int main() {
     col_pipe_check<9, 0>();
     col_pipe_check<10, 0>();
     col_pipe_check<10, 2>();
+    CHECK(col_pipe1_smem_bytes(10) + 1024 <= 228 * 1024, "colpipe1 shared memory");
+    CHECK(col_pipe1_smem_bytes(10) == 2 * col_tile_words(10, 2) * 4 + 1024 * 8, "colpipe1 layout");
     col_inv_pipe_check<9>();
     col_inv_pipe_check<10>();
     shoup_quot_check();
