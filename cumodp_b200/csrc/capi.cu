@@ -60,14 +60,14 @@ float global_memory_in_megabytes(void) {
 int can_call_fftmul_uni(sfixn df, sfixn dg) {
     if (!have_device() || df < 0 || dg < 0) return 0;
     const int logn = product_logn((long long)df + 1, (long long)dg + 1);
-    if (logn > kMaxLog) return 0;
+    if (logn > kMaxSplitLog) return 0;
     size_t fr = 0, tot = 0;
     if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
-    // staging (F, G, H) plus two transform-length workspaces
-    const size_t need = ((size_t)df + dg + 2 + ((size_t)df + dg + 1) + (2ull << logn)) * 4;
+    // staging (F, G, H) plus the product's workspace
+    const size_t need = ((size_t)df + dg + 2 + ((size_t)df + dg + 1) + mul_ws_words(logn)) * 4;
     return need < tot / 2 ? 1 : 0;
 }
 

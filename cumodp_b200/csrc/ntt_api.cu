@@ -278,6 +278,91 @@ int column_pass(const PrimeCtx& pc, u32 root_c, int l1, int l2, const u32* src, 
     return OK;
 }
 
+// First radix-2 (decimation-in-frequency) step of a transform of n = 2h
+// words with root w: y0[j] = s (x[j] + x[j+h]) and y1[j] = s (x[j] - x[j+h])
+// w^j for j < h, written over x_out[j] and x_out[j+h] (x_out may be x_in:
+// each thread reads and writes the same four pairs).  Then the even outputs
+// are DFT_h(y0; w^2) and the odd ones DFT_h(y1; w^2).  w^j * 2^32 is the
+// Montgomery product of the seed-table words w^(j mod 4096) 2^32 and
+// w^(4096 floor(j / 4096)) 2^32.  Inputs are any 32-bit words (reduced
+// here); s = 1 (scaled = 0) or the inverse transform's 2^-k.
+__global__ void __launch_bounds__(256) k_split_dif(const u32* x_in, u32* x_out, long long h,
+                                                   const u32* __restrict__ seeds, int nlo, PrimeK pk, Tw s,
+                                                   int scaled) {
+    const u32 p = pk.p;
+    const uint4* a4 = reinterpret_cast<const uint4*>(x_in);
+    const uint4* b4 = reinterpret_cast<const uint4*>(x_in + h);
+    uint4* y0 = reinterpret_cast<uint4*>(x_out);
+    uint4* y1 = reinterpret_cast<uint4*>(x_out + h);
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < h / 4;
+         q += (long long)gridDim.x * blockDim.x) {
+        const uint4 av = a4[q], bv = b4[q];
+        u32 a[4] = {av.x, av.y, av.z, av.w}, b[4] = {bv.x, bv.y, bv.z, bv.w}, u[4], v[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const u32 ra = red1(mul_shoup(a[t], 1u, pk.one_q, p), p);
+            const u32 rb = red1(mul_shoup(b[t], 1u, pk.one_q, p), p);
+            const u32 e = (u32)(4 * q + t);  // j < h <= 2^28
+            const u32 wj = seed_mont_at(seeds, nlo, e, p, pk.pinv_neg);  // w^j 2^32, [0, 2p)
+            u32 s0 = red1(ra + rb, p);
+            u32 s1 = red1(mul_mont(ra - rb + p, wj, p, pk.pinv_neg), p);
+            if (scaled) {
+                s0 = red1(mul_shoup(s0, s.w, s.wq, p), p);
+                s1 = red1(mul_shoup(s1, s.w, s.wq, p), p);
+            }
+            u[t] = s0;
+            v[t] = s1;
+        }
+        y0[q] = make_uint4(u[0], u[1], u[2], u[3]);
+        y1[q] = make_uint4(v[0], v[1], v[2], v[3]);
+    }
+}
+
+// x[2m] = s0[m], x[2m+1] = s1[m] for m < h (the even and odd outputs of the
+// split transform back in natural order).
+__global__ void __launch_bounds__(256) k_interleave2(const u32* __restrict__ s0, const u32* __restrict__ s1,
+                                                     u32* __restrict__ x, long long h) {
+    const uint4* a4 = reinterpret_cast<const uint4*>(s0);
+    const uint4* b4 = reinterpret_cast<const uint4*>(s1);
+    uint4* x4 = reinterpret_cast<uint4*>(x);
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < h / 4;
+         q += (long long)gridDim.x * blockDim.x) {
+        const uint4 a = a4[q], b = b4[q];
+        x4[2 * q] = make_uint4(a.x, b.x, a.y, b.y);
+        x4[2 * q + 1] = make_uint4(a.z, b.z, a.w, b.w);
+    }
+}
+
+}  // namespace
+
+int ntt_natural_dev(const u32* x_in, u32* x_out, int k, u32 w, u32 p, bool inverse, cudaStream_t st);
+
+namespace {
+
+// A transform longer than the four-step kernels' 2^kMaxLog: one radix-2
+// step over HBM (k_split_dif, which also applies the inverse's scaling),
+// the two half-length transforms with root^2 (recursively), and the
+// interleave of their outputs.  root is the transform's own root (already
+// inverted for an inverse transform).
+int ntt_split_dev(const PrimeCtx& pc, const u32* x_in, u32* x_out, int k, u32 root, u32 sc, cudaStream_t st) {
+    int err = OK;
+    const u32 p = pc.info.p;
+    const long long n = 1ll << k, h = n / 2;
+    const int dev = current_device();
+    const u32* seeds = seed_tables(dev, p, root, k, &err);
+    if (!seeds) return err ? err : OUT_OF_MEMORY;
+    u32* S = (u32*)workspace(dev, kWsSplitNtt + (k - kMaxLog - 1), (size_t)n * sizeof(u32), &err);
+    if (!S) return err;
+    const int grid = 4 * sm_count(dev);
+    k_split_dif<<<grid, 256, 0, st>>>(x_in, x_out, h, seeds, (int)std::min<long long>(n, 4096), pc.pk,
+                                      tw_of(sc, p), sc != 1u);
+    const u32 root2 = mulmod_exact(root, root, p);
+    if ((err = ntt_natural_dev(x_out, S, k - 1, root2, p, false, st)) != OK) return err;
+    if ((err = ntt_natural_dev(x_out + h, S + h, k - 1, root2, p, false, st)) != OK) return err;
+    k_interleave2<<<grid, 256, 0, st>>>(S, S + h, x_out, h);
+    return cuda_err(cudaGetLastError());
+}
+
 }  // namespace
 
 // x_out = DFT(x_in) with root w (inverse: root w^-1 and scaling by 2^-k).
@@ -289,10 +374,11 @@ int ntt_natural_dev(const u32* x_in, u32* x_out, int k, u32 w, u32 p, bool inver
     if (k >= 6 && (((uintptr_t)x_in | (uintptr_t)x_out) & 15)) return ASSUMPTION_ERROR;  // 16-byte rows
     if (k > pc->info.two_adic) return FFT_SIZE_TOO_LARGE;
     if (!root_has_order(w, k, p)) return ASSUMPTION_ERROR;
-    if (k > kMaxLog) return FFT_SIZE_TOO_LARGE;
+    if (k > kMaxSplitLog) return FFT_SIZE_TOO_LARGE;
     const int dev = current_device();
     const u32 root = inverse ? inv_of(w, p) : w;
     const u32 sc = inverse ? inv_of((u32)((1ull << k) % p), p) : 1u;
+    if (k > kMaxLog) return ntt_split_dev(*pc, x_in, x_out, k, root, sc, st);
     if (k <= 5) {
         k_tiny_dft<<<1, 1 << k, 0, st>>>(x_in, x_out, 1 << k, root, p, sc);
         return cuda_err(cudaGetLastError());

@@ -60,7 +60,8 @@ void launch_col_fwd_t(const LargeArgs& a, dim3 grid, cudaStream_t st) {
     }
     k_col_fwd<L1, col_warps(L1, false)><<<grid, col_warps(L1, false) * 32, smem, st>>>(a);
 }
-// SMs of the current device (cached per device).
+}  // namespace
+
 int sm_count(int dev) {
     static int cache[64] = {0};
     if (dev < 0 || dev >= 64) return 148;
@@ -71,6 +72,8 @@ int sm_count(int dev) {
     }
     return cache[dev];
 }
+
+namespace {
 
 // Whether pass A uses the persistent pipelined kernel where it applies
 // (CUMODP_COL_PIPE=0 selects the one-tile-per-CTA kernel, for comparison).
@@ -408,6 +411,62 @@ void launch_large(const LargeArgs& a, int njobs, cudaStream_t st) {
     if (tr) pass_timing_end(st, kColInvName[a.l1], e0);
 }
 
+// h[i] = (h[i] + t[i]) mod p for i < len; both in [0, p).
+__global__ void k_add_mod(u32* __restrict__ h, const u32* __restrict__ t, long long len, u32 p) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len;
+         i += (long long)gridDim.x * blockDim.x)
+        h[i] = red1(h[i] + t[i], p);
+}
+
+size_t mul_ws_words(int logn) {
+    // direct: the two n-word arrays of the three passes; split: those of a
+    // 2^kMaxLog piece plus the piece's product
+    return logn <= kMaxLog ? (size_t)2 << logn : (size_t)3 << kMaxLog;
+}
+
+namespace {
+
+// A product whose transform is longer than 2^kMaxLog.  Each operand is cut
+// into pieces of 2^(kMaxLog-1) coefficients; every pair of pieces (i, j)
+// is multiplied by the three-pass kernels (a transform of at most
+// 2^kMaxLog) and added into h at offset i + j.  At most four pairs for
+// balanced operands of a 2^26 product.  An operand that overlaps h is first
+// copied aside (h is cleared before the pieces are added).
+int mul_split_dev(const u32* a, long long la, const u32* b, long long lb, u32* h, long long lh, u32 p,
+                  cudaStream_t st) {
+    const long long C = 1ll << (kMaxLog - 1);
+    const int dev = current_device();
+    int err = OK;
+    auto overlaps = [&](const u32* x, long long lx) { return x < h + lh && h < x + lx; };
+    if (overlaps(a, la) || overlaps(b, lb)) {
+        u32* in = (u32*)workspace(dev, kWsSplitIn, (size_t)(la + lb) * sizeof(u32), &err);
+        if (!in) return err;
+        cudaError_t e = cudaMemcpyAsync(in, a, (size_t)la * sizeof(u32), cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(in + la, b, (size_t)lb * sizeof(u32), cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return cuda_err(e);
+        a = in;
+        b = in + la;
+    }
+    u32* t = (u32*)workspace(dev, kWsSplitProd, (size_t)(2 * C) * sizeof(u32), &err);
+    if (!t) return err;
+    cudaError_t e = cudaMemsetAsync(h, 0, (size_t)lh * sizeof(u32), st);
+    if (e != cudaSuccess) return cuda_err(e);
+    const int grid = 4 * sm_count(dev);
+    for (long long i = 0; i < la; i += C)
+        for (long long j = 0; j < lb; j += C) {
+            const long long off = i + j;
+            if (off >= lh) continue;
+            const long long li = std::min(C, la - i), lj = std::min(C, lb - j);
+            const long long lt = std::min(li + lj - 1, lh - off);
+            if ((err = mul_dev(a + i, li, b + j, lj, t, lt, p, st)) != OK) return err;
+            k_add_mod<<<grid, 256, 0, st>>>(h + off, t, lt, p);
+        }
+    return cuda_err(cudaGetLastError());
+}
+
+}  // namespace
+
 int mul_dev(const u32* a, long long la, const u32* b, long long lb, u32* h, long long lh, u32 p,
             cudaStream_t st) {
     if (la <= 0 || lb <= 0 || lh < 0) return ASSUMPTION_ERROR;
@@ -417,7 +476,8 @@ int mul_dev(const u32* a, long long la, const u32* b, long long lb, u32* h, long
     if (!pc) return err;
     const int logn = product_logn(la, lb);
     if (logn > pc->info.two_adic) return FFT_SIZE_TOO_LARGE;
-    if (logn > kMaxLog) return FFT_SIZE_TOO_LARGE;
+    if (logn > kMaxSplitLog) return FFT_SIZE_TOO_LARGE;
+    if (logn > kMaxLog) return mul_split_dev(a, la, b, lb, h, lh, p, st);
     const long long n = 1ll << logn;
     const int dev = current_device();
     ensure_kernel_attrs();

@@ -10,12 +10,18 @@ constexpr int kMaxSmallLog = 14;  // largest single-CTA product (2 x 64 KiB of s
 constexpr int kMaxColLog = 11;    // 16-column tile of 2^11 rows = 136 KiB of shared memory
 constexpr int kMaxRowLog = 14;
 constexpr int kMinRowLog = 6;
-constexpr int kMaxLog = 24;        // largest product transform (2^24)
+constexpr int kMaxLog = 25;        // largest transform of the three-pass kernels (2^11 x 2^14)
+constexpr int kMaxSplitLog = 29;   // longer single products and transforms, up to the prime's 2-adic
+                                   // order (at most 29 for p < 2^30), are split into 2^25 pieces
 constexpr int kDefaultColLog = 10;  // column length of the default split (rows of 2^14)
 
 // workspace slots (runtime.cuh: workspace)
 enum WsSlot { kWsSingle = 0, kWsBatch = 1, kWsStage = 2, kWsNtt = 3, kWsTwoConv = 4, kWsServer = 5,
-              kWsBiv = 6, kWsBivHost = 7, kWsBig = 8 };
+              kWsBiv = 6, kWsBivHost = 7, kWsBig = 8, kWsSplitProd = 9, kWsSplitIn = 10,
+              kWsSplitNtt = 11 /* + (k - kMaxLog - 1) for a 2^k transform */ };
+
+// SMs of device dev (cached per device).
+int sm_count(int dev);
 
 // Transform length log2 for a product of la and lb coefficients.
 int product_logn(long long la, long long lb);
@@ -45,6 +51,10 @@ size_t direct_job_bytes(int count);
 int direct_batch(int count, const u32* const* a, const long long* la, const u32* const* b, const long long* lb,
                  u32* const* h, const long long* lh, u32 p, u32* ws, void* djobs, void* hjobs,
                  cudaStream_t st, bool allow_tuning);
+
+// Device words of workspace a single product of transform length 2^logn
+// takes (mul_dev), beside its operands and result.
+size_t mul_ws_words(int logn);
 
 // h[0..lh) = a[0..la) * b[0..lb) mod p on device pointers, on stream st.
 int mul_dev(const u32* a, long long la, const u32* b, long long lb, u32* h, long long lh, u32 p,

@@ -65,7 +65,9 @@ unsigned int global_memory_in_bytes(void);
 /* Replaces src/modpn.cu:103-108. */
 float global_memory_in_megabytes(void);
 /* Replaces src/modpn.cu:113-126: nonzero when a product of degrees df, dg
- * fits this library's transform limits and the device's memory. */
+ * fits this library's transform limits (2^29; the prime's 2-adic order is
+ * checked by the product itself, as the reference's stockham path leaves it
+ * to the caller) and the device's memory. */
 int can_call_fftmul_uni(sfixn df, sfixn dg);
 /* Replace src/modpn.cu:142-173.  The subresultant GPU path is not part of
  * this library: always 0, so modpn keeps its CPU subresultant code. */
@@ -79,7 +81,8 @@ int can_call_subres3(sfixn dx, sfixn dy, sfixn d1, sfixn d2);
  * or a w that is not a primitive n-th root return CUMODP_ASSUMPTION_ERROR;
  * n above the prime's 2-adic order returns CUMODP_FFT_SIZE_TOO_LARGE (the
  * reference computes garbage); n < 256 is supported (the reference's grid
- * arithmetic breaks below k = 8). */
+ * arithmetic breaks below k = 8).  n up to 2^25 runs as one four-step
+ * transform; longer ones take one radix-2 step over HBM first. */
 cumodp_err cumodp_fft_uni(sfixn *X, sfixn n, sfixn k, sfixn w, sfixn p);
 /* Inverse: DFT with w^-1 then scaling by n^-1.  Replaces src/modpn.cu:197-210
  * (inverse_stockham_host, src/stockham.cu:489-503). */
@@ -93,6 +96,9 @@ cumodp_err cumodp_invfft_bivariate(sfixn *X, sfixn em, sfixn wm, sfixn en, sfixn
 /* H = F * G mod p: F has df+1 coefficients, G dg+1, H receives dh+1 words.
  * Replaces src/modpn.cu:249-261 (stockham_poly_mul_host, src/stockham.cu:
  * 562-611).  H may alias F or G (modpn multiplies in place, FMUL.c:1949).
+ * Every transform length up to the prime's 2-adic order is computed: up to
+ * 2^25 directly, beyond that as 2^25-point products of 2^24-coefficient
+ * pieces added at their offsets.
  * Deviations (documented fixes): every size is computed (the reference
  * returns SUCCESS with H untouched below transform size 256); exactly dh+1
  * words are written, zero beyond df+dg (the reference writes 2^ceil(log2
@@ -155,7 +161,9 @@ cumodp_err cumodp_fftmul_uni_dev_noalloc(sfixn lh, sfixn *H, sfixn df, const sfi
  * h_off, df, dg are HOST arrays of length count; F, G, H are DEVICE
  * pointers.  Products are grouped by transform size and run as one
  * CUDA-graph launch; the plan (grouping, job tables, workspace) is cached
- * per batch shape.  stream: 0 = library stream, then synchronised. */
+ * per batch shape.  Transforms up to 2^25 (CUMODP_FFT_SIZE_TOO_LARGE beyond:
+ * longer products go through cumodp_fftmul_uni_dev).  stream: 0 = library
+ * stream, then synchronised. */
 cumodp_err cumodp_fftmul_batch_dev(int count, const sfixn *df, const int64_t *f_off, const sfixn *F,
                                    const sfixn *dg, const int64_t *g_off, const sfixn *G,
                                    const int64_t *h_off, sfixn *H, sfixn p, void *stream);

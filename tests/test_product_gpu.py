@@ -107,6 +107,59 @@ def test_c2_product_2_24(cm, oracle_mod):
     assert np.array_equal(got, want)
 
 
+def test_product_2_25(cm, oracle_mod):
+    """Transform 2^25, the longest of the three-pass kernels (2^11-row columns x 2^14-word rows);
+    the same product through the batch entry, beside a small one."""
+    r = SplitMix64(0xC0DA0025)
+    a, b = _rand(r, (1 << 24) + 5, P0), _rand(r, (1 << 24) - 77, P0)
+    want = oracle_mod.polymul(a, b, P0)
+    assert np.array_equal(cm.fftmul_uni(a, b, P0), want)
+    c, d = _rand(r, 300, P0), _rand(r, 1000, P0)
+    got = cm.fftmul_batch([(a, b), (c, d)], P0)
+    assert np.array_equal(got[0], want)
+    assert np.array_equal(got[1], oracle_mod.polymul_school(c, d, P0))
+
+
+def test_split_product_2_26(cm, oracle_mod):
+    """Transform 2^26 (the 2-adic order of 469762049): beyond the three-pass kernels' 2^25 the
+    operands are cut into 2^24-coefficient pieces whose pairwise products are added at their
+    offsets.  Full length, truncated inside a piece, zero fill past the product, and H over F
+    through the device entry."""
+    import torch
+
+    r = SplitMix64(0xC0DA0026)
+    la, lb = (1 << 25) - 3, (1 << 25) - 1000
+    a, b = _rand(r, la, P0), _rand(r, lb, P0)
+    want = oracle_mod.polymul(a, b, P0)
+    assert len(want) > 1 << 25
+    assert np.array_equal(cm.fftmul_uni(a, b, P0), want)
+    dh = (1 << 24) + 12345
+    assert np.array_equal(cm.fftmul_uni(a, b, P0, dh=dh), want[:dh + 1])
+    got = cm.fftmul_uni(a, b, P0, dh=len(want) + 98)
+    assert np.array_equal(got[:len(want)], want) and not got[len(want):].any()
+    lh = (1 << 25) + 4321
+    buf = torch.zeros(max(la, lh), dtype=torch.int32, device="cuda")
+    buf[:la] = torch.from_numpy(a.view(np.int32)).cuda()
+    g = torch.from_numpy(b.view(np.int32)).cuda()
+    cm.fftmul_uni_dev(buf.data_ptr(), lh, buf.data_ptr(), la - 1, g.data_ptr(), lb - 1, P0)
+    torch.cuda.synchronize()
+    assert np.array_equal(buf[:lh].cpu().numpy().view(np.uint32), want[:lh])
+
+
+def test_split_product_unbalanced(cm):
+    """A long operand times a short one past 2^25 (three pieces of the long operand against one of
+    the short): equal to the sum of two three-pass products, a_lo * b + x^m (a_hi * b)."""
+    r = SplitMix64(0xC0DA0027)
+    m = (1 << 25) - 1000  # a[:m] * b and a[m:] * b stay within 2^25
+    a, b = _rand(r, (1 << 25) + 9, P0), _rand(r, 700, P0)
+    assert len(a) + len(b) - 1 > 1 << 25
+    lo, hi = cm.fftmul_uni(a[:m], b, P0), cm.fftmul_uni(a[m:], b, P0)
+    want = np.zeros(len(a) + len(b) - 1, dtype=np.uint64)
+    want[:len(lo)] += lo
+    want[m:m + len(hi)] += hi
+    assert np.array_equal(cm.fftmul_uni(a, b, P0), (want % P0).astype(np.uint32))
+
+
 @pytest.mark.parametrize("da,db,dh", [(100, 50, 20), (100, 50, 150), (100, 50, 400), (4095, 4095, 9000),
                                       (20000, 20000, 100), (20000, 20000, 70000)])
 def test_output_length_contract(cm, oracle_mod, da, db, dh):

@@ -39,6 +39,19 @@ def test_fft_uni_2_24_round_trip(cm, oracle_mod):
     assert np.array_equal(cm.invfft_uni(got, w, P0), x)
 
 
+@pytest.mark.parametrize("k", [25, 26])
+def test_fft_uni_beyond_2_24(cm, oracle_mod, k):
+    """2^25: the four-step kernels with 2^11-row columns; 2^26 (the 2-adic order of 469762049): one
+    radix-2 step over HBM, two 2^25 transforms and an interleave.  Forward vs oracle, inverse
+    round trip (the inverse's 2^-26 is applied in the split step)."""
+    r = SplitMix64(0xC0DA0000 + k)
+    x = r.residues(1 << k, P0)
+    w = oracle_mod.primitive_root(k, P0)
+    got = cm.fft_uni(x, w, P0)
+    assert np.array_equal(got, oracle_mod.ntt(x, w, P0))
+    assert np.array_equal(cm.invfft_uni(got, w, P0), x)
+
+
 def test_uni_fft_tst_identity(cm, oracle_mod):
     """The reference's self-test uni_fft_tst (src/modpn.cu:416-449): X[i] = i, FFT then inverse = identity."""
     for k in (8, 12, 16):
