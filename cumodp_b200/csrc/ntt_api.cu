@@ -482,6 +482,51 @@ int list_ntt_dev(u32* x, long long m, int k, u32 w, u32 p, bool inverse, cudaStr
     return OK;
 }
 
+namespace {
+
+// out[c * rows + r] = in[r * cols + c]: 32 x 32 tiles through shared memory,
+// bounds-checked.  blockIdx.x runs over the longer side (rows_on_x), so any
+// shape with rows * cols <= 2^30 fits the grid (the shorter side is then at
+// most 2^15 long).
+__global__ void k_transpose_long(const u32* __restrict__ in, u32* __restrict__ out, long long rows, long long cols,
+                                 int rows_on_x) {
+    __shared__ u32 t[32][33];
+    const long long r0 = 32ll * (rows_on_x ? blockIdx.x : blockIdx.y);
+    const long long c0 = 32ll * (rows_on_x ? blockIdx.y : blockIdx.x);
+    for (int y = threadIdx.y; y < 32; y += blockDim.y)
+        if (r0 + y < rows && c0 + threadIdx.x < cols) t[y][threadIdx.x] = in[(r0 + y) * cols + c0 + threadIdx.x];
+    __syncthreads();
+    for (int y = threadIdx.y; y < 32; y += blockDim.y)
+        if (c0 + y < cols && r0 + threadIdx.x < rows) out[(c0 + y) * rows + r0 + threadIdx.x] = t[threadIdx.x][y];
+}
+
+void transpose_long(const u32* in, u32* out, long long rows, long long cols, cudaStream_t st) {
+    const unsigned tr = (unsigned)((rows + 31) / 32), tc = (unsigned)((cols + 31) / 32);
+    const bool rx = tr >= tc;
+    k_transpose_long<<<rx ? dim3(tr, tc) : dim3(tc, tr), dim3(32, 8), 0, st>>>(in, out, rows, cols, rx ? 1 : 0);
+}
+
+// A 2-D transform past the fused path's limits (columns longer than
+// 2^kMaxColLog or rows longer than 2^kMaxRowLog): the rows as a list
+// transform in place, then the columns as a list transform of the
+// transposed array, transposed back.  Each list transform applies its own
+// inverse scaling (2^-en, 2^-em).
+int bivariate_general(u32* x, int em, u32 wm, int en, u32 wn, u32 p, bool inverse, cudaStream_t st) {
+    int err = OK;
+    if (em + en > 30) return FFT_SIZE_TOO_LARGE;
+    const long long rows = 1ll << em, cols = 1ll << en;
+    if ((err = list_ntt_dev(x, rows, en, wn, p, inverse, st)) != OK) return err;
+    if (em == 0) return OK;
+    u32* t = (u32*)workspace(current_device(), kWsBivT, (size_t)(rows * cols) * sizeof(u32), &err);
+    if (!t) return err;
+    transpose_long(x, t, rows, cols, st);
+    if ((err = list_ntt_dev(t, cols, em, wm, p, inverse, st)) != OK) return err;
+    transpose_long(t, x, cols, rows, st);
+    return cuda_err(cudaGetLastError());
+}
+
+}  // namespace
+
 // 2-D DFT of a row-major 2^em x 2^en array, in place.
 int bivariate_dev(u32* x, int em, u32 wm, int en, u32 wn, u32 p, bool inverse, cudaStream_t st) {
     int err = OK;
@@ -492,7 +537,7 @@ int bivariate_dev(u32* x, int em, u32 wm, int en, u32 wn, u32 p, bool inverse, c
     if (em > pc->info.two_adic || en > pc->info.two_adic) return FFT_SIZE_TOO_LARGE;
     if (!root_has_order(wm, em, p) || !root_has_order(wn, en, p)) return ASSUMPTION_ERROR;
     if (en < 6) return FFT_SIZE_TOO_SMALL;
-    if (en > kMaxRowLog || em > kMaxColLog) return FFT_SIZE_TOO_LARGE;
+    if (en > kMaxRowLog || em > kMaxColLog) return bivariate_general(x, em, wm, en, wn, p, inverse, st);
     const int dev = current_device();
     const u32 rm = inverse ? inv_of(wm, p) : wm, rn = inverse ? inv_of(wn, p) : wn;
     const u32 sc = inverse ? inv_of((u32)((1ull << (em + en)) % p), p) : 1u;
@@ -518,18 +563,6 @@ int bivariate_dev(u32* x, int em, u32 wm, int en, u32 wn, u32 p, bool inverse, c
     A.src = w1;
     kRowNtt[en](A, 1 << em, st);
     return cuda_err(cudaGetLastError());
-}
-
-// out[c * rows + r] = in[r * cols + c] for any shape: 32 x 32 tiles through
-// shared memory, bounds-checked.
-__global__ void k_transpose_any(const u32* __restrict__ in, u32* __restrict__ out, int rows, int cols) {
-    __shared__ u32 t[32][33];
-    const long long c0 = (long long)blockIdx.x * 32, r0 = (long long)blockIdx.y * 32;
-    for (int y = threadIdx.y; y < 32; y += blockDim.y)
-        if (r0 + y < rows && c0 + threadIdx.x < cols) t[y][threadIdx.x] = in[(r0 + y) * cols + c0 + threadIdx.x];
-    __syncthreads();
-    for (int y = threadIdx.y; y < 32; y += blockDim.y)
-        if (c0 + y < cols && r0 + threadIdx.x < rows) out[(c0 + y) * rows + r0 + threadIdx.x] = t[threadIdx.x][y];
 }
 
 // a[i] = a[i] * b[i] mod p (inputs in [0, p)).
@@ -581,19 +614,16 @@ int bivariate_mul_dev(u32* F, u32* G, int em, int en, u32 p, cudaStream_t st) {
     u32* ws = (u32*)workspace(dev, kWsBiv, (size_t)2 * tpad * sizeof(u32), &err);
     if (!ws) return err;
     u32 *W1 = ws, *W2 = ws + tpad;
-    const dim3 tb(32, 8);
-    const dim3 g_mn((unsigned)((n + 31) / 32), (unsigned)((m + 31) / 32));  // m rows x n columns
-    const dim3 g_nm((unsigned)((m + 31) / 32), (unsigned)((n + 31) / 32));  // n rows x m columns
     u32* src[2] = {F, G};
     u32* spec[2] = {W1, W2};
     for (int o = 0; o < 2; ++o) {
         if ((err = list_ntt_dev(src[o], m, en, wn, p, false, st)) != OK) return err;
-        k_transpose_any<<<g_mn, tb, 0, st>>>(src[o], spec[o], (int)m, (int)n);
+        transpose_long(src[o], spec[o], m, n, st);
         if ((err = list_ntt_dev(spec[o], n, em, wm, p, false, st)) != OK) return err;
     }
     k_pointwise_mod<<<grid_for(total), 256, 0, st>>>(W1, W2, total, p);
     if ((err = list_ntt_dev(W1, n, em, wm, p, true, st)) != OK) return err;
-    k_transpose_any<<<g_nm, tb, 0, st>>>(W1, F, (int)n, (int)m);
+    transpose_long(W1, F, n, m, st);
     if ((err = list_ntt_dev(F, m, en, wn, p, true, st)) != OK) return err;
     return cuda_err(cudaGetLastError());
 }

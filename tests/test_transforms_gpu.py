@@ -67,8 +67,11 @@ def test_fft_uni_rejects_bad_root(cm):
     assert e.value.code == cm.ASSUMPTION_ERROR
 
 
-@pytest.mark.parametrize("em,en", [(0, 6), (1, 6), (3, 8), (8, 8), (5, 10), (10, 12), (6, 14)])
+@pytest.mark.parametrize("em,en", [(0, 6), (1, 6), (3, 8), (8, 8), (5, 10), (10, 12), (6, 14),
+                                   (12, 6), (13, 7), (16, 6), (6, 15), (3, 17)])
 def test_bivariate_matches_row_column_dft(cm, oracle_mod, em, en):
+    """Columns up to 2^11 and rows up to 2^14 run fused (column pass + row pass); longer ones as
+    list transforms of the rows and of the transposed columns."""
     p = P0
     r = SplitMix64(em * 100 + en)
     X = r.residues(1 << (em + en), p).reshape(1 << em, 1 << en)
