@@ -90,7 +90,10 @@ cumodp_err cumodp_invfft_uni(sfixn *X, sfixn n, sfixn k, sfixn w, sfixn p);
 /* 2-D DFT of a row-major 2^em x 2^en array X: w_m-DFT down the columns
  * (length 2^em) and w_n-DFT along the rows (length 2^en).  Replaces
  * src/modpn.cu:215-244 (bivariate_stockham_host, src/list_stockham.cu).
- * Deviation: em != en is computed correctly (the reference is square-only). */
+ * Deviation: em != en is computed correctly (the reference is square-only).
+ * Rows of 2^6 words or more, em + en <= 30; columns up to 2^11 with rows up to
+ * 2^14 run as one column pass and one row pass, larger shapes as row
+ * transforms and transposed column transforms. */
 cumodp_err cumodp_fft_bivariate(sfixn *X, sfixn em, sfixn wm, sfixn en, sfixn wn, sfixn p);
 cumodp_err cumodp_invfft_bivariate(sfixn *X, sfixn em, sfixn wm, sfixn en, sfixn wn, sfixn p);
 /* H = F * G mod p: F has df+1 coefficients, G dg+1, H receives dh+1 words.
