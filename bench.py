@@ -20,7 +20,9 @@ Printed JSON line (rank 0):
                HBM copy bandwidth
   cpu_baseline modpn's own FFT multiply (the reference CPU path) on the host
   extras       2^24-point forward+inverse transform GB/s; the batched
-               mixed-degree workload (4096 pairs) against one call per pair
+               mixed-degree workload (4096 pairs) against one call per pair;
+               the list transform, the 2-D transform, the bivariate product
+               and a subproduct-tree level, each with its own check
 
 --impl reference runs the reference's CPU implementation of the same path
 (modpn EX_Mont_FFTMul, compiled from the reference sources into
@@ -417,6 +419,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         extras["c3_exact_int64"] = c3_exact(cm, torch, dev, stream)
         extras["big_1024bit_1024terms"] = big_coefficients(cm, torch, dev, stream)
         extras["serving_c5"] = serving_c5(cm)
+        extras["list_and_bivariate"] = list_and_bivariate(cm, torch, dev, stream, hbm_peak)
     cpu = None
     if rank == 0 and world == 1 and not args.no_extras:
         cpu = cpu_baseline()
@@ -473,6 +476,112 @@ def ntt_2_24(cm, torch, dev, stream, hbm_peak):
             "frac_bio": round(bio / (ms / 1000) / 1e9 / hbm_peak, 4),
             "gbs_strict_8n": round(8 * n / (ms / 1000) / 1e9, 1), "per_pass": per_pass,
             "round_trip_bit_exact": round_trip_ok}
+
+
+def _timed(torch, stream, fn, reps: int = 10, warm: int = 2) -> float:
+    """Mean ms of fn() over reps calls on stream (CUDA events), after warm calls."""
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def list_and_bivariate(cm, torch, dev, stream, hbm_peak):
+    """The list transform, the 2-D transform, the bivariate product and a subproduct-tree level on
+    resident operands larger than L2, each with a bit-exact check.  GB/s are on the algorithmic
+    bytes: one HBM round trip (8 bytes a word) per pass the kernels need."""
+    from cumodp_b200.workloads import SplitMix64
+    r = SplitMix64(0xC0DA0F00)
+    sp = stream.cuda_stream
+    out = {}
+
+    def rate(nbytes, ms):
+        gbs = nbytes / (ms / 1000) / 1e9
+        return round(gbs, 1), round(gbs / hbm_peak, 4)
+
+    # list transform: 2^13 rows of 2^12 words (128 MiB), one CTA per row -> one pass
+    m, k = 1 << 13, 12
+    x = r.residues(m << k, P)
+    dx = torch.from_numpy(x.view(np.int32)).to(dev)
+    w = pow(3, (P - 1) >> k, P)
+
+    def lst():
+        cm.list_fft_dev(dx.data_ptr(), m, k, w, P, False, sp)
+        cm.list_fft_dev(dx.data_ptr(), m, k, w, P, True, sp)
+    ms = _timed(torch, stream, lst) / 2
+    gbs, frac = rate(8 * (m << k), ms)
+    out["list_fft_2^13x2^12"] = {"ms_per_transform": round(ms, 5), "gbs": gbs, "frac": frac,
+                                 "round_trip_bit_exact": bool(np.array_equal(dx.cpu().numpy().view(np.uint32), x))}
+    del dx
+    # 2-D transform: 2^11 x 2^14 (128 MiB): column pass + row pass
+    em, en = 11, 14
+    x = r.residues(1 << (em + en), P)
+    dx = torch.from_numpy(x.view(np.int32)).to(dev)
+    wm, wn = pow(3, (P - 1) >> em, P), pow(3, (P - 1) >> en, P)
+
+    def biv():
+        cm.fft_bivariate_dev(dx.data_ptr(), em, wm, en, wn, P, False, sp)
+        cm.fft_bivariate_dev(dx.data_ptr(), em, wm, en, wn, P, True, sp)
+    ms = _timed(torch, stream, biv) / 2
+    gbs, frac = rate(16 << (em + en), ms)
+    out["bivariate_fft_2^11x2^14"] = {"ms_per_transform": round(ms, 5), "gbs_bio": gbs, "frac_bio": frac,
+                                      "round_trip_bit_exact": bool(np.array_equal(dx.cpu().numpy().view(np.uint32), x))}
+    del dx
+    # bivariate product on a 2^12 x 2^12 grid: operands of 2^11 x 2^11 coefficients, zero padded
+    em = en = 12
+    half = 1 << (em - 1)
+    fa = np.zeros((1 << em, 1 << en), dtype=np.uint32)
+    ga = np.zeros_like(fa)
+    fa[:half, :half] = r.residues(half * half, P).reshape(half, half)
+    ga[:half, :half] = r.residues(half * half, P).reshape(half, half)
+    dF = torch.from_numpy(fa.view(np.int32)).to(dev)
+    dG = torch.from_numpy(ga.view(np.int32)).to(dev)
+    tF, tG = torch.empty_like(dF), torch.empty_like(dG)
+
+    def bmul():
+        tF.copy_(dF)
+        tG.copy_(dG)
+        cm.bivariate_mul_dev(em, en, tF.data_ptr(), tG.data_ptr(), P, sp)
+    with torch.cuda.stream(stream):
+        ms = _timed(torch, stream, bmul)
+    h = tF.cpu().numpy().view(np.uint32)
+    x0, y0 = 987654321 % P, 192837465 % P
+    px, py = powers_mod(x0, 1 << en), powers_mod(y0, 1 << em)
+
+    def ev(a):
+        rows = [eval_mod(a[j], px) for j in range(a.shape[0])]
+        return eval_mod(np.array(rows, dtype=np.uint64), py[:len(rows)])
+    ok = ev(h) == ev(fa) * ev(ga) % P
+    n2 = 1 << (em + en)
+    out["bivariate_mul_2^12x2^12"] = {"ms_per_product_incl_operand_copies": round(ms, 5),
+                                      "products_per_s": round(1000 / ms, 1),
+                                      "gbs_strict_12N": rate(12 * n2, ms)[0], "eval_point_identity": bool(ok)}
+    del dF, dG, tF, tG
+    # subproduct-tree level: 2^16 monic polynomials of degree 512 -> 2^15 products of degree 1024
+    l, npairs = 512, 1 << 15
+    mi = r.residues(2 * npairs * l, P)
+    dI = torch.from_numpy(mi.view(np.int32)).to(dev)
+    dO = torch.empty(2 * npairs * l, dtype=torch.int32, device=dev)
+    ms = _timed(torch, stream, lambda: cm.subproduct_level_dev(l, npairs, dI.data_ptr(), dO.data_ptr(), P, sp))
+    mo = dO.cpu().numpy().view(np.uint32)
+    ok = True
+    for j in (0, npairs - 1):
+        a = np.append(mi[2 * j * l:(2 * j + 1) * l], 1).astype(np.uint32)
+        b = np.append(mi[(2 * j + 1) * l:(2 * j + 2) * l], 1).astype(np.uint32)
+        ok = ok and np.array_equal(cm.fftmul_uni(a, b, P)[:2 * l], mo[2 * j * l:2 * (j + 1) * l])
+    gbs, frac = rate(16 * npairs * l, ms)
+    out["subproduct_level_l512_x32768"] = {"ms": round(ms, 5), "pairs_per_s": round(npairs / (ms / 1000), 1),
+                                          "gbs_strict": gbs, "frac_strict": frac,
+                                          "equals_single_products": bool(ok)}
+    del dI, dO
+    return out
 
 
 def batched_c4(cm, torch, dev, stream):

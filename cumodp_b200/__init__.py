@@ -103,6 +103,9 @@ def _lib():
         L.cumodp_fft_uni_dev.restype = C.c_int
         L.cumodp_fft_uni_dev.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int,
                                          C.c_void_p]
+        L.cumodp_fft_bivariate_dev.restype = C.c_int
+        L.cumodp_fft_bivariate_dev.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                               C.c_int, C.c_void_p]
         L.cumodp_list_fft_dev.restype = C.c_int
         L.cumodp_list_fft_dev.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int,
                                           C.c_void_p]
@@ -318,6 +321,13 @@ def fft_uni_dev(x_ptr: int, k: int, w: int, p: int, inverse: bool = False, strea
     """In-place natural-order transform of 2^k device words (``cumodp_fft_uni_dev``)."""
     _check(_lib().cumodp_fft_uni_dev(x_ptr, 1 << k, k, w, p, int(inverse), stream or None),
            "cumodp_fft_uni_dev")
+
+
+def fft_bivariate_dev(x_ptr: int, em: int, wm: int, en: int, wn: int, p: int, inverse: bool = False,
+                      stream: int = 0) -> None:
+    """In-place 2-D transform of a 2^em x 2^en device array (``cumodp_fft_bivariate_dev``)."""
+    _check(_lib().cumodp_fft_bivariate_dev(x_ptr, em, wm, en, wn, p, int(inverse), stream or None),
+           "cumodp_fft_bivariate_dev")
 
 
 def list_fft_dev(x_ptr: int, m: int, k: int, w: int, p: int, inverse: bool = False, stream: int = 0) -> None:

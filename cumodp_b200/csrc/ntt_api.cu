@@ -725,6 +725,21 @@ cumodp_err cumodp_fft_uni_dev(sfixn* X, sfixn n, sfixn k, sfixn w, sfixn p, int 
     return (cumodp_err)e;
 }
 
+cumodp_err cumodp_fft_bivariate_dev(sfixn* X, sfixn em, sfixn wm, sfixn en, sfixn wn, sfixn p, int inverse,
+                                    void* stream) {
+    int cnt = 0;
+    if (cudaGetDeviceCount(&cnt) != cudaSuccess || cnt == 0) {
+        cudaGetLastError();
+        return CUMODP_NO_CUDA_DEVICE;
+    }
+    if (!X || em < 0 || en < 0 || em + en > 30 || p <= 0) return CUMODP_ASSUMPTION_ERROR;
+    std::lock_guard<std::mutex> g(lib_mutex());
+    cudaStream_t st = stream ? (cudaStream_t)stream : lib_stream(current_device());
+    int e = bivariate_dev((u32*)X, em, (u32)wm, en, (u32)wn, (u32)p, inverse != 0, st);
+    if (e == OK && !stream) e = cuda_err(cudaStreamSynchronize(st));
+    return (cumodp_err)e;
+}
+
 cumodp_err cumodp_list_fft_dev(sfixn* X, sfixn m, sfixn k, sfixn w, sfixn p, int inverse, void* stream) {
     int cnt = 0;
     if (cudaGetDeviceCount(&cnt) != cudaSuccess || cnt == 0) {

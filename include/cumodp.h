@@ -276,6 +276,16 @@ void cumodp_server_destroy(cumodp_server *s);
  * 16-byte aligned (as cudaMalloc returns) when k >= 6. */
 cumodp_err cumodp_fft_uni_dev(sfixn *X, sfixn n, sfixn k, sfixn w, sfixn p, int inverse, void *stream);
 
+/* Addition.  Device-pointer 2-D transform on a caller stream (0 = the
+ * library's stream, then synchronised): cumodp_fft_bivariate, or
+ * cumodp_invfft_bivariate when `inverse` is nonzero, in place on the DEVICE
+ * array X (16-byte aligned).  Counterpart of the reference's C++
+ * bivariate_stockham_dev / inverse_bivariate_stockham_dev
+ * (src/list_stockham.cu:1161-1204, 1251-1263), given the roots wm, wn
+ * instead of their power tables. */
+cumodp_err cumodp_fft_bivariate_dev(sfixn *X, sfixn em, sfixn wm, sfixn en, sfixn wn, sfixn p, int inverse,
+                                    void *stream);
+
 /* Addition.  The list transform I_m (x) DFT_n: m independent natural-order
  * transforms of length n = 2^k of the DEVICE array X (row i at X + i n), in
  * place, root w (inverse: w^-1 and scaling by n^-1); X 16-byte aligned when

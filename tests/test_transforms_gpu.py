@@ -84,3 +84,21 @@ def test_bivariate_matches_row_column_dft(cm, oracle_mod, em, en):
     assert np.array_equal(got, want)
     back = cm.fft_bivariate(got, em, wm, en, wn, p, inverse=True).reshape(X.shape)
     assert np.array_equal(back, X)
+
+
+@pytest.mark.parametrize("em,en", [(4, 8), (11, 14), (12, 6)])
+def test_fft_bivariate_dev_equals_host_entry(cm, em, en):
+    """The device-pointer 2-D transform gives the host entry's result, forward and inverse."""
+    import torch
+
+    r = SplitMix64(em * 1000 + en)
+    x = r.residues(1 << (em + en), P0)
+    wm, wn = pow(3, (P0 - 1) >> em, P0), pow(3, (P0 - 1) >> en, P0)
+    want = cm.fft_bivariate(x, em, wm, en, wn, P0)
+    d = torch.from_numpy(x.view(np.int32)).cuda()
+    cm.fft_bivariate_dev(d.data_ptr(), em, wm, en, wn, P0)
+    torch.cuda.synchronize()
+    assert np.array_equal(d.cpu().numpy().view(np.uint32), want.reshape(-1))
+    cm.fft_bivariate_dev(d.data_ptr(), em, wm, en, wn, P0, inverse=True)
+    torch.cuda.synchronize()
+    assert np.array_equal(d.cpu().numpy().view(np.uint32), x)
