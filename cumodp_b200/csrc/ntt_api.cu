@@ -565,10 +565,12 @@ int bivariate_dev(u32* x, int em, u32 wm, int en, u32 wn, u32 p, bool inverse, c
     return cuda_err(cudaGetLastError());
 }
 
-// a[i] = a[i] * b[i] mod p (inputs in [0, p)).
-__global__ void k_pointwise_mod(u32* __restrict__ a, const u32* __restrict__ b, long long n, u32 p) {
+// a[i] = a[i] * b[i] mod p (inputs in [0, p)): a Montgomery product
+// (a b 2^-32) times r2 = 2^64 mod p by a second one, then one reduction.
+__global__ void k_pointwise_mod(u32* __restrict__ a, const u32* __restrict__ b, long long n, u32 p, u32 pinv_neg,
+                                u32 r2) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        a[i] = (u32)(((u64)a[i] * b[i]) % p);
+        a[i] = red1(mul_mont(mul_mont(a[i], b[i], p, pinv_neg), r2, p, pinv_neg), p);
 }
 
 // dst (2^ey2 rows of 2^ex2) = src (ny1 rows of nx1) zero-padded, reduced mod p.
@@ -596,7 +598,9 @@ int grid_for(long long n) { return (int)std::max<long long>(1, std::min<long lon
 
 // F <- DFT^-1(DFT F * DFT G) on a 2^em x 2^en row-major grid (rows: y, of
 // length 2^en in x): the 2-D cyclic convolution, i.e. the bivariate product
-// when both operands are zero-padded to the product's size.  Row transforms,
+// when both operands are zero-padded to the product's size.  Grids within
+// the fused 2-D transform's limits use it (column pass + row pass per
+// transform).  Otherwise: row transforms,
 // a transpose, column transforms (as rows) give both spectra in transposed
 // order; the pointwise product and the inverse steps run in that order, so
 // nothing is permuted back before the last transpose.  G is overwritten.
@@ -609,6 +613,14 @@ int bivariate_mul_dev(u32* F, u32* G, int em, int en, u32 p, cudaStream_t st) {
     if (em > pc->info.two_adic || en > pc->info.two_adic || em + en > 30) return FFT_SIZE_TOO_LARGE;
     const long long m = 1ll << em, n = 1ll << en, total = m * n;
     const u32 wm = em ? canonical_root(*pc, em) : 1u, wn = en ? canonical_root(*pc, en) : 1u;
+    if (en >= 6 && en <= kMaxRowLog && em <= kMaxColLog) {
+        // grids the fused 2-D transform covers: two passes per transform, no transposes
+        if ((err = bivariate_dev(F, em, wm, en, wn, p, false, st)) != OK) return err;
+        if ((err = bivariate_dev(G, em, wm, en, wn, p, false, st)) != OK) return err;
+        k_pointwise_mod<<<grid_for(total), 256, 0, st>>>(F, G, total, p, pc->info.pinv_neg, pc->info.r2);
+        if ((err = bivariate_dev(F, em, wm, en, wn, p, true, st)) != OK) return err;
+        return cuda_err(cudaGetLastError());
+    }
     const int dev = current_device();
     const long long tpad = (total + 3) & ~3ll;  // 16-byte aligned halves
     u32* ws = (u32*)workspace(dev, kWsBiv, (size_t)2 * tpad * sizeof(u32), &err);
@@ -621,7 +633,7 @@ int bivariate_mul_dev(u32* F, u32* G, int em, int en, u32 p, cudaStream_t st) {
         transpose_long(src[o], spec[o], m, n, st);
         if ((err = list_ntt_dev(spec[o], n, em, wm, p, false, st)) != OK) return err;
     }
-    k_pointwise_mod<<<grid_for(total), 256, 0, st>>>(W1, W2, total, p);
+    k_pointwise_mod<<<grid_for(total), 256, 0, st>>>(W1, W2, total, p, pc->info.pinv_neg, pc->info.r2);
     if ((err = list_ntt_dev(W1, n, em, wm, p, true, st)) != OK) return err;
     transpose_long(W1, F, n, m, st);
     if ((err = list_ntt_dev(F, m, en, wn, p, true, st)) != OK) return err;
