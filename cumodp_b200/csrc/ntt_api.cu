@@ -16,6 +16,7 @@
 // directly in natural order.
 #include <algorithm>
 #include <cstring>
+#include <vector>
 
 #include "../../include/cumodp.h"
 #include "product.cuh"
@@ -34,6 +35,7 @@ struct RowNttArgs {
     Tw scale;                       // applied to every output
     int rows_in_place;              // 1: independent rows, row s written to dst row s
     const Tw* __restrict__ rowtab;  // per-slot level-0 factor tables (RowTab, forward direction), or nullptr
+    long long job_stride;           // words between the transforms of grid row blockIdx.y (list transforms)
 };
 
 __device__ __forceinline__ u32 seed_mont_at(const u32* __restrict__ seeds, int nlo, u32 e, u32 p, u32 pinv) {
@@ -72,7 +74,8 @@ __global__ void __launch_bounds__(ntt_row_threads(L2), ntt_row_ctas(L2)) k_row_n
     using RT = RowTab<L2>;
     const bool tabbed = RT::USE && twid && A.rowtab;
     Tw* tab = reinterpret_cast<Tw*>(sm + n2);
-    row_load_issue<L2, T>(sm, A.src + (size_t)s * n2);
+    const size_t joff = (size_t)blockIdx.y * (size_t)A.job_stride;
+    row_load_issue<L2, T>(sm, A.src + joff + (size_t)s * n2);
     if (tabbed) {
         const Tw* src = A.rowtab + (size_t)s * RT::TABW;  // forward direction
         for (int i = threadIdx.x; i < RT::TABW / 2; i += T) {
@@ -151,7 +154,7 @@ __global__ void __launch_bounds__(ntt_row_threads(L2), ntt_row_ctas(L2)) k_row_n
         for (int j = 0; j < 32; ++j) sm[swz_nat((int)row_pos_to_freq<L2>((u32)(r * 32 + j)))] = x[j];
     }
     __syncthreads();
-    u32* out = A.dst + (size_t)out_row * n2;
+    u32* out = A.dst + joff + (size_t)out_row * n2;
 #pragma unroll 4
     for (int i = threadIdx.x; i < n2; i += T) out[i] = sm[swz_nat(i)];
 }
@@ -162,6 +165,8 @@ __global__ void __launch_bounds__(ntt_row_threads(L2), ntt_row_ctas(L2)) k_row_n
 __global__ void __launch_bounds__(256) k_transpose64(const u32* __restrict__ in, u32* __restrict__ out, int rows,
                                                      int cols) {
     __shared__ u32 t[64][65];
+    in += (size_t)blockIdx.z * rows * cols;  // transform blockIdx.z of a list
+    out += (size_t)blockIdx.z * rows * cols;
     const size_t c0 = (size_t)blockIdx.x * 64, r0 = (size_t)blockIdx.y * 64;
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     const u32* src = in + r0 * cols + c0 + 4 * tx;
@@ -187,6 +192,8 @@ __global__ void __launch_bounds__(256) k_transpose64(const u32* __restrict__ in,
 // out[c * rows + r] = in[r * cols + c]: 32 x 32 tiles through shared memory.
 __global__ void k_transpose(const u32* __restrict__ in, u32* __restrict__ out, int rows, int cols) {
     __shared__ u32 t[32][33];
+    in += (size_t)blockIdx.z * rows * cols;  // transform blockIdx.z of a list
+    out += (size_t)blockIdx.z * rows * cols;
     const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
     for (int y = threadIdx.y; y < 32; y += blockDim.y)
         t[y][threadIdx.x] = in[(size_t)(r0 + y) * cols + c0 + threadIdx.x];
@@ -215,16 +222,16 @@ __global__ void k_tiny_dft(const u32* __restrict__ x, u32* __restrict__ y, int n
 namespace {
 
 template <int L2>
-void launch_row_ntt_t(const RowNttArgs& a, int rows, cudaStream_t st) {
+void launch_row_ntt_t(const RowNttArgs& a, int rows, cudaStream_t st, int jobs) {
     const size_t smem = (size_t)(1 << L2) * sizeof(u32) + (size_t)RowTab<L2>::TABW * sizeof(Tw);
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_row_ntt<L2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    k_row_ntt<L2><<<rows, ntt_row_threads(L2), smem, st>>>(a);
+    k_row_ntt<L2><<<dim3(rows, jobs), ntt_row_threads(L2), smem, st>>>(a);
 }
-typedef void (*RowNttFn)(const RowNttArgs&, int, cudaStream_t);
+typedef void (*RowNttFn)(const RowNttArgs&, int, cudaStream_t, int);
 const RowNttFn kRowNtt[15] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
                               launch_row_ntt_t<6>, launch_row_ntt_t<7>, launch_row_ntt_t<8>,
                               launch_row_ntt_t<9>, launch_row_ntt_t<10>, launch_row_ntt_t<11>,
@@ -240,7 +247,7 @@ void launch_colfwd1_t(const LargeArgs& a, int tiles, cudaStream_t st) {
                              (int)smem);
         attr = true;
     }
-    k_col_fwd<L1, col_warps(L1, 2), 2><<<dim3(tiles, 1, 1), col_warps(L1, 2) * 32, smem, st>>>(a);
+    k_col_fwd<L1, col_warps(L1, 2), 2><<<dim3(tiles, 1, a.njobs), col_warps(L1, 2) * 32, smem, st>>>(a);
 }
 typedef void (*ColFn)(const LargeArgs&, int, cudaStream_t);
 const ColFn kColFwd1[12] = {nullptr, launch_colfwd1_t<1>, launch_colfwd1_t<2>, launch_colfwd1_t<3>,
@@ -259,7 +266,7 @@ u32 inv_of(u32 a, u32 p) { return powmod_exact(a, p - 2, p); }
 
 // Column pass of a single array (rows of n2 words, 2^l1 rows) into dst.
 int column_pass(const PrimeCtx& pc, u32 root_c, int l1, int l2, const u32* src, long long len, u32* dst,
-                int dev, cudaStream_t st) {
+                int dev, cudaStream_t st, const LargeJob* djobs = nullptr, int njobs = 1) {
     int err = OK;
     const u32 p = pc.info.p;
     const Tw* twc = col_tables(dev, p, root_c, l1, &err);
@@ -273,8 +280,9 @@ int column_pass(const PrimeCtx& pc, u32 root_c, int l1, int l2, const u32* src, 
     A.l2 = l2;
     A.colpl = col_plan(l1);
     A.job0 = LargeJob{src, nullptr, nullptr, (int)std::min<long long>(len, 1ll << 30), 0, 0, 0, dst, nullptr};
-    A.njobs = 1;
-    if (!launch_col_fwd_pipe1(A, 1, st)) kColFwd1[l1](A, (1 << l2) / col_tile_cols_rt(l1, 2), st);
+    A.jobs = djobs;  // a device job table (a list of transforms), or nullptr: job0
+    A.njobs = njobs;
+    if (!launch_col_fwd_pipe1(A, njobs, st)) kColFwd1[l1](A, (1 << l2) / col_tile_cols_rt(l1, 2), st);
     return OK;
 }
 
@@ -395,7 +403,7 @@ int ntt_natural_dev(const u32* x_in, u32* x_out, int k, u32 w, u32 p, bool inver
         A.scale = tw_of(sc, p);
         cudaEvent_t e0;
         const bool tr = pass_timing_begin(st, &e0);
-        kRowNtt[k](A, 1, st);
+        kRowNtt[k](A, 1, st, 1);
         if (tr) pass_timing_end(st, "ntt_row", e0);
         return cuda_err(cudaGetLastError());
     }
@@ -429,7 +437,7 @@ int ntt_natural_dev(const u32* x_in, u32* x_out, int k, u32 w, u32 p, bool inver
         if (large_args(*pc, root, k, l2, dev, &LA) == OK) A.rowtab = LA.rowtab;
     }
     tr = pass_timing_begin(st, &e0);
-    kRowNtt[l2](A, 1 << l1, st);
+    kRowNtt[l2](A, 1 << l1, st, 1);
     if (tr) pass_timing_end(st, "ntt_row", e0);
     tr = pass_timing_begin(st, &e0);
     if (l1 >= 6)
@@ -439,6 +447,68 @@ int ntt_natural_dev(const u32* x_in, u32* x_out, int k, u32 w, u32 p, bool inver
     if (tr) pass_timing_end(st, "ntt_transpose", e0);
     return cuda_err(cudaGetLastError());
 }
+
+namespace {
+
+// m transforms of 2^k words (kMaxSmallLog < k <= kMaxLog), in place: the
+// four-step passes of ntt_natural_dev, each launch covering up to
+// min(2^16 - 1, 2^26 / 2^k) transforms (the column pass reads them from a
+// job table, the row pass and the transpose take them from a grid
+// dimension).  root is already inverted for an inverse transform.
+int list_ntt_four_step(const PrimeCtx& pc, u32* x, long long m, int k, u32 root, u32 sc, cudaStream_t st) {
+    int err = OK;
+    const u32 p = pc.info.p;
+    const int dev = current_device();
+    const int l1 = std::max(5, k - kMaxRowLog), l2 = k - l1;
+    const long long n = 1ll << k;
+    const long long cm = std::min<long long>(m, std::max<long long>(1, std::min<long long>(65535, (1ll << 26) >> k)));
+    u32* ws = (u32*)workspace(dev, kWsNtt, (size_t)2 * cm * n * sizeof(u32), &err);
+    if (!ws) return err;
+    LargeJob* dj = (LargeJob*)workspace(dev, kWsListJobs, (size_t)cm * sizeof(LargeJob), &err);
+    if (!dj) return err;
+    u32 *w1 = ws, *w2 = ws + cm * n;
+    const u32 root_c = powmod_exact(root, 1ull << l2, p), root_r = powmod_exact(root, 1ull << l1, p);
+    RowNttArgs A;
+    memset(&A, 0, sizeof(A));
+    const Tw* twr = row_tables(dev, p, root_r, l2, &err);
+    const u32* seeds = seed_tables(dev, p, root, k, &err);
+    if (!twr || !seeds) return err ? err : OUT_OF_MEMORY;
+    A.pk = make_prime_k_for(pc.info, root_r, l2);
+    A.twr = twr;
+    A.seeds = seeds;
+    A.nlo = (int)std::min<long long>(n, 4096);
+    A.nhi = (int)std::max<long long>(1, n / 4096);
+    A.l1 = l1;
+    A.colpl = col_plan(l1);
+    A.src = w1;
+    A.dst = w2;
+    A.scale = tw_of(sc, p);
+    A.job_stride = n;
+    {
+        LargeArgs LA;
+        if (large_args(pc, root, k, l2, dev, &LA) == OK) A.rowtab = LA.rowtab;
+    }
+    std::vector<LargeJob> hj((size_t)cm);
+    for (long long r0 = 0; r0 < m; r0 += cm) {
+        const int cnt = (int)std::min(cm, m - r0);
+        for (int t = 0; t < cnt; ++t)
+            hj[t] = LargeJob{x + (r0 + t) * n, nullptr, nullptr, (int)n, 0, 0, 0, w1 + (long long)t * n, nullptr};
+        // pageable source: staged before the call returns, so hj is free to refill
+        cudaError_t e = cudaMemcpyAsync(dj, hj.data(), (size_t)cnt * sizeof(LargeJob), cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return cuda_err(e);
+        if ((err = column_pass(pc, root_c, l1, l2, nullptr, n, nullptr, dev, st, dj, cnt)) != OK) return err;
+        kRowNtt[l2](A, 1 << l1, st, cnt);
+        u32* out = x + r0 * n;
+        if (l1 >= 6)
+            k_transpose64<<<dim3((1 << l2) / 64, (1 << l1) / 64, cnt), 256, 0, st>>>(w2, out, 1 << l1, 1 << l2);
+        else
+            k_transpose<<<dim3((1 << l2) / 32, (1 << l1) / 32, cnt), dim3(32, 8), 0, st>>>(w2, out, 1 << l1,
+                                                                                          1 << l2);
+    }
+    return cuda_err(cudaGetLastError());
+}
+
+}  // namespace
 
 // m independent natural-order transforms of length 2^k (row i at x + i 2^k),
 // in place: the list transform I_m (x) DFT_n.
@@ -473,10 +543,11 @@ int list_ntt_dev(u32* x, long long m, int k, u32 w, u32 p, bool inverse, cudaStr
         for (long long r0 = 0; r0 < m; r0 += (1ll << 30)) {
             A.src = x + (r0 << k);
             A.dst = x + (r0 << k);
-            kRowNtt[k](A, (int)std::min<long long>(1ll << 30, m - r0), st);
+            kRowNtt[k](A, (int)std::min<long long>(1ll << 30, m - r0), st, 1);
         }
         return cuda_err(cudaGetLastError());
     }
+    if (k <= kMaxLog) return list_ntt_four_step(*pc, x, m, k, root, sc, st);
     for (long long r = 0; r < m; ++r)
         if ((err = ntt_natural_dev(x + (r << k), x + (r << k), k, w, p, inverse, st)) != OK) return err;
     return OK;
@@ -552,7 +623,7 @@ int bivariate_dev(u32* x, int em, u32 wm, int en, u32 wn, u32 p, bool inverse, c
     A.dst = x;
     if (em == 0) {
         A.src = x;
-        kRowNtt[en](A, 1, st);
+        kRowNtt[en](A, 1, st, 1);
         return cuda_err(cudaGetLastError());
     }
     u32* w1 = (u32*)workspace(dev, kWsNtt, (size_t)total * sizeof(u32), &err);
@@ -561,7 +632,7 @@ int bivariate_dev(u32* x, int em, u32 wm, int en, u32 wn, u32 p, bool inverse, c
     A.l1 = em;
     A.colpl = col_plan(em);
     A.src = w1;
-    kRowNtt[en](A, 1 << em, st);
+    kRowNtt[en](A, 1 << em, st, 1);
     return cuda_err(cudaGetLastError());
 }
 

@@ -18,7 +18,8 @@ constexpr int kDefaultColLog = 10;  // column length of the default split (rows 
 // workspace slots (runtime.cuh: workspace)
 enum WsSlot { kWsSingle = 0, kWsBatch = 1, kWsStage = 2, kWsNtt = 3, kWsTwoConv = 4, kWsServer = 5,
               kWsBiv = 6, kWsBivHost = 7, kWsBig = 8, kWsSplitProd = 9, kWsSplitIn = 10,
-              kWsSplitNtt = 11 /* + (k - kMaxLog - 1) for a 2^k transform: 11..14 */, kWsBivT = 15 };
+              kWsSplitNtt = 11 /* + (k - kMaxLog - 1) for a 2^k transform: 11..14 */, kWsBivT = 15,
+              kWsListJobs = 16 };
 
 // SMs of device dev (cached per device).
 int sm_count(int dev);

@@ -23,7 +23,7 @@ def _run(cm, x, m, k, w, p, inverse=False):
 
 
 @pytest.mark.parametrize("m,k", [(1, 0), (7, 1), (5, 3), (300, 5), (3, 6), (17, 10), (100, 12),
-                                 (9, 14), (3, 16), (2, 18)])
+                                 (9, 14), (3, 16), (2, 18), (5, 15), (70, 16), (3, 20)])
 @pytest.mark.parametrize("p", [469762049, 962592769])
 def test_list_fft_matches_rowwise_dft(cm, oracle_mod, m, k, p):
     r = SplitMix64(m * 1000 + k * 7 + p)
@@ -36,6 +36,20 @@ def test_list_fft_matches_rowwise_dft(cm, oracle_mod, m, k, p):
         assert np.array_equal(got.reshape(m, 1 << k)[i], want), i
     back = _run(cm, got, m, k, w, p, inverse=True)
     assert np.array_equal(back, x)
+
+
+@pytest.mark.parametrize("m,k", [(2, 22), (5, 24)])
+def test_list_fft_long_rows(cm, oracle_mod, m, k):
+    """Rows of 2^22 and 2^24 words mod 469762049 (2-adic order 26); five 2^24-word rows take two
+    launches of the batched four-step passes (at most 2^26 words in flight)."""
+    r = SplitMix64(m * 1000 + k * 7)
+    x = r.residues(m << k, P0)
+    w = oracle_mod.primitive_root(k, P0)
+    got = _run(cm, x, m, k, w, P0)
+    rows = x.reshape(m, 1 << k)
+    for i in sorted({0, m // 2, m - 1}):
+        assert np.array_equal(got.reshape(m, 1 << k)[i], oracle_mod.ntt(rows[i], w, P0)), i
+    assert np.array_equal(_run(cm, got, m, k, w, P0, inverse=True), x)
 
 
 def test_list_fft_every_row_small(cm, oracle_mod):
