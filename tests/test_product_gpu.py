@@ -120,6 +120,19 @@ def test_product_2_25(cm, oracle_mod):
     assert np.array_equal(got[1], oracle_mod.polymul_school(c, d, P0))
 
 
+@pytest.mark.parametrize("p,order", [(962592769, 21), (950009857, 21), (940572673, 20), (754974721, 24)])
+def test_products_at_the_primes_2_adic_order(cm, oracle_mod, p, order):
+    """The longest product each prime allows (transform 2^order, 2^order - 1 coefficients) is
+    computed; a product of 2^order + 1 coefficients is refused with CUMODP_FFT_SIZE_TOO_LARGE."""
+    r = SplitMix64(p ^ 0x5A5A)
+    half = 1 << (order - 1)
+    a, b = _rand(r, half, p), _rand(r, half, p)
+    assert np.array_equal(cm.fftmul_uni(a, b, p), oracle_mod.polymul(a, b, p))
+    with pytest.raises(cm.CumodpError) as e:
+        cm.fftmul_uni(np.append(a, [1, 1]).astype(np.uint32), b, p)
+    assert e.value.code == cm.FFT_SIZE_TOO_LARGE
+
+
 def test_split_product_2_26(cm, oracle_mod):
     """Transform 2^26 (the 2-adic order of 469762049): beyond the three-pass kernels' 2^25 the
     operands are cut into 2^24-coefficient pieces whose pairwise products are added at their

@@ -15,7 +15,7 @@ P0 = 469762049
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("k", [0, 1, 3, 5, 6, 8, 10, 13, 14, 15, 16, 18, 20])
+@pytest.mark.parametrize("k", [0, 1, 3, 5, 6, 8, 10, 13, 14, 15, 16, 18, 20, 21])
 @pytest.mark.parametrize("p", [469762049, 962592769])
 def test_fft_uni_matches_dft(cm, oracle_mod, k, p):
     r = SplitMix64(k * 31 + p)
