@@ -32,7 +32,7 @@ struct RowNttArgs {
     LevelPlan colpl;
     const u32* src;                 // row slot s at src + s * n2
     u32* dst;                       // natural row k1 at dst + k1 * n2
-    Tw scale;                       // applied to every output
+    Tw scale;                       // applied to every output (folded into level 0's input factors)
     int rows_in_place;              // 1: independent rows, row s written to dst row s
     const Tw* __restrict__ rowtab;  // per-slot level-0 factor tables (RowTab, forward direction), or nullptr
     long long job_stride;           // words between the transforms of grid row blockIdx.y (list transforms)
@@ -52,14 +52,26 @@ __device__ __forceinline__ u32 seed_mont_at(const u32* __restrict__ seeds, int n
 // buffer, and the row is stored with 16-byte accesses.  With the prebuilt
 // per-slot factor tables (rows of 2^11-2^14 words) level 0 is that of the
 // product's row kernels: inputs times W^(TB0 m), DIF, outputs times the two
-// shared-memory factors of U_j^o.
-template <int L2>
-__global__ void __launch_bounds__(ntt_row_threads(L2), ntt_row_ctas(L2)) k_row_ntt(const __grid_constant__ RowNttArgs A) {
+// shared-memory factors of U_j^o.  The output scale (the inverse transform's
+// 2^-k) is folded into level 0's input factors, so a transform is linear in
+// it at no cost per word: the last level only reduces to [0, p).
+//
+// QOUT (rows of a four-step transform that a permuting transpose,
+// k_transpose64_q, puts in natural order): the in-row reorder is skipped and
+// each thread stores its last-level groups straight from registers in the
+// layout of the product's row spectra -- digit-reversed positions, quad c of
+// 32-word group r at c n2/8 + 4r, so a warp store covers one contiguous
+// 512-byte run -- with the split row kernels' CTA shape (256 threads, three
+// CTAs per SM for 2^14-word rows).
+template <int L2, bool QOUT = false>
+__global__ void __launch_bounds__(QOUT ? rowsplit_threads(L2) : ntt_row_threads(L2),
+                                  QOUT ? rowsplit_ctas(L2) : ntt_row_ctas(L2))
+    k_row_ntt(const __grid_constant__ RowNttArgs A) {
     constexpr int n2 = 1 << L2;
-    constexpr int T = ntt_row_threads(L2);
+    constexpr int T = QOUT ? rowsplit_threads(L2) : ntt_row_threads(L2);
     constexpr LevelPlan PL = row_plan(L2);
     static_assert(PL.nlev >= 2, "row transform needs two levels");
-    static_assert(T * 32 >= n2, "one last-level group per thread");
+    static_assert(QOUT || T * 32 >= n2, "one last-level group per thread");
     using LV0 = SmallLevel<L2, 0>;
     constexpr int R0 = LV0::R, TB0 = LV0::TB;
     extern __shared__ __align__(16) u32 sm[];
@@ -73,6 +85,7 @@ __global__ void __launch_bounds__(ntt_row_threads(L2), ntt_row_ctas(L2)) k_row_n
     const u32 p = A.pk.p, p2 = A.pk.p2, pinv = A.pk.pinv_neg;
     using RT = RowTab<L2>;
     const bool tabbed = RT::USE && twid && A.rowtab;
+    const bool scaled = A.scale.w != 1u;
     Tw* tab = reinterpret_cast<Tw*>(sm + n2);
     const size_t joff = (size_t)blockIdx.y * (size_t)A.job_stride;
     row_load_issue<L2, T>(sm, A.src + joff + (size_t)s * n2);
@@ -85,11 +98,20 @@ __global__ void __launch_bounds__(ntt_row_threads(L2), ntt_row_ctas(L2)) k_row_n
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     } else if (twid && threadIdx.x < R0) {
         const u32 e = (k1 * (u32)TB0 * threadIdx.x) & nmask;
-        const u32 v = red1(mul_mont(seed_mont_at(A.seeds, A.nlo, e, p, pinv), 1u, p, pinv), p);
-        bf[threadIdx.x] = Tw{v, (u32)(((u64)v << 32) / p)};
+        u32 v = red1(mul_mont(seed_mont_at(A.seeds, A.nlo, e, p, pinv), 1u, p, pinv), p);
+        if (scaled) v = mulmod_exact(v, A.scale.w, p);
+        bf[threadIdx.x] = Tw{v, shoup_quot(v, p)};
     }
     row_load_wait();
     __syncthreads();
+    if (tabbed && scaled) {  // the slot factors times the scale (factor 0 becomes the scale)
+        if (threadIdx.x < R0) {
+            Tw* vf = tab + RT::ENTRIES;
+            const u32 v = threadIdx.x == 0 ? A.scale.w : mulmod_exact(vf[threadIdx.x].w, A.scale.w, p);
+            vf[threadIdx.x] = Tw{v, shoup_quot(v, p)};
+        }
+        __syncthreads();
+    }
 
     if constexpr (RT::USE) {
         if (tabbed) {
@@ -100,7 +122,7 @@ __global__ void __launch_bounds__(ntt_row_threads(L2), ntt_row_ctas(L2)) k_row_n
 #pragma unroll
                 for (int m = 0; m < R0; ++m) {
                     const u32 v = sm[swz_task<TB0, n2>(o, bs, m)];
-                    x[m] = m == 0 ? v : mul_shoup(v, vf[m].w, vf[m].wq, p);
+                    x[m] = m == 0 && !scaled ? v : mul_shoup(v, vf[m].w, vf[m].wq, p);
                 }
                 dif_regs<R0, true>(x, A.pk.rc.f, p, p2);
                 const Tw* ta = tab + (o % RT::NA);
@@ -123,6 +145,7 @@ __global__ void __launch_bounds__(ntt_row_threads(L2), ntt_row_ctas(L2)) k_row_n
         for (int m = 0; m < R0; ++m) {
             const u32 v = sm[swz_task<TB0, n2>(o, bs, m)];
             if (twid) x[m] = mul_mont(v, mul_shoup(mo, bf[m].w, bf[m].wq, p), p, pinv);
+            else if (scaled) x[m] = mul_shoup(v, A.scale.w, A.scale.wq, p);
             else x[m] = mul_shoup(v, 1u, A.pk.one_q, p);
         }
         dif_regs<R0, true>(x, A.pk.rc.f, p, p2);
@@ -136,6 +159,19 @@ __global__ void __launch_bounds__(ntt_row_threads(L2), ntt_row_ctas(L2)) k_row_n
     __syncthreads();
     fwd1_levels<L2, 1, T>(sm, A.pk, A.twr);
 
+    if constexpr (QOUT) {
+        u32* out = A.dst + joff + (size_t)out_row * n2;
+        for (int r = threadIdx.x; r < n2 / 32; r += T) {
+            u32 x[32];
+            load_row32(x, sm, r * 32);
+            dif_regs<32>(x, A.pk.rc.f, p, p2);
+#pragma unroll
+            for (int c = 0; c < 8; ++c)
+                *reinterpret_cast<uint4*>(out + c * (n2 / 8) + 4 * r) =
+                    make_uint4(red1(x[4 * c], p), red1(x[4 * c + 1], p), red1(x[4 * c + 2], p), red1(x[4 * c + 3], p));
+        }
+        return;
+    }
     const int r = threadIdx.x;
     const bool has = r < n2 / 32;
     u32 x[32];
@@ -143,7 +179,7 @@ __global__ void __launch_bounds__(ntt_row_threads(L2), ntt_row_ctas(L2)) k_row_n
         load_row32(x, sm, r * 32);
         dif_regs<32>(x, A.pk.rc.f, p, p2);
 #pragma unroll
-        for (int j = 0; j < 32; ++j) x[j] = red1(mul_shoup(x[j], A.scale.w, A.scale.wq, p), p);
+        for (int j = 0; j < 32; ++j) x[j] = red1(x[j], p);
     }
     __syncthreads();
     // natural order through shared memory (swz_nat layout: the reorder's
@@ -189,6 +225,43 @@ __global__ void __launch_bounds__(256) k_transpose64(const u32* __restrict__ in,
     }
 }
 
+// out[f(c) * rows + r] = in[r * n2 + c] for rows a multiple of 64, where row
+// r of `in` is a row spectrum in the layout k_row_ntt<L2, true> stores and
+// f(c) is the frequency word c holds: word c = q n2/8 + 4 g + e (e < 4,
+// g < n2/32) holds digit-reversed position P = 32 g + 4 q + e, whose
+// frequency is row_pos_to_freq<L2>(P).  64 x 64 tiles through shared
+// memory, 16-byte loads and stores (each of a tile's 64 words is one
+// frequency, whose 64 rows are one 256-byte run of the output).
+template <int L2>
+__global__ void __launch_bounds__(256) k_transpose64_q(const u32* __restrict__ in, u32* __restrict__ out, int rows) {
+    constexpr int n2 = 1 << L2;
+    __shared__ u32 t[64][65];
+    in += (size_t)blockIdx.z * rows * n2;  // transform blockIdx.z of a list
+    out += (size_t)blockIdx.z * rows * n2;
+    const int c0 = blockIdx.x * 64;
+    const size_t r0 = (size_t)blockIdx.y * 64;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const u32* src = in + r0 * n2 + c0 + 4 * tx;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int rr = ty + 16 * k;
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(src + (size_t)rr * n2));
+        t[rr][4 * tx] = v.x;
+        t[rr][4 * tx + 1] = v.y;
+        t[rr][4 * tx + 2] = v.z;
+        t[rr][4 * tx + 3] = v.w;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int cc = ty + 16 * k;
+        const u32 c = (u32)(c0 + cc), q = c / (n2 / 8), g = (c % (n2 / 8)) / 4, e = c % 4;
+        const u32 f = row_pos_to_freq<L2>(32 * g + 4 * q + e);
+        const uint4 v = make_uint4(t[4 * tx][cc], t[4 * tx + 1][cc], t[4 * tx + 2][cc], t[4 * tx + 3][cc]);
+        *reinterpret_cast<uint4*>(out + (size_t)f * rows + r0 + 4 * tx) = v;
+    }
+}
+
 // out[c * rows + r] = in[r * cols + c]: 32 x 32 tiles through shared memory.
 __global__ void k_transpose(const u32* __restrict__ in, u32* __restrict__ out, int rows, int cols) {
     __shared__ u32 t[32][33];
@@ -230,6 +303,26 @@ void launch_row_ntt_t(const RowNttArgs& a, int rows, cudaStream_t st, int jobs) 
         attr = true;
     }
     k_row_ntt<L2><<<dim3(rows, jobs), ntt_row_threads(L2), smem, st>>>(a);
+}
+
+// The rows of a four-step transform with 2^14-word rows and at least 64 of
+// them: k_row_ntt<14, true> then the permuting transpose into x_out (jobs
+// transforms of rows x 2^14 words, w2 and x_out job_stride words apart).
+void row_ntt_q_and_transpose(const RowNttArgs& a, int rows, u32* x_out, cudaStream_t st, int jobs) {
+    constexpr int L2 = kMaxRowLog;
+    const size_t smem = (size_t)(1 << L2) * sizeof(u32) + (size_t)RowTab<L2>::TABW * sizeof(Tw);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_row_ntt<L2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    cudaEvent_t e0;
+    bool tr = pass_timing_begin(st, &e0);
+    k_row_ntt<L2, true><<<dim3(rows, jobs), rowsplit_threads(L2), smem, st>>>(a);
+    if (tr) pass_timing_end(st, "ntt_row", e0);
+    tr = pass_timing_begin(st, &e0);
+    k_transpose64_q<L2><<<dim3((1 << L2) / 64, rows / 64, jobs), 256, 0, st>>>(a.dst, x_out, rows);
+    if (tr) pass_timing_end(st, "ntt_transpose", e0);
 }
 typedef void (*RowNttFn)(const RowNttArgs&, int, cudaStream_t, int);
 const RowNttFn kRowNtt[15] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
@@ -436,6 +529,10 @@ int ntt_natural_dev(const u32* x_in, u32* x_out, int k, u32 w, u32 p, bool inver
         LargeArgs LA;  // the level-0 factor tables of this root and shape (built once, cached)
         if (large_args(*pc, root, k, l2, dev, &LA) == OK) A.rowtab = LA.rowtab;
     }
+    if (l1 >= 6 && l2 == kMaxRowLog) {
+        row_ntt_q_and_transpose(A, 1 << l1, x_out, st, 1);
+        return cuda_err(cudaGetLastError());
+    }
     tr = pass_timing_begin(st, &e0);
     kRowNtt[l2](A, 1 << l1, st, 1);
     if (tr) pass_timing_end(st, "ntt_row", e0);
@@ -497,8 +594,12 @@ int list_ntt_four_step(const PrimeCtx& pc, u32* x, long long m, int k, u32 root,
         cudaError_t e = cudaMemcpyAsync(dj, hj.data(), (size_t)cnt * sizeof(LargeJob), cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess) return cuda_err(e);
         if ((err = column_pass(pc, root_c, l1, l2, nullptr, n, nullptr, dev, st, dj, cnt)) != OK) return err;
-        kRowNtt[l2](A, 1 << l1, st, cnt);
         u32* out = x + r0 * n;
+        if (l1 >= 6 && l2 == kMaxRowLog) {
+            row_ntt_q_and_transpose(A, 1 << l1, out, st, cnt);
+            continue;
+        }
+        kRowNtt[l2](A, 1 << l1, st, cnt);
         if (l1 >= 6)
             k_transpose64<<<dim3((1 << l2) / 64, (1 << l1) / 64, cnt), 256, 0, st>>>(w2, out, 1 << l1, 1 << l2);
         else
