@@ -239,11 +239,12 @@ def fftmul_uni_dev_noalloc(h_ptr: int, lh: int, f_ptr: int, df: int, g_ptr: int,
                            stream: int = 0) -> None:
     """Device-pointer product that allocates no device memory (``cumodp_fftmul_uni_dev_noalloc``).
 
-    For callers that may not allocate device memory (work captured into
-    someone else's CUDA graph, pool-owned device memory, plugins in a host
-    that partitioned device memory).  Scratch is a fixed ~8.4 MiB array in
-    the library's device data segment; products up to df + dg + 1 <= 2^20;
-    calls that overlap on the GPU race on that array.
+    For callers that may not allocate device memory (pool-owned device
+    memory, plugins in a host that partitioned device memory, latency-critical
+    code that cannot take cudaMalloc's implicit synchronisation).  Scratch is
+    a fixed ~8.4 MiB array in the library's device data segment, whose tables
+    every call rewrites; products up to df + dg + 1 <= 2^20; calls that
+    overlap on the GPU race on that array.
     """
     _check(_lib().cumodp_fftmul_uni_dev_noalloc(lh, h_ptr, df, f_ptr, dg, g_ptr, p, stream or None),
            "cumodp_fftmul_uni_dev_noalloc")

@@ -85,6 +85,21 @@ cumodp_err cumodp_fftmul_uni_dev(sfixn lh, sfixn* H, sfixn df, const sfixn* F, s
     return to_err(e);
 }
 
+cumodp_err cumodp_cyclic_mul_dev(sfixn e, sfixn* F, const sfixn* G, sfixn p, void* stream) {
+    if (!have_device()) return CUMODP_NO_CUDA_DEVICE;
+    if (e < 0 || !F || !G) return CUMODP_ASSUMPTION_ERROR;
+    if (e < 31) {
+        const size_t n = (size_t)1 << e;
+        const char *f = (const char*)F, *g = (const char*)G;
+        if (f < g + 4 * n && g < f + 4 * n) return CUMODP_ASSUMPTION_ERROR;  // F and G overlap
+    }
+    std::lock_guard<std::mutex> g(lib_mutex());
+    cudaStream_t st = stream ? (cudaStream_t)stream : lib_stream(current_device());
+    int err = cyclic_mul_dev((u32*)F, (const u32*)G, (int)e, (u32)p, st);
+    if (err == OK && !stream) err = cuda_err(cudaStreamSynchronize(st));
+    return to_err(err);
+}
+
 cumodp_err cumodp_fftmul_uni(sfixn dh, sfixn* H, sfixn df, const sfixn* F, sfixn dg, const sfixn* G, sfixn p) {
     if (!have_device()) return CUMODP_NO_CUDA_DEVICE;
     if (df < 0 || dg < 0 || dh < 0 || !F || !G || !H) return CUMODP_ASSUMPTION_ERROR;

@@ -1,25 +1,32 @@
 // A product entry point that allocates no device memory.
 //
-// Some callers of this library cannot call cudaMalloc: code that runs while
-// another component is capturing the device's work into a CUDA graph, a
-// service whose device memory is owned by its own pool allocator and may not
-// be allocated behind its back, or a plugin loaded into a host that has
-// already partitioned all device memory.  cumodp_fftmul_uni_dev_noalloc
-// serves them: the caller passes device buffers for the operands and the
-// result, and everything else the product needs -- the three-pass workspace
-// and the twiddle tables -- lives in one fixed array in the library's own
-// device data segment (g_noalloc_scratch below, about 8.4 MiB), which every
-// GPU that loads the library holds until the process exits.
+// Some callers of this library cannot call cudaMalloc: a service whose device
+// memory is owned by its own pool allocator and may not be allocated behind
+// its back, a plugin loaded into a host that has already partitioned all
+// device memory, or code on a latency-critical path where cudaMalloc's
+// implicit device synchronisation is not acceptable.
+// cumodp_fftmul_uni_dev_noalloc serves them: the caller passes device buffers
+// for the operands and the result, and everything else the product needs --
+// the three-pass workspace and the twiddle tables -- lives in one fixed array
+// in the library's own device data segment (g_noalloc_scratch below, about
+// 8.4 MiB), which every GPU that loads the library holds until the process
+// exits.
 //
 // Limits and sharing:
 //   * products with df + dg + 1 <= 2^20 (transform length <= 2^20); larger
 //     requests are rejected with CUMODP_FFT_SIZE_TOO_LARGE;
-//   * every call uses the same array, which keeps the last call's contents
-//     (the workspace of the last product and the tables of the last
-//     (prime, size)); nothing in it has to start at zero because each call
-//     writes every word it reads;
-//   * calls whose work overlaps on the GPU (different streams, or other host
-//     threads' calls still running) race on the array.
+//   * every call writes the twiddle tables of its (prime, size) into the
+//     array with a small kernel on the caller's stream, then runs the
+//     product: no state is carried from one call to the next, and nothing in
+//     the array has to start at zero, because each call writes every word it
+//     reads before reading it;
+//   * every call uses the same array, which keeps the last call's contents:
+//     calls whose work overlaps on the GPU (different streams, or other host
+//     threads' calls still running) race on the array;
+//   * the array's device address is looked up once per device (the first
+//     call on that device, with that device current); cudaDeviceReset after
+//     that first call is not supported, as for the library's other
+//     per-device state.
 #include <cstring>
 #include <mutex>
 
@@ -48,17 +55,92 @@ static __device__ __align__(256) u32 g_noalloc_scratch[kNaWords];
 
 struct NaDevice {
     u32* base = nullptr;  // device address of g_noalloc_scratch on this device
-    u32 key_p = 0;        // (prime, size) whose tables the array holds
-    int key_logn = -1;
 };
 
 std::mutex g_na_m;
 NaDevice g_na[64];
 
-// Host staging for the tables: fixed storage, nothing allocated per call.
-Tw g_host_row[kNaRowTw];
-Tw g_host_col[kNaColTw];
-u32 g_host_seeds[kNaSeeds];
+// One plan's level tables (the layout of level_tables_into: per level i,
+// task o and slot j at off_i + o R_i + j hold w_B^(o bitrev(j)) in Shoup
+// form, the forward tables first and the inverse ones nf entries later, then
+// two zero words), with w_B and w_B^-1 of every level in Montgomery form.
+struct NaPlan {
+    Tw* out;
+    LevelPlan pl;
+    int logl, nf;
+    u32 wb[6], wbi[6];
+};
+
+// x^e * 2^32 mod p from the Montgomery form xm = x 2^32 (lazy, in [0, 2p)).
+__device__ __forceinline__ u32 na_pow_m(u32 xm, u64 e, u32 one_m, u32 p, u32 pinv) {
+    u32 acc = one_m;
+    for (int b = 63 - __clzll((long long)(e | 1)); b >= 0; --b) {
+        acc = mul_mont(acc, acc, p, pinv);
+        if ((e >> b) & 1) acc = mul_mont(acc, xm, p, pinv);
+    }
+    return acc;
+}
+
+__device__ __forceinline__ Tw na_level_entry(const NaPlan& P, int t, u32 one_m, u32 p, u32 pinv) {
+    const bool inv = t >= P.nf;
+    if (inv) t -= P.nf;
+    int off = 0, lb = P.logl;
+    for (int i = 0; i + 1 < P.pl.nlev; ++i) {
+        const int r = P.pl.logr[i];
+        if (t < off + (1 << lb)) {
+            const int q = t - off, o = q >> r, j = q & ((1 << r) - 1);
+            const u32 m = na_pow_m(inv ? P.wbi[i] : P.wb[i], (u64)o * rev_bits((u32)j, r), one_m, p, pinv);
+            const u32 v = red1(mul_mont(m, 1u, p, pinv), p);
+            return Tw{v, shoup_quot(v, p)};
+        }
+        off += 1 << lb;
+        lb -= r;
+    }
+    return Tw{0u, 0u};  // the two padding entries after the inverse tables
+}
+
+// Every table one product reads, into the scratch array: the row plan's
+// level tables, and for a three-pass product the column plan's and the
+// inter-pass seeds (seeds_into's layout: lo[e] = w^e 2^32 for e < nlo, then
+// hi[e] = w^(4096 e) 2^32 for e < nhi, forward then inverse; wm, wim, w4m,
+// wi4m: w, w^-1, w^4096, w^-4096 in Montgomery form).
+__global__ void k_na_tables(const NaPlan row, const NaPlan col, u32* seeds, u32 nlo, u32 nhi, u32 wm, u32 wim,
+                            u32 w4m, u32 wi4m, u32 p, u32 pinv, u32 one_m) {
+    const int nr = row.out ? 2 * row.nf + 2 : 0, nc = col.out ? 2 * col.nf + 2 : 0;
+    const int ns = seeds ? (int)(2 * (nlo + nhi)) : 0;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nr + nc + ns; t += gridDim.x * blockDim.x) {
+        if (t < nr) {
+            row.out[t] = na_level_entry(row, t, one_m, p, pinv);
+        } else if (t < nr + nc) {
+            col.out[t - nr] = na_level_entry(col, t - nr, one_m, p, pinv);
+        } else {
+            const u32 s = (u32)(t - nr - nc);
+            const bool inv = s >= nlo + nhi;
+            const u32 u = inv ? s - (nlo + nhi) : s;
+            const u32 base = u < nlo ? (inv ? wim : wm) : (inv ? wi4m : w4m);
+            seeds[s] = red1(na_pow_m(base, u < nlo ? u : u - nlo, one_m, p, pinv), p);
+        }
+    }
+}
+
+// The host side of k_na_tables' arguments for one plan (scalars only).
+NaPlan na_plan(Tw* out, const LevelPlan& pl, int logl, u32 root, const PrimeInfo& pi) {
+    NaPlan P;
+    memset(&P, 0, sizeof(P));
+    P.out = out;
+    P.pl = pl;
+    P.logl = logl;
+    P.nf = plan_tw_entries(pl, logl);
+    const u32 p = pi.p;
+    const u32 rinv = powmod_exact(root, (1ull << logl) - 1, p);
+    int lb = logl;
+    for (int i = 0; i + 1 < pl.nlev; ++i) {
+        P.wb[i] = mulmod_exact(powmod_exact(root, 1ull << (logl - lb), p), pi.r1, p);
+        P.wbi[i] = mulmod_exact(powmod_exact(rinv, 1ull << (logl - lb), p), pi.r1, p);
+        lb -= pl.logr[i];
+    }
+    return P;
+}
 
 }  // namespace
 
@@ -92,28 +174,29 @@ int mul_dev_noalloc(const u32* a, long long la, const u32* b, long long lb, u32*
     Tw* d_row = reinterpret_cast<Tw*>(D.base + kNaOffRow);
     Tw* d_col = reinterpret_cast<Tw*>(D.base + kNaOffCol);
     u32* d_seeds = D.base + kNaOffSeeds;
-    if (D.key_p != p || D.key_logn != logn) {
-        // tables of this (prime, size) into the array; the pageable source
-        // is staged by the copy before the call returns
-        if ((err = level_tables_into(0, p, root_r, l2, g_host_row, kNaRowTw)) != OK) return err;
-        cudaError_t ce = cudaMemcpyAsync(d_row, g_host_row, level_tables_entries(0, l2) * sizeof(Tw),
-                                         cudaMemcpyHostToDevice, st);
-        if (ce == cudaSuccess && large) {
-            const u32 root_c = powmod_exact(root, 1ull << l2, p);
-            if ((err = level_tables_into(1, p, root_c, l1, g_host_col, kNaColTw)) != OK) return err;
-            if ((err = seeds_into(p, root, logn, g_host_seeds, kNaSeeds)) != OK) return err;
-            ce = cudaMemcpyAsync(d_col, g_host_col, level_tables_entries(1, l1) * sizeof(Tw),
-                                 cudaMemcpyHostToDevice, st);
-            if (ce == cudaSuccess)
-                ce = cudaMemcpyAsync(d_seeds, g_host_seeds, seed_words(logn) * sizeof(u32), cudaMemcpyHostToDevice,
-                                     st);
+    // the tables of this (prime, size), written on the caller's stream ahead
+    // of the product's kernels (nothing is carried over from earlier calls)
+    {
+        const PrimeInfo& pi = pc->info;
+        const NaPlan rowp = na_plan(d_row, row_plan(l2), l2, root_r, pi);
+        NaPlan colp;
+        memset(&colp, 0, sizeof(colp));
+        u32 nlo = 0, nhi = 0, wm = 0, wim = 0, w4m = 0, wi4m = 0;
+        if ((size_t)(2 * rowp.nf + 2) > kNaRowTw) return ASSUMPTION_ERROR;  // the array's row-table region
+        if (large) {
+            colp = na_plan(d_col, col_plan(l1), l1, powmod_exact(root, 1ull << l2, p), pi);
+            if ((size_t)(2 * colp.nf + 2) > kNaColTw || seed_words(logn) > kNaSeeds) return ASSUMPTION_ERROR;
+            nlo = (u32)std::min<long long>(n, 4096);
+            nhi = (u32)std::max<long long>(1, n / 4096);
+            const u32 rinv = powmod_exact(root, (u64)n - 1, p);
+            wm = mulmod_exact(root, pi.r1, p);
+            wim = mulmod_exact(rinv, pi.r1, p);
+            w4m = mulmod_exact(powmod_exact(root, 4096, p), pi.r1, p);
+            wi4m = mulmod_exact(powmod_exact(rinv, 4096, p), pi.r1, p);
         }
-        if (ce != cudaSuccess) {
-            D.key_logn = -1;
-            return cuda_err(ce);
-        }
-        D.key_p = p;
-        D.key_logn = logn;
+        k_na_tables<<<2 * sm_count(dev), 256, 0, st>>>(rowp, colp, large ? d_seeds : nullptr, nlo, nhi, wm, wim, w4m,
+                                                       wi4m, p, pi.pinv_neg, pi.r1);
+        if (cudaError_t ce = cudaGetLastError(); ce != cudaSuccess) return cuda_err(ce);
     }
     if (lh > n) {  // coefficients beyond the transform length are zero
         cudaError_t ce = cudaMemsetAsync(h + n, 0, (size_t)(lh - n) * sizeof(u32), st);

@@ -768,6 +768,25 @@ __global__ void k_extract2(const u32* __restrict__ src, int ex2, u32* __restrict
 
 int grid_for(long long n) { return (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148 * 16)); }
 
+// f <- f * g mod (x^n - 1, p), n = 2^e, for the lengths the product kernels
+// do not cover (e < 5 or e > 25): natural-order transforms of f (in place)
+// and of g (into workspace, so g is left as it is), the pointwise product and
+// the inverse transform of f.
+int cyclic_mul_compose(u32* f, const u32* g, int e, u32 p, cudaStream_t st) {
+    int err = OK;
+    const PrimeCtx* pc = prime_ctx(p, &err);
+    if (!pc) return err;
+    const long long n = 1ll << e;
+    const u32 w = canonical_root(*pc, e);
+    u32* gt = (u32*)workspace(current_device(), kWsCyclic, (size_t)n * sizeof(u32), &err);
+    if (!gt) return err;
+    if ((err = ntt_natural_dev(g, gt, e, w, p, false, st)) != OK) return err;
+    if ((err = ntt_natural_dev(f, f, e, w, p, false, st)) != OK) return err;
+    k_pointwise_mod<<<grid_for(n), 256, 0, st>>>(f, gt, n, p, pc->info.pinv_neg, pc->info.r2);
+    if ((err = cuda_err(cudaGetLastError())) != OK) return err;
+    return ntt_natural_dev(f, f, e, w, p, true, st);
+}
+
 // F <- DFT^-1(DFT F * DFT G) on a 2^em x 2^en row-major grid (rows: y, of
 // length 2^en in x): the 2-D cyclic convolution, i.e. the bivariate product
 // when both operands are zero-padded to the product's size.  Grids within

@@ -467,6 +467,46 @@ int mul_split_dev(const u32* a, long long la, const u32* b, long long lb, u32* h
 
 }  // namespace
 
+namespace {
+
+// h[0..lh) = a * b mod (x^n - 1, p) with n = 2^logn (kMinLog <= logn <=
+// kMaxLog, la, lb <= n): one forward transform of each operand, the
+// pointwise product and the inverse transform -- the linear product when
+// la + lb - 1 <= n, the cyclic convolution otherwise (the forward column
+// passes take operands of any length up to n).
+int mul_dev_len(const u32* a, long long la, const u32* b, long long lb, u32* h, long long lh, u32 p, int logn,
+                const PrimeCtx& pc, cudaStream_t st) {
+    int err = OK;
+    const long long n = 1ll << logn;
+    const int dev = current_device();
+    ensure_kernel_attrs();
+    if (lh > n) {  // coefficients beyond the transform length are zero
+        cudaError_t e = cudaMemsetAsync(h + n, 0, (size_t)(lh - n) * sizeof(u32), st);
+        if (e != cudaSuccess) return cuda_err(e);
+        lh = n;
+    }
+    const u32 root = canonical_root(pc, logn);
+    if (logn <= kMaxSmallLog && logn < single_large_min_log()) {
+        SmallArgs A;
+        if ((err = small_args(pc, root, logn, dev, &A)) != OK) return err;
+        A.job0 = ProdJob{a, b, h, (int)la, (int)lb, (int)lh, 0};
+        A.njobs = 1;
+        launch_small(logn, A, 1, st);
+    } else {
+        const int l2 = default_row_log(logn);
+        LargeArgs A;
+        if ((err = large_args(pc, root, logn, l2, dev, &A)) != OK) return err;
+        u32* ws = (u32*)workspace(dev, kWsSingle, (size_t)2 * n * sizeof(u32), &err);
+        if (!ws) return err;
+        A.job0 = LargeJob{a, b, h, (int)la, (int)lb, (int)lh, 0, ws, ws + n};
+        A.njobs = 1;
+        launch_large(A, 1, st);
+    }
+    return cuda_err(cudaGetLastError());
+}
+
+}  // namespace
+
 int mul_dev(const u32* a, long long la, const u32* b, long long lb, u32* h, long long lh, u32 p,
             cudaStream_t st) {
     if (la <= 0 || lb <= 0 || lh < 0) return ASSUMPTION_ERROR;
@@ -478,32 +518,18 @@ int mul_dev(const u32* a, long long la, const u32* b, long long lb, u32* h, long
     if (logn > pc->info.two_adic) return FFT_SIZE_TOO_LARGE;
     if (logn > kMaxSplitLog) return FFT_SIZE_TOO_LARGE;
     if (logn > kMaxLog) return mul_split_dev(a, la, b, lb, h, lh, p, st);
-    const long long n = 1ll << logn;
-    const int dev = current_device();
-    ensure_kernel_attrs();
-    if (lh > n) {  // coefficients beyond the transform length are zero
-        cudaError_t e = cudaMemsetAsync(h + n, 0, (size_t)(lh - n) * sizeof(u32), st);
-        if (e != cudaSuccess) return cuda_err(e);
-        lh = n;
-    }
-    const u32 root = canonical_root(*pc, logn);
-    if (logn <= kMaxSmallLog && logn < single_large_min_log()) {
-        SmallArgs A;
-        if ((err = small_args(*pc, root, logn, dev, &A)) != OK) return err;
-        A.job0 = ProdJob{a, b, h, (int)la, (int)lb, (int)lh, 0};
-        A.njobs = 1;
-        launch_small(logn, A, 1, st);
-    } else {
-        const int l2 = default_row_log(logn);
-        LargeArgs A;
-        if ((err = large_args(*pc, root, logn, l2, dev, &A)) != OK) return err;
-        u32* ws = (u32*)workspace(dev, kWsSingle, (size_t)2 * n * sizeof(u32), &err);
-        if (!ws) return err;
-        A.job0 = LargeJob{a, b, h, (int)la, (int)lb, (int)lh, 0, ws, ws + n};
-        A.njobs = 1;
-        launch_large(A, 1, st);
-    }
-    return cuda_err(cudaGetLastError());
+    return mul_dev_len(a, la, b, lb, h, lh, p, logn, *pc, st);
+}
+
+int cyclic_mul_dev(u32* f, const u32* g, int e, u32 p, cudaStream_t st) {
+    int err = OK;
+    const PrimeCtx* pc = prime_ctx(p, &err);
+    if (!pc) return err;
+    if (e < 0) return ASSUMPTION_ERROR;
+    if (e > pc->info.two_adic || e > kMaxSplitLog) return FFT_SIZE_TOO_LARGE;
+    if (e < kMinLog || e > kMaxLog) return cyclic_mul_compose(f, g, e, p, st);
+    const long long n = 1ll << e;
+    return mul_dev_len(f, n, g, n, f, n, p, e, *pc, st);
 }
 
 }  // namespace cmb

@@ -19,7 +19,7 @@ constexpr int kDefaultColLog = 10;  // column length of the default split (rows 
 enum WsSlot { kWsSingle = 0, kWsBatch = 1, kWsStage = 2, kWsNtt = 3, kWsTwoConv = 4, kWsServer = 5,
               kWsBiv = 6, kWsBivHost = 7, kWsBig = 8, kWsSplitProd = 9, kWsSplitIn = 10,
               kWsSplitNtt = 11 /* + (k - kMaxLog - 1) for a 2^k transform: 11..14 */, kWsBivT = 15,
-              kWsListJobs = 16 };
+              kWsListJobs = 16, kWsCyclic = 17 };
 
 // SMs of device dev (cached per device).
 int sm_count(int dev);
@@ -60,5 +60,13 @@ size_t mul_ws_words(int logn);
 // h[0..lh) = a[0..la) * b[0..lb) mod p on device pointers, on stream st.
 int mul_dev(const u32* a, long long la, const u32* b, long long lb, u32* h, long long lh, u32 p,
             cudaStream_t st);
+
+// f <- f * g mod (x^(2^e) - 1, p), the length-2^e cyclic convolution, on
+// device arrays of 2^e words (f may not overlap g): the product kernels on
+// one transform of length 2^e for kMinLog <= e <= kMaxLog, otherwise
+// natural-order transforms around a pointwise product (cyclic_mul_compose,
+// which needs 16-byte aligned arrays when e >= 6).
+int cyclic_mul_dev(u32* f, const u32* g, int e, u32 p, cudaStream_t st);
+int cyclic_mul_compose(u32* f, const u32* g, int e, u32 p, cudaStream_t st);
 
 }  // namespace cmb

@@ -142,19 +142,34 @@ const sfixn *interp_subres_coeff3(sfixn *nx, sfixn *ny, void *scb, sfixn i, sfix
 cumodp_err cumodp_fftmul_uni_dev(sfixn lh, sfixn *H, sfixn df, const sfixn *F,
                                  sfixn dg, const sfixn *G, sfixn p, void *stream);
 
+/* Addition.  Cyclic convolution on DEVICE arrays of n = 2^e words:
+ * F <- DFT^-1(DFT F * DFT G) = F * G mod (x^n - 1, p), the operation of the
+ * reference's C++ stockham_poly_mul_dev(n, e, F, G, p)
+ * (src/stockham.cu:521-542), which is the polynomial product when F and G are
+ * zero-padded so that deg F + deg G < n.  Inputs in [0, p).  G is left
+ * unchanged (the reference overwrites it with its transform); F and G must
+ * not overlap.  Lengths 2^5..2^25 run on the product kernels (one transform
+ * of length n, no padding), others as natural-order transforms around a
+ * pointwise product (then F and G 16-byte aligned when e >= 6).  e up to the
+ * prime's 2-adic order.  stream 0 = the library's stream, then synchronised. */
+cumodp_err cumodp_cyclic_mul_dev(sfixn e, sfixn *F, const sfixn *G, sfixn p, void *stream);
+
 /* Addition (no counterpart in the reference).  The device-pointer product of
  * cumodp_fftmul_uni_dev for callers that cannot allocate device memory --
- * code running while another component captures the device's work into a
- * CUDA graph, services whose device memory belongs to their own pool
- * allocator, plugins loaded after the host partitioned all device memory.
- * It calls no cudaMalloc/cudaFree and no allocating library routine: its
- * scratch (workspace and twiddle tables) is one fixed ~8.4 MiB array in the
+ * services whose device memory belongs to their own pool allocator, plugins
+ * loaded after the host partitioned all device memory, latency-critical code
+ * that cannot afford cudaMalloc's implicit synchronisation.  It calls no
+ * cudaMalloc/cudaFree and no allocating library routine: its scratch
+ * (workspace and twiddle tables) is one fixed ~8.4 MiB array in the
  * library's device data segment, held by every GPU that loads the library
  * until exit.  Limit: df + dg + 1 <= 2^20 (CUMODP_FFT_SIZE_TOO_LARGE
- * beyond).  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
- * All calls share the array: calls whose GPU work overlaps race.  stream 0
- * runs on the default stream and synchronises before returning. */
+ * beyond).  Every call first writes the twiddle tables of its prime and size
+ * into the array (a small kernel on `stream`), so no state passes from one
+ * call to the next.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture, and do not cudaDeviceReset that device afterwards.  All calls
+ * share the array: calls whose GPU work overlaps race.  stream 0 runs on the
+ * default stream and synchronises before returning. */
 cumodp_err cumodp_fftmul_uni_dev_noalloc(sfixn lh, sfixn *H, sfixn df, const sfixn *F,
                                          sfixn dg, const sfixn *G, sfixn p, void *stream);
 

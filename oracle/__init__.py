@@ -32,6 +32,12 @@ _i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
 _u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
 
 
+def reference_present() -> bool:
+    """Whether the reference sources the ``ref`` targets compile are present
+    (``make has-ref``: the Makefile's REF, or the CUMODP_REFERENCE variable)."""
+    return subprocess.run(["make", "-s", "-C", HERE, "has-ref"], capture_output=True).returncode == 0
+
+
 def build(ref: bool = False) -> None:
     """Compile liboracle.so (and, when ``ref``, the modpn reference builds)."""
     subprocess.check_call(["make", "-s", "-C", HERE, "oracle"])
@@ -114,7 +120,14 @@ def fourier_degree(p: int) -> int:
 
 
 def primitive_root(e: int, p: int) -> int:
-    """The reference's deterministic 2^e-th root (include/inlines.h:460-485)."""
+    """The reference's deterministic 2^e-th root (include/inlines.h:460-485).
+
+    Defined for e >= 1 (the reference's search shifts by e - 1; for e = 0 it
+    never ends): the primitive 1st root is 1, returned without the search."""
+    if e == 0:
+        return 1
+    if e < 0:
+        raise ValueError("e >= 0")
     return int(lib().or_primitive_root(e, p))
 
 

@@ -77,10 +77,10 @@ def parse_unit_kats(path: str) -> dict:
 def main(ref_root: str = "/root/reference") -> None:
     bench = os.path.join(ref_root, "benchmark")
     names = sorted(f for f in os.listdir(bench) if f.endswith(".test"))
-    # every fixed-width golden file, plus the big-coefficient files up to 512
-    # terms (the 1024-term one is 1.9 MB of text; seeded 1024-bit cases
-    # against the schoolbook oracle stand in for it)
-    keep = [f for f in names if "_p" in f or f in ("n32.test", "n64.test", "n128.test", "n256.test", "n512.test")]
+    # every fixed-width golden file and every big-coefficient file (n32 ... n1024:
+    # 32 ... 1024 terms of as many bits; n1024 is 1.9 MB of text, 0.9 MB gzipped)
+    keep = [f for f in names if "_p" in f or f in ("n32.test", "n64.test", "n128.test", "n256.test", "n512.test",
+                                                   "n1024.test")]
     for f in keep:
         data = open(os.path.join(bench, f), "rb").read()
         with gzip.GzipFile(os.path.join(HERE, f"bench_{f}.gz"), "wb", mtime=0) as g:

@@ -64,7 +64,7 @@ def test_modpn_links_against_this_library():
 
 
 def test_cpp_forwarding_header_compiles():
-    """include/list_stockham_b200.h gives the reference's C++ list_stockham_dev overloads."""
+    """include/list_stockham_b200.h and stockham_b200.h give the reference's C++ overloads."""
     import shutil
     import subprocess
     import tempfile
@@ -74,10 +74,19 @@ def test_cpp_forwarding_header_compiles():
         pytest.skip("g++ or CUDA headers absent")
     src = (
         '#include "list_stockham_b200.h"\n'
+        '#include "stockham_b200.h"\n'
         "void use(sfixn* X, const sfixn* W) {\n"
         "  cumodp_err a = list_stockham_dev(X, 4, 10, 3, 469762049);\n"
         "  cumodp_err b = list_stockham_dev(X, 4, 10, W, 469762049);\n"
         "  cumodp_err c = bi_stockham_poly_mul_dev(64, 6, 512, 9, X, X + 32768, 469762049);\n"
+        "  stockham_dev(X, 1024, 10, 3, 469762049);\n"
+        "  stockham_dev(X, 1024, 10, W, 469762049);\n"
+        "  inverse_stockham_dev(X, 1024, 10, 3, 469762049);\n"
+        "  inverse_stockham_dev(X, 1024, 10, W, 469762049);\n"
+        "  stockham_host(X, 1024, 10, 3, 469762049);\n"
+        "  inverse_stockham_host(X, 1024, 10, 3, 469762049);\n"
+        "  stockham_poly_mul_dev(1024, 10, X, X + 1024, 469762049);\n"
+        "  stockham_poly_mul_host(10, X, 5, W, 5, W, 469762049);\n"
         "  (void)a; (void)b; (void)c;\n}\n")
     with tempfile.TemporaryDirectory() as d:
         f = os.path.join(d, "use.cpp")
