@@ -420,6 +420,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         extras["big_1024bit_1024terms"] = big_coefficients(cm, torch, dev, stream)
         extras["serving_c5"] = serving_c5(cm)
         extras["list_and_bivariate"] = list_and_bivariate(cm, torch, dev, stream, hbm_peak)
+        extras["reference_gpu"] = reference_gpu(cm, torch, dev, stream, extras,
+                                                {"product_ms": round(ms / args.steps, 5),
+                                                 "host_product_ms": round(1000 * single_s / e2e_steps, 3)})
     cpu = None
     if rank == 0 and world == 1 and not args.no_extras:
         cpu = cpu_baseline()
@@ -631,9 +634,38 @@ def batched_c4(cm, torch, dev, stream):
     t_single_wall = (time.perf_counter() - t0) * 1000
     t_single = e0.elapsed_time(e1)
     same = bool(torch.equal(H, H1))
+    # the same one-call-per-pair path from a compiled C loop (no interpreter between the calls)
+    import ctypes as C
+    pc = C.CDLL(os.path.join(ROOT, "cumodp_b200", "libcumodp_percall.so"))
+    pc.percall_fftmul.restype = C.c_int
+    pc.percall_fftmul.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]
+    H1.zero_()
+
+    def c_loop():
+        rc = pc.percall_fftmul(cnt, da.ctypes.data, f_off.ctypes.data, fp, db.ctypes.data, g_off.ctypes.data, gp,
+                               h_off.ctypes.data, hp, P, C.c_void_p(sp))
+        assert rc == 0, rc
+    c_loop()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0.record(stream)
+    c_loop()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_c_wall = (time.perf_counter() - t0) * 1000
+    t_c = e0.elapsed_time(e1)
+    same_c = bool(torch.equal(H, H1))
     return {"pairs": cnt, "ms_batched": round(t_batch, 4), "products_per_s_batched": round(cnt / (t_batch / 1000), 1),
             "ms_one_call_per_pair": round(t_single, 4), "ms_one_call_per_pair_wall": round(t_single_wall, 4),
-            "speedup_vs_one_call": round(t_single / t_batch, 2), "batched_equals_single": same}
+            "speedup_vs_one_call": round(t_single / t_batch, 2), "batched_equals_single": same,
+            "one_call_per_pair_c_loop": {"ms": round(t_c, 4), "ms_wall": round(t_c_wall, 4),
+                                         "us_per_call": round(1000 * t_c / cnt, 2),
+                                         "speedup_batched_vs_c_loop": round(t_c / t_batch, 2),
+                                         "equals_batched": same_c,
+                                         "how": "cumodp_fftmul_uni_dev once per pair from a compiled C loop "
+                                                "(cumodp_b200/bench/percall.c), device pointers, one stream, "
+                                                "CUDA events"}}
 
 
 def c3_exact(cm, torch, dev, stream):
@@ -671,13 +703,22 @@ def c3_exact(cm, torch, dev, stream):
         e1.record(stream)
         torch.cuda.synchronize()
         dev_ms = e0.elapsed_time(e1) / reps
+        # the C host entry alone (raw 128-bit words: no Python int per coefficient)
+        for _ in range(3):
+            cm.twoconv_mul(a, b, raw=True)
         t0 = time.perf_counter()
-        for _ in range(5):
-            c = cm.twoconv_mul(a, b)
-        host_ms = (time.perf_counter() - t0) * 1000 / 5
+        for _ in range(20):
+            cw = cm.twoconv_mul(a, b, raw=True)
+        host_ms = (time.perf_counter() - t0) * 1000 / 20
+        t0 = time.perf_counter()
+        c = cm.int128_words_to_ints(cw)
+        conv_ms = (time.perf_counter() - t0) * 1000
         ok = sum(c) == sum(int(x) for x in a) * sum(int(x) for x in b)
         K, M, npr = cm.twoconv_plan(bw, bw, d + 1, d + 1)
         out[f"deg_{d}"] = {"device_ms": round(dev_ms, 4), "host_entry_ms": round(host_ms, 3),
+                           "host_entry_api": "cumodp_twoconv_mul_i64 (host int64 arrays in, 128-bit words out, "
+                                             "pinned staging inside)",
+                           "python_int_conversion_ms": round(conv_ms, 3),
                            "products_per_s_device": round(1000 / dev_ms, 1), "plan": {"K": K, "M": M, "primes": npr},
                            "sum_identity": bool(ok)}
     return out
@@ -850,15 +891,137 @@ def serving_c5(cm, rates=(1000, 3000, 10000, 30000, 100000), max_requests=20000,
     return out
 
 
+def reference_gpu(cm, torch, dev, stream, extras, ours):
+    """The reference's own GPU path on the same GPU in the same run (src/stockham.cu and src/fft_aux.cu,
+    compiled from the reference sources for sm_100a by oracle/Makefile into oracle/_ref/libcumodp_refgpu.so and
+    run as shipped: radix-2 Stockham, one launch and one device sync per step, per-call allocation).
+
+    C1 and C2 products device-resident (stockham_poly_mul_dev, CUDA events on the default stream it uses) and
+    host to host (stockham_poly_mul_host, the body of cumodp_fftmul_uni); the 2^24 transform device-resident
+    (stockham_dev) and host to host (stockham_host, the body of cumodp_fft_uni); C4 as a loop of host-to-host
+    products, pairs whose transform is below 256 (refused by the reference) counted apart.  Each figure sits
+    beside this library's figure for the same work and their ratio (reference time / ours)."""
+    import oracle
+    from cumodp_b200.workloads import SplitMix64, seed_for
+    if not oracle.ref_gpu_available():
+        return {"unavailable": "reference GPU build absent (make -C oracle ref_gpu needs the reference sources)"}
+    out = {}
+    sp = stream.cuda_stream
+
+    def host_ms(fn, reps):
+        with oracle.quiet_stdout():
+            fn()
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                fn()
+            return (time.perf_counter() - t0) * 1000 / reps
+
+    # C1: 4095 x 4095, transform 8192
+    r = SplitMix64(seed_for(0))
+    a, b = r.residues(4096, P), r.residues(4096, P)
+    F = torch.zeros(8192, dtype=torch.int32, device=dev)
+    G = torch.zeros(8192, dtype=torch.int32, device=dev)
+    F[:4096] = torch.from_numpy(a.view(np.int32)).to(dev)
+    G[:4096] = torch.from_numpy(b.view(np.int32)).to(dev)
+    torch.cuda.synchronize()
+    ref_dev = oracle.ref_gpu_time_polymul_dev(F.data_ptr(), G.data_ptr(), 13, P, 50)
+    ref_host = host_ms(lambda: oracle.ref_gpu_polymul(a, b, P), 20)
+    c1 = extras.get("c1_4095x4095") or {}
+    ours_dev = c1.get("device_us_per_call", float("nan")) / 1000
+    ours_host = c1.get("host_us_per_call", float("nan")) / 1000
+    out["c1_product_4095x4095"] = {"reference_device_ms": round(ref_dev, 4), "ours_device_ms": round(ours_dev, 4),
+                                   "ratio_device": round(ref_dev / ours_dev, 1),
+                                   "reference_host_ms": round(ref_host, 4), "ours_host_ms": round(ours_host, 4),
+                                   "ratio_host": round(ref_host / ours_host, 1)}
+    # C2: the 2^24 product and transform
+    n = 1 << LOGN
+    r = SplitMix64(0xC0DA0001)
+    a, b = r.residues(DEG + 1, P), r.residues(DEG + 1, P)
+    F = torch.zeros(n, dtype=torch.int32, device=dev)
+    G = torch.zeros(n, dtype=torch.int32, device=dev)
+    F[:DEG + 1] = torch.from_numpy(a.view(np.int32)).to(dev)
+    G[:DEG + 1] = torch.from_numpy(b.view(np.int32)).to(dev)
+    torch.cuda.synchronize()
+    ref_dev = oracle.ref_gpu_time_polymul_dev(F.data_ptr(), G.data_ptr(), LOGN, P, 3)
+    ref_host = host_ms(lambda: oracle.ref_gpu_polymul(a, b, P), 2)
+    out["c2_product_2^24"] = {"reference_device_ms": round(ref_dev, 3), "ours_device_ms": ours["product_ms"],
+                              "ratio_device": round(ref_dev / ours["product_ms"], 1),
+                              "reference_host_ms": round(ref_host, 2), "ours_host_ms": ours["host_product_ms"],
+                              "ratio_host": round(ref_host / ours["host_product_ms"], 1)}
+    w = oracle.primitive_root(LOGN, P)
+    ref_dev = oracle.ref_gpu_time_fft_dev(F.data_ptr(), LOGN, w, P, 3)  # F: any 2^24 device words
+    x = SplitMix64(0xC0DA0002).residues(n, P)
+    ref_host = host_ms(lambda: oracle.ref_gpu_fft(x, w, P), 2)
+    cm.fft_uni(x, w, P)
+    t0 = time.perf_counter()
+    for _ in range(2):
+        cm.fft_uni(x, w, P)
+    our_host = (time.perf_counter() - t0) * 1000 / 2
+    ntt = extras.get("ntt_2_24") or {}
+    our_dev = ntt.get("ms_per_transform", float("nan"))
+    out["c2_transform_2^24"] = {"reference_device_ms": round(ref_dev, 3), "ours_device_ms": our_dev,
+                                "ratio_device": round(ref_dev / our_dev, 1),
+                                "reference_host_ms": round(ref_host, 2), "ours_host_ms": round(our_host, 2),
+                                "ratio_host": round(ref_host / our_host, 1)}
+    # C4: 4096 pairs (the batched leg's seed), one host-to-host reference call per pair
+    r = SplitMix64(seed_for(3))
+    cnt = 4096
+    da = r.log_uniform_int(cnt, 32, 65536)
+    db = r.log_uniform_int(cnt, 32, 65536)
+    fa = r.residues(int((da + 1).sum()), P)
+    gb = r.residues(int((db + 1).sum()), P)
+    fo = np.concatenate([[0], np.cumsum(da + 1)])
+    go = np.concatenate([[0], np.cumsum(db + 1)])
+    pairs = [(fa[fo[i]:fo[i + 1]], gb[go[i]:go[i + 1]]) for i in range(cnt)]
+    small = [i for i in range(cnt) if (1 << int(da[i] + db[i]).bit_length()) < 256]
+    big = [i for i in range(cnt) if i not in set(small)]
+    with oracle.quiet_stdout():
+        oracle.ref_gpu_polymul(*pairs[big[0]], P)
+        t0 = time.perf_counter()
+        for i in big:
+            oracle.ref_gpu_polymul(*pairs[i], P)
+        ref_loop = (time.perf_counter() - t0) * 1000
+    cm.fftmul_batch(pairs, P)
+    t0 = time.perf_counter()
+    cm.fftmul_batch(pairs, P)
+    our_batch_host = (time.perf_counter() - t0) * 1000
+    c4 = extras.get("batched_c4") or {}
+    out["c4_4096_pairs"] = {"reference_loop_ms_host_to_host": round(ref_loop, 1),
+                            "reference_pairs_timed": len(big), "pairs_refused_by_reference_transform_below_256": len(small),
+                            "ours_batched_host_to_host_ms": round(our_batch_host, 2),
+                            "ratio_host": round(ref_loop / our_batch_host, 1),
+                            "ours_batched_device_ms": c4.get("ms_batched"),
+                            "ours_c_loop_device_ms": (c4.get("one_call_per_pair_c_loop") or {}).get("ms"),
+                            "note": "ours host-to-host covers all 4096 pairs (the refused ones included)"}
+    return out
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
 def cpu_baseline():
+    """modpn's own CPU product (the reference's CPU path) on this host: one product on one thread, and one
+    product per thread on every usable thread (capped by memory and at 64)."""
     import oracle
     if not oracle.ref_available():
         return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": "unavailable"}
-    threads = min(ref_threads_bounded(), 8)
+    one = modpn_sample(1, 1, 0xC0DA0001)
+    threads = ref_threads_bounded()
     secs = modpn_sample(threads, threads, 0xC0DA0001)
     return {"value": round(threads / secs, 4), "unit": UNIT, "cores": threads, "kind": "reference",
             "sample": f"{threads} products of degree 2^23-1 mod 469762049, one per host thread "
-                      f"({secs:.1f} s wall)"}
+                      f"({secs:.1f} s wall)",
+            "single_thread": {"value": round(1 / one, 4), "unit": UNIT, "cores": 1,
+                              "sample": f"1 product of degree 2^23-1 on one thread ({one:.2f} s)"},
+            "host_threads": host_threads(), "nproc": os.cpu_count(), "cpu_model": cpu_model()}
 
 
 def run_leg(name: str) -> None:
@@ -874,8 +1037,31 @@ def run_leg(name: str) -> None:
               "c3": lambda: c3_exact(cm, torch, dev, stream),
               "c4": lambda: batched_c4(cm, torch, dev, stream),
               "big": lambda: big_coefficients(cm, torch, dev, stream),
-              "serving": lambda: serving_c5(cm)}[name]
+              "serving": lambda: serving_c5(cm),
+              "refgpu": lambda: refgpu_leg(cm, torch, dev, stream, hbm_peak)}[name]
         print(json.dumps({"leg": name, "result": fn()}))
+
+
+def refgpu_leg(cm, torch, dev, stream, hbm_peak):
+    """reference_gpu on its own: the legs it compares with, then the reference's GPU path."""
+    extras = {"ntt_2_24": ntt_2_24(cm, torch, dev, stream, hbm_peak), "c1_4095x4095": c1_latency(cm, torch, dev, stream),
+              "batched_c4": batched_c4(cm, torch, dev, stream)}
+    ops = gen_operands(0xC0DA0001, 1)
+    a, b = ops[0]
+    dA = torch.from_numpy(a.view(np.int32)).to(dev)
+    dB = torch.from_numpy(b.view(np.int32)).to(dev)
+    n = 1 << LOGN
+    dH = torch.empty(n - 1, dtype=torch.int32, device=dev)
+    prod = lambda: cm.fftmul_uni_dev(dH.data_ptr(), n - 1, dA.data_ptr(), DEG, dB.data_ptr(), DEG, P,
+                                     stream.cuda_stream)
+    dev_ms = _timed(torch, stream, prod, reps=10, warm=3)
+    cm.fftmul_uni(a, b, P)
+    t0 = time.perf_counter()
+    for _ in range(3):
+        cm.fftmul_uni(a, b, P)
+    host_ms = (time.perf_counter() - t0) * 1000 / 3
+    return reference_gpu(cm, torch, dev, stream, extras, {"product_ms": round(dev_ms, 5),
+                                                          "host_product_ms": round(host_ms, 3)})
 
 
 def main():
@@ -886,7 +1072,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-extras", action="store_true",
                     help="headline only (no e2e extras, transform, batch or CPU legs); for profiling")
-    ap.add_argument("--leg", choices=["ntt", "c1", "c3", "c4", "big", "serving"],
+    ap.add_argument("--leg", choices=["ntt", "c1", "c3", "c4", "big", "serving", "refgpu"],
                     help="run only this extra leg and print its result (for profiling it alone)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

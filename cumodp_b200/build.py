@@ -5,7 +5,8 @@
 Each csrc/*.cu is compiled to an object under cumodp_b200/_build/ with
 ``nvcc -gencode arch=compute_100a,code=sm_100a``; the objects are linked into
 cumodp_b200/libcumodp.so against the CUDA runtime.  Rebuilds only what
-changed (sources or any header in csrc/ or include/).
+changed (sources or any header in csrc/ or include/).  bench/percall.c (the
+benchmark's one-call-per-product loop in C) becomes libcumodp_percall.so.
 """
 from __future__ import annotations
 
@@ -21,6 +22,7 @@ ROOT = os.path.dirname(HERE)
 SRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libcumodp.so")
+PERCALL = os.path.join(HERE, "libcumodp_percall.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
@@ -59,7 +61,23 @@ def build(force: bool = False, jobs: int = 8, ptxas_v: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    _build_percall(force)
     return LIB
+
+
+def _build_percall(force: bool) -> None:
+    """bench/percall.c -> libcumodp_percall.so: a C loop of one product call each (benchmark driver)."""
+    src = os.path.join(HERE, "bench", "percall.c")
+    if not os.path.exists(src):
+        return
+    if not force and os.path.exists(PERCALL) and os.path.getmtime(PERCALL) >= max(os.path.getmtime(src),
+                                                                                  os.path.getmtime(LIB)):
+        return
+    cmd = [os.environ.get("CC", "gcc"), "-O2", "-shared", "-fPIC", "-I" + os.path.join(ROOT, "include"), src,
+           "-o", PERCALL, "-L" + HERE, "-lcumodp", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"percall driver build failed:\n{r.stdout}\n{r.stderr}")
 
 
 if __name__ == "__main__":

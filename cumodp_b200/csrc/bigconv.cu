@@ -35,7 +35,7 @@
 #include <cstring>
 
 #include "../../include/cumodp.h"
-#include "product.cuh"
+#include "exact.cuh"
 
 namespace cmb {
 
@@ -116,25 +116,27 @@ int big_out_words(long long na, long long nb, int bw) {
     return (bits + 63) / 64;
 }
 
-// |x_j| (in_words words) and sign, one thread per coefficient.
+// |x_j| (in_words words) and sign, one coefficient per thread and step of a
+// grid-stride loop (the grid is capped by grid_of).
 __global__ void k_big_abs(const unsigned long long* __restrict__ x, long long len, int words,
                           unsigned long long* __restrict__ mag, unsigned char* __restrict__ neg) {
-    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (j >= len) return;
-    const unsigned long long* w = x + j * words;
-    unsigned long long* m = mag + j * words;
-    const bool s = (long long)w[words - 1] < 0;
-    unsigned long long carry = 1;
-    for (int i = 0; i < words; ++i) {
-        if (s) {
-            const unsigned long long v = ~w[i] + carry;
-            carry = (carry && v == 0) ? 1 : 0;
-            m[i] = v;
-        } else {
-            m[i] = w[i];
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < len;
+         j += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long* w = x + j * words;
+        unsigned long long* m = mag + j * words;
+        const bool s = (long long)w[words - 1] < 0;
+        unsigned long long carry = 1;
+        for (int i = 0; i < words; ++i) {
+            if (s) {
+                const unsigned long long v = ~w[i] + carry;
+                carry = (carry && v == 0) ? 1 : 0;
+                m[i] = v;
+            } else {
+                m[i] = w[i];
+            }
         }
+        neg[j] = s ? 1 : 0;
     }
-    neg[j] = s ? 1 : 0;
 }
 
 struct BigSplitArgs {
@@ -337,6 +339,12 @@ int bigconv_mul_dev(const unsigned long long* a, long long na, const unsigned lo
     C.c = c;
     k_big_crt<<<(unsigned)((lc + 127) / 128), 128, 0, st>>>(C);
     return cuda_err(cudaGetLastError());
+}
+
+int exact_i64_long_dev(const long long* a, long long la, const long long* b, long long lb, long long* c, int bw,
+                       cudaStream_t st) {
+    return bigconv_mul_dev((const unsigned long long*)a, la, (const unsigned long long*)b, lb, 1,
+                           (unsigned long long*)c, 2, bw, st, nullptr);
 }
 
 }  // namespace cmb

@@ -25,4 +25,11 @@ int twoconv_plan(int ba, int bb, long long la, long long lb, bool force_two_prim
 int twoconv_mul_dev(const long long* a, long long la, const long long* b, long long lb, long long* c, int ba,
                     int bb, bool force_two_prime, cudaStream_t st, TwoConvPlan* used, const TwoConvBufs* bufs);
 
+// The same product for lengths past the reference primes' transforms
+// (twoconv_plan: FFT_SIZE_TOO_LARGE): the big-coefficient path with one
+// 64-bit word per input coefficient and two per output coefficient, over
+// Fourier primes of 2-adic order >= 22 (bigconv.cu); library workspace.
+int exact_i64_long_dev(const long long* a, long long la, const long long* b, long long lb, long long* c, int bw,
+                       cudaStream_t st);
+
 }  // namespace cmb

@@ -20,6 +20,8 @@ enum WsSlot { kWsSingle = 0, kWsBatch = 1, kWsStage = 2, kWsNtt = 3, kWsTwoConv 
               kWsBiv = 6, kWsBivHost = 7, kWsBig = 8, kWsSplitProd = 9, kWsSplitIn = 10,
               kWsSplitNtt = 11 /* + (k - kMaxLog - 1) for a 2^k transform: 11..14 */, kWsBivT = 15,
               kWsListJobs = 16, kWsCyclic = 17 };
+// pinned host staging slots (runtime.cuh: pinned_workspace)
+enum PinSlot { kPinTwoConv = 0 };
 
 // SMs of device dev (cached per device).
 int sm_count(int dev);

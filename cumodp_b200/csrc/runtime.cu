@@ -53,6 +53,7 @@ struct Caches {
     std::map<std::tuple<int, u32, u32, int, int>, Tw*> tables;  // dev, p, root, logl, kind
     std::map<std::tuple<int, u32, u32, int>, u32*> seeds;
     std::map<std::pair<int, int>, std::pair<void*, size_t>> ws;
+    std::map<int, std::pair<void*, size_t>> pinned;
     std::map<int, cudaStream_t> streams;
 };
 
@@ -321,6 +322,25 @@ void* workspace(int dev, int slot, size_t bytes, int* err) {
     }
     e.second = sz;
     C.bytes += (long long)sz;
+    return e.first;
+}
+
+void* pinned_workspace(int slot, size_t bytes, int* err) {
+    Caches& C = caches();
+    std::lock_guard<std::mutex> g(C.m);
+    auto& e = C.pinned[slot];
+    if (e.second >= bytes && e.first) return e.first;
+    if (e.first) cudaFreeHost(e.first);  // synchronises with the device: no copy from it is in flight
+    e.first = nullptr;
+    e.second = 0;
+    const size_t sz = std::max<size_t>(bytes + bytes / 4, 1 << 16);
+    if (cudaHostAlloc(&e.first, sz, cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();
+        *err = OUT_OF_MEMORY;
+        e.first = nullptr;
+        return nullptr;
+    }
+    e.second = sz;
     return e.first;
 }
 

@@ -72,6 +72,10 @@ int seeds_into(u32 p, u32 root, int logn, u32* out, size_t cap);
 // lives).  Each call site names a slot so concurrent users do not collide.
 void* workspace(int dev, int slot, size_t bytes, int* err);
 
+// Pinned host staging that grows on demand (shared by every device; the
+// caller holds lib_mutex and keeps no copy from it in flight past its call).
+void* pinned_workspace(int slot, size_t bytes, int* err);
+
 // The stream every synchronous entry point issues its work on.
 cudaStream_t lib_stream(int dev);
 

@@ -334,6 +334,29 @@ int bw_host(const int64_t* x, long long n) {
 
 }  // namespace
 
+namespace cmb {
+namespace {
+
+// The two-convolution product (the reference's primes, 962592769,
+// 950009857, 940572673) where its plan exists; longer products (transforms
+// past 2^21, which those primes do not have) through the big-coefficient
+// path over primes of higher 2-adic order.  method 1 (the forced two-prime
+// split of the reference's scheme) has no such fallback.
+int exact_i64_any_len(const int64_t* a, long long na, const int64_t* b, long long nb, int64_t* c, int ba, int bb,
+                      int method, cudaStream_t st) {
+    TwoConvPlan pl;
+    const int pe = twoconv_plan(ba, bb, na, nb, method == 1, &pl);
+    if (pe == FFT_SIZE_TOO_LARGE && method != 1)
+        return exact_i64_long_dev((const long long*)a, na, (const long long*)b, nb, (long long*)c, std::max(ba, bb),
+                                  st);
+    if (pe != OK) return pe;
+    return twoconv_mul_dev((const long long*)a, na, (const long long*)b, nb, (long long*)c, ba, bb, method == 1, st,
+                           nullptr, nullptr);
+}
+
+}  // namespace
+}  // namespace cmb
+
 extern "C" {
 
 int cumodp_twoconv_bit_width(long long na, const int64_t* a, long long nb, const int64_t* b) {
@@ -360,12 +383,11 @@ cumodp_err cumodp_twoconv_mul_i64_dev(long long na, const int64_t* a, long long 
         cudaGetLastError();
         return CUMODP_NO_CUDA_DEVICE;
     }
-    if (na <= 0 || nb <= 0 || !a || !b || !c || bit_width <= 0 || bit_width > 63 || na + nb - 1 > (1ll << 21))
+    if (na <= 0 || nb <= 0 || !a || !b || !c || bit_width <= 0 || bit_width > 63 || na + nb - 1 > (1ll << 25))
         return CUMODP_ASSUMPTION_ERROR;
     std::lock_guard<std::mutex> g(lib_mutex());
     cudaStream_t st = stream ? (cudaStream_t)stream : lib_stream(current_device());
-    int e = twoconv_mul_dev((const long long*)a, na, (const long long*)b, nb, (long long*)c, bit_width, bit_width,
-                            method == 1, st, nullptr, nullptr);
+    int e = exact_i64_any_len(a, na, b, nb, c, bit_width, bit_width, method, st);
     if (e == OK && !stream) e = cuda_err(cudaStreamSynchronize(st));
     return (cumodp_err)e;
 }
@@ -377,27 +399,34 @@ cumodp_err cumodp_twoconv_mul_i64(long long na, const int64_t* a, long long nb, 
         cudaGetLastError();
         return CUMODP_NO_CUDA_DEVICE;
     }
-    if (na <= 0 || nb <= 0 || !a || !b || !c || na + nb - 1 > (1ll << 21)) return CUMODP_ASSUMPTION_ERROR;
+    if (na <= 0 || nb <= 0 || !a || !b || !c || na + nb - 1 > (1ll << 25)) return CUMODP_ASSUMPTION_ERROR;
     const int ba = bw_host(a, na), bb = bw_host(b, nb);
     std::lock_guard<std::mutex> g(lib_mutex());
     const int dev = current_device();
     cudaStream_t st = lib_stream(dev);
     const long long lc = na + nb - 1;
+    const size_t in_bytes = (size_t)(na + nb) * 8, out_bytes = (size_t)lc * 16;
     int err = OK;
-    long long* d = (long long*)workspace(dev, kWsStage, (size_t)(na + nb + 2 * lc) * 8, &err);
+    long long* d = (long long*)workspace(dev, kWsStage, in_bytes + out_bytes, &err);
     if (!d) return (cumodp_err)err;
+    // the operands and the result pass through pinned staging: one copy each way
+    char* hs = (char*)pinned_workspace(kPinTwoConv, std::max(in_bytes, out_bytes), &err);
+    if (!hs) return (cumodp_err)err;
+    memcpy(hs, a, (size_t)na * 8);
+    memcpy(hs + (size_t)na * 8, b, (size_t)nb * 8);
     long long *da = d, *db = d + na, *dc = d + na + nb;
-    cudaError_t ce = cudaMemcpyAsync(da, a, (size_t)na * 8, cudaMemcpyHostToDevice, st);
-    if (ce == cudaSuccess) ce = cudaMemcpyAsync(db, b, (size_t)nb * 8, cudaMemcpyHostToDevice, st);
+    cudaError_t ce = cudaMemcpyAsync(da, hs, in_bytes, cudaMemcpyHostToDevice, st);
     if (ce != cudaSuccess) return (cumodp_err)cuda_err(ce);
-    err = twoconv_mul_dev(da, na, db, nb, dc, ba, bb, method == 1, st, nullptr, nullptr);
-    if (err != OK) {
+    err = exact_i64_any_len((const int64_t*)da, na, (const int64_t*)db, nb, (int64_t*)dc, ba, bb, method, st);
+    if (err == OK) {
+        ce = cudaMemcpyAsync(hs, dc, out_bytes, cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+        err = cuda_err(ce);
+    } else {
         cudaStreamSynchronize(st);
-        return (cumodp_err)err;
     }
-    ce = cudaMemcpyAsync(c, dc, (size_t)lc * 16, cudaMemcpyDeviceToHost, st);
-    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
-    return (cumodp_err)cuda_err(ce);
+    if (err == OK) memcpy(c, hs, out_bytes);
+    return (cumodp_err)err;
 }
 
 }  // extern "C"

@@ -201,8 +201,13 @@ cumodp_err cumodp_fftmul_batch(int count, const sfixn *df, const int64_t *f_off,
  * negacyclic x-convolutions mod Fourier primes 962592769, 950009857,
  * 940572673, CRT, (u+v)/2 + 2^N (u-v)/2.  method 0 picks the cheapest exact
  * (K, M, primes); method 1 forces the smallest limb split that needs only
- * two primes.  Returns CUMODP_ASSUMPTION_ERROR when the exact product does
- * not fit 127 bits, CUMODP_FFT_SIZE_TOO_LARGE beyond 2^21 coefficients. */
+ * two primes.  Products longer than those primes' transforms allow (past
+ * 2^21 coefficients, or past 2^20 where the plan needs 940572673) run, for
+ * method 0, on the big-coefficient path (cumodp_twoconv_mul_big's planner,
+ * Fourier primes of 2-adic order >= 22), up to 2^25 coefficients.  Host
+ * arrays pass through pinned staging (one copy each way).  Returns
+ * CUMODP_ASSUMPTION_ERROR when the exact product does not fit 127 bits or
+ * na + nb - 1 > 2^25, CUMODP_FFT_SIZE_TOO_LARGE when no plan exists. */
 cumodp_err cumodp_twoconv_mul_i64(long long na, const int64_t *a, long long nb, const int64_t *b, int64_t *c,
                                   int method);
 /* Addition.  Same on DEVICE pointers, on a caller stream (0 = library stream,

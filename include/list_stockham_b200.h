@@ -22,8 +22,10 @@ inline cumodp_err list_stockham_dev(sfixn *X, sfixn m, sfixn k, sfixn w, sfixn p
 }
 
 inline cumodp_err list_stockham_dev(sfixn *X, sfixn m, sfixn k, const sfixn *W, sfixn p) {
-    sfixn w = 1;
-    if (k > 0 && cudaMemcpy(&w, W + 1, sizeof(sfixn), cudaMemcpyDeviceToHost) != cudaSuccess)
+    /* W[i] = w^i for i < n/2: W[1] is the root for k >= 2; for k = 1 the
+     * table holds only w^0 and the root is p - 1 */
+    sfixn w = k == 1 ? p - 1 : 1;
+    if (k >= 2 && cudaMemcpy(&w, W + 1, sizeof(sfixn), cudaMemcpyDeviceToHost) != cudaSuccess)
         return CUMODP_FFT_ERROR;
     return cumodp_list_fft_dev(X, m, k, w, p, 0, 0);
 }

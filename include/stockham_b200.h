@@ -14,7 +14,8 @@
  *   stockham_dev(X, n, k, w, p)          X <- DFT_n(X) with root w
  *                                        (src/stockham.cu:413-434)
  *   stockham_dev(X, n, k, W, p)          the same with the device table of
- *                                        powers W[i] = w^i; W[1] is the root
+ *                                        powers W[i] = w^i (i < n/2); W[1] is
+ *                                        the root (p - 1 for k = 1)
  *                                        (src/stockham.cu:437-453)
  *   inverse_stockham_dev(X, n, k, w, p)  X <- n^-1 DFT_n(X) with root w^-1
  *                                        (src/stockham.cu:462-467)
@@ -47,10 +48,12 @@ inline sfixn inv_mod_p(sfixn a, sfixn p) {
     }
     return (sfixn)r;
 }
-/* W[1] of a device table of powers (the root), or 1 for k = 0. */
-inline cumodp_err root_from_table(const sfixn *W, sfixn k, sfixn *w) {
-    *w = 1;
-    if (k > 0 && cudaMemcpy(w, W + 1, sizeof(sfixn), cudaMemcpyDeviceToHost) != cudaSuccess)
+/* The root of a device table of powers W[i] = w^i, i < n/2: W[1] for
+ * k >= 2; for k = 1 the table holds only w^0 and the root is p - 1 (the only
+ * primitive square root of unity); 1 for k = 0. */
+inline cumodp_err root_from_table(const sfixn *W, sfixn k, sfixn p, sfixn *w) {
+    *w = k == 1 ? p - 1 : 1;
+    if (k >= 2 && cudaMemcpy(w, W + 1, sizeof(sfixn), cudaMemcpyDeviceToHost) != cudaSuccess)
         return CUMODP_FFT_ERROR;
     return CUMODP_SUCCESS;
 }
@@ -65,7 +68,7 @@ inline cumodp_err stockham_dev(sfixn *X, sfixn n, sfixn k, sfixn w, sfixn p) {
 inline cumodp_err stockham_dev(sfixn *X, sfixn n, sfixn k, const sfixn *W, sfixn p) {
     if (!cumodp_detail::length_ok(n, k)) return CUMODP_ASSUMPTION_ERROR;
     sfixn w = 1;
-    cumodp_err e = cumodp_detail::root_from_table(W, k, &w);
+    cumodp_err e = cumodp_detail::root_from_table(W, k, p, &w);
     return e != CUMODP_SUCCESS ? e : cumodp_fft_uni_dev(X, n, k, w, p, 0, 0);
 }
 
@@ -77,7 +80,7 @@ inline cumodp_err inverse_stockham_dev(sfixn *X, sfixn n, sfixn k, sfixn w, sfix
 inline cumodp_err inverse_stockham_dev(sfixn *X, sfixn n, sfixn k, const sfixn *W, sfixn p) {
     if (!cumodp_detail::length_ok(n, k)) return CUMODP_ASSUMPTION_ERROR;
     sfixn wi = 1;
-    cumodp_err e = cumodp_detail::root_from_table(W, k, &wi);
+    cumodp_err e = cumodp_detail::root_from_table(W, k, p, &wi);
     if (e != CUMODP_SUCCESS) return e;
     if (wi <= 0 || wi >= p) return CUMODP_ASSUMPTION_ERROR;
     return cumodp_fft_uni_dev(X, n, k, cumodp_detail::inv_mod_p(wi, p), p, 1, 0);

@@ -338,19 +338,82 @@ def ref_gpu_polymul(a: np.ndarray, b: np.ndarray, p: int) -> np.ndarray:
     reference itself (it returns with H untouched), so callers keep to
     len(a) + len(b) - 1 > 128.
     """
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.uint32).view(np.int32))
+    b = np.ascontiguousarray(np.asarray(b, dtype=np.uint32).view(np.int32))
+    dh = len(a) + len(b) - 2
+    h = np.zeros(dh + 1, dtype=np.int32)
+    rc = _ref_gpu_lib().ref_gpu_fftmul(dh, h, len(a) - 1, a, len(b) - 1, b, p)
+    if rc != 0:
+        raise RuntimeError(f"reference GPU product failed: CUDA error {rc}")
+    return h.view(np.uint32)
+
+
+def _ref_gpu_lib():
     global _rg
     if _rg is None:
         _rg = C.CDLL(REF_GPU_SO)
         _rg.ref_gpu_fftmul.restype = C.c_int
         _rg.ref_gpu_fftmul.argtypes = [C.c_int, _i32p, C.c_int, _i32p, C.c_int, _i32p, C.c_int]
-    a = np.ascontiguousarray(np.asarray(a, dtype=np.uint32).view(np.int32))
-    b = np.ascontiguousarray(np.asarray(b, dtype=np.uint32).view(np.int32))
-    dh = len(a) + len(b) - 2
-    h = np.zeros(dh + 1, dtype=np.int32)
-    rc = _rg.ref_gpu_fftmul(dh, h, len(a) - 1, a, len(b) - 1, b, p)
+        _rg.ref_gpu_fft_host.restype = C.c_int
+        _rg.ref_gpu_fft_host.argtypes = [_i32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+        _rg.ref_gpu_time_fft_dev.restype = C.c_int
+        _rg.ref_gpu_time_fft_dev.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                             C.POINTER(C.c_float)]
+        _rg.ref_gpu_time_polymul_dev.restype = C.c_int
+        _rg.ref_gpu_time_polymul_dev.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                                 C.POINTER(C.c_float)]
+    return _rg
+
+
+def ref_gpu_fft(x: np.ndarray, w: int, p: int, inverse: bool = False) -> np.ndarray:
+    """The reference's own GPU transform, host to host: stockham_host, or
+    inverse_stockham_host with the forward root w (src/stockham.cu:479-503)."""
+    x = np.array(np.asarray(x, dtype=np.uint32).view(np.int32), copy=True)
+    k = int(len(x)).bit_length() - 1
+    assert len(x) == 1 << k
+    rc = _ref_gpu_lib().ref_gpu_fft_host(x, len(x), k, w, p, int(inverse))
+    if rc != 0:
+        raise RuntimeError(f"reference GPU transform failed: CUDA error {rc}")
+    return x.view(np.uint32)
+
+
+def ref_gpu_time_fft_dev(x_ptr: int, k: int, w: int, p: int, reps: int) -> float:
+    """Mean ms of the reference's stockham_dev on a device array (CUDA events)."""
+    ms = C.c_float(0)
+    rc = _ref_gpu_lib().ref_gpu_time_fft_dev(x_ptr, 1 << k, k, w, p, reps, C.byref(ms))
+    if rc != 0:
+        raise RuntimeError(f"reference GPU transform failed: CUDA error {rc}")
+    return float(ms.value)
+
+
+def ref_gpu_time_polymul_dev(f_ptr: int, g_ptr: int, e: int, p: int, reps: int) -> float:
+    """Mean ms of the reference's stockham_poly_mul_dev on device arrays of 2^e words (CUDA events)."""
+    ms = C.c_float(0)
+    rc = _ref_gpu_lib().ref_gpu_time_polymul_dev(f_ptr, g_ptr, 1 << e, e, p, reps, C.byref(ms))
     if rc != 0:
         raise RuntimeError(f"reference GPU product failed: CUDA error {rc}")
-    return h.view(np.uint32)
+    return float(ms.value)
+
+
+class quiet_stdout:
+    """Sends file descriptor 1 to /dev/null while the reference's GPU product
+    runs: stockham_poly_mul_host prints its timing to stdout on every call
+    (src/stockham.cu:600), which would mix with a caller's own output."""
+
+    def __enter__(self):
+        import sys
+        sys.stdout.flush()
+        self._saved = os.dup(1)
+        self._null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self._null, 1)
+        return self
+
+    def __exit__(self, *exc):
+        C.CDLL(None).fflush(None)
+        os.dup2(self._saved, 1)
+        os.close(self._saved)
+        os.close(self._null)
+        return False
 
 
 def ref_polymul_batch(pairs, p: int, threads: int):

@@ -131,8 +131,9 @@ def test_poly_mul_host(drv, oracle_mod, df, dg, dh):
 
 
 @pytest.mark.parametrize("use_table", [0, 1])
-def test_list_overloads(drv, oracle_mod, use_table):
-    m, k = 5, 10
+@pytest.mark.parametrize("k", [1, 10])
+def test_list_overloads(drv, oracle_mod, use_table, k):
+    m = 5
     x = SplitMix64(1400 + use_table).residues(m << k, P)
     w = oracle_mod.primitive_root(k, P)
     X = x.view(np.int32).copy()
