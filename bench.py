@@ -828,31 +828,52 @@ def c1_latency(cm, torch, dev, stream):
             "batched_mulmods_per_s": round(R * 167936 / (batch_ms / 1000), 1), "batched_equals_single": same}
 
 
+def _page_aligned(values: np.ndarray) -> np.ndarray:
+    """A copy of `values` in page-aligned memory (what page-locking registers)."""
+    buf = np.empty(values.nbytes + 4096, np.uint8)
+    off = (-buf.ctypes.data) % 4096
+    out = buf[off:off + values.nbytes].view(values.dtype)
+    out[:] = values
+    return out
+
+
 def serving_c5(cm, rates=(1000, 3000, 10000, 30000, 100000), max_requests=20000, max_seconds=2.0, threads=4):
     """Config 5: Poisson arrivals of mixed requests into the continuous-batching server.
 
     Degrees log-uniform in [2^5, 2^20]; prime uniform over {469762049,
     754974721, 962592769}; 20% exact int64 products (|c| <= 10^10, degrees
-    capped at 2^14 so the 127-bit bound holds).  The trace is replayed
-    open-loop by the library's native replay threads (cumodp_server_replay):
-    request i is submitted at its arrival time whatever happened before, and
-    its latency runs from the scheduled arrival to the result in a host
-    buffer.  Each rate replays min(max_requests, rate * max_seconds)
-    requests.  Requests whose product exceeds the prime's 2-adic order
-    (962592769 supports 2^21 points) are answered with
-    CUMODP_FFT_SIZE_TOO_LARGE and counted as rejected; requests shed by the
-    server's pinned host budget are counted as shed.
+    log-uniform in [2^5, 2^20] too).  The trace is replayed open-loop by the
+    library's native replay threads (cumodp_server_replay): request i is
+    submitted at its arrival time whatever happened before, and its latency
+    runs from the scheduled arrival to the result in a host buffer.  Each
+    rate replays min(max_requests, rate * max_seconds) requests.  The operand
+    pools are registered with the server (cumodp_server_register), so
+    operands go to the device straight from them, and each result lands in
+    the server's pinned slab (the replay gives no output buffer): operands
+    and results cross the host link with no host copy.  Requests whose
+    product exceeds the prime's 2-adic order (962592769 supports 2^21 points)
+    are answered with CUMODP_FFT_SIZE_TOO_LARGE and counted as rejected;
+    requests shed by the server's host budget (4 GiB of unfinished operand
+    and result bytes) are counted as shed.  `link_ceiling_per_s` is the rate
+    the measured host link allows for the trace's mean request (its operand
+    bytes at the measured host-to-device bandwidth, its result bytes at the
+    device-to-host one, both directions busy at once).
     """
+    import torch
     from cumodp_b200.workloads import SplitMix64, seed_for
     primes = (469762049, 754974721, 962592769)
     r = SplitMix64(seed_for(4))
-    pool_u = r.residues(1 << 21, 469762049)        # operand slices come from these pools
-    pool_i = r.int64_in(1 << 15, 10**10)
+    pool_u = _page_aligned(r.residues((1 << 21) + 2, 469762049))  # operand slices come from these pools
+    pool_i = _page_aligned(r.int64_in((1 << 21) + 2, 10**10))
+    link = host_link_bound(torch, torch.device("cuda", torch.cuda.current_device()), 64 << 20, 64 << 20)
+    link_bps = link["gbs_per_direction"] * 1e9
     out = {}
-    with cm.Server(max_batch=256, batch_window_us=50, lanes=4) as srv:
+    with cm.Server(max_batch=256, batch_window_us=50, lanes=4, host_budget=4 << 30) as srv:
+        srv.register(pool_u)
+        srv.register(pool_i)
         # warm-up: tables for every prime and size class, lane buffers
         warm = [(pool_u[:(1 << k) + 1], pool_u[:(1 << k) + 1], p) for p in primes for k in range(4, 21)]
-        warm += [(pool_i[:(1 << k) + 1], pool_i[:(1 << k) + 1], None) for k in range(4, 15)]
+        warm += [(pool_i[:(1 << k) + 1], pool_i[:(1 << k) + 1], None) for k in range(4, 21)]
         srv.replay(np.zeros(len(warm)), warm, threads=threads)
         for rate in rates:
             n = int(min(max_requests, rate * max_seconds))
@@ -865,9 +886,8 @@ def serving_c5(cm, rates=(1000, 3000, 10000, 30000, 100000), max_requests=20000,
             reqs = []
             for i in range(n):
                 if kind[i] < 0.2:
-                    a = pool_i[offs[i] % (1 << 14):][: min(int(da[i]), 1 << 14) + 1]
-                    b = pool_i[offs[n + i] % (1 << 14):][: min(int(db[i]), 1 << 14) + 1]
-                    reqs.append((a, b, None))
+                    reqs.append((pool_i[offs[i]:offs[i] + int(da[i]) + 1],
+                                 pool_i[offs[n + i]:offs[n + i] + int(db[i]) + 1], None))
                 else:
                     reqs.append((pool_u[offs[i]:offs[i] + int(da[i]) + 1],
                                  pool_u[offs[n + i]:offs[n + i] + int(db[i]) + 1], primes[pidx[i]]))
@@ -878,6 +898,8 @@ def serving_c5(cm, rates=(1000, 3000, 10000, 30000, 100000), max_requests=20000,
             pct = (lambda q: round(float(lat_ok[min(len(lat_ok) - 1, int(q * len(lat_ok)))]), 3)) \
                 if len(lat_ok) else (lambda q: None)
             in_bytes = sum(a.nbytes + b.nbytes for a, b, _ in reqs)
+            res_bytes = sum((len(a) + len(b) - 1) * (16 if p is None else 4) for a, b, p in reqs)
+            ceiling = n / max(in_bytes / link_bps, res_bytes / link_bps)
             out[str(rate)] = {"requests": n, "completed": int(ok.sum()),
                               "rejected_size": int((st == cm.FFT_SIZE_TOO_LARGE).sum()),
                               "shed": int((st == cm.OUT_OF_MEMORY).sum()),
@@ -887,7 +909,9 @@ def serving_c5(cm, rates=(1000, 3000, 10000, 30000, 100000), max_requests=20000,
                               "products_per_s": round(ok.sum() / (span_us * 1e-6), 1),
                               "offered_per_s": round(n / (arrival[-1] * 1e-6), 1),
                               "operand_gb_per_s": round(in_bytes / (span_us * 1e3), 2),
-                              "batches": srv.stats()["batches"], "replay_threads": threads}
+                              "link_ceiling_per_s": round(ceiling, 1),
+                              "batches": srv.stats()["batches"], "replay_threads": threads,
+                              "copies": "registered operand pools, results in pinned slabs: no host copy"}
     return out
 
 

@@ -166,6 +166,10 @@ def _lib():
         L.cumodp_server_replay.argtypes = [C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
                                            C.c_void_p, C.POINTER(C.c_double)]
+        L.cumodp_server_register.restype = C.c_int
+        L.cumodp_server_register.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
+        L.cumodp_server_unregister.restype = C.c_int
+        L.cumodp_server_unregister.argtypes = [C.c_void_p, C.c_void_p]
         L.cumodp_server_get_stats.restype = None
         L.cumodp_server_get_stats.argtypes = [C.c_void_p, C.POINTER(ServerStats)]
         L.cumodp_server_reset_stats.restype = None
@@ -496,6 +500,7 @@ class Server:
         if not self._h:
             raise CumodpError(NO_CUDA_DEVICE, "cumodp_server_create")
         self._outs = {}
+        self._regs = []
 
     def submit_mod(self, F, G, p: int):
         f = _as_i32(F)
@@ -561,6 +566,18 @@ class Server:
                "cumodp_server_replay")
         return st, lat, span.value
 
+    def register(self, arr: np.ndarray) -> None:
+        """Registers a C-contiguous host array (``cumodp_server_register``): requests whose operands or
+        outputs lie in it skip the server's pinned staging copies.  Keep the array alive, and unchanged
+        while requests read it, until unregister (or close)."""
+        assert arr.flags["C_CONTIGUOUS"]
+        _check(_lib().cumodp_server_register(self._h, arr.ctypes.data, arr.nbytes), "cumodp_server_register")
+        self._regs.append(arr)
+
+    def unregister(self, arr: np.ndarray) -> None:
+        _check(_lib().cumodp_server_unregister(self._h, arr.ctypes.data), "cumodp_server_unregister")
+        self._regs = [a for a in self._regs if a is not arr]
+
     def poll(self, rid: int) -> int:
         return int(_lib().cumodp_server_poll(self._h, rid))
 
@@ -580,8 +597,9 @@ class Server:
 
     def close(self) -> None:
         if self._h:
-            _lib().cumodp_server_destroy(self._h)
+            _lib().cumodp_server_destroy(self._h)  # drains, then unregisters what is left
             self._h = None
+            self._regs = []
 
     def __enter__(self):
         return self

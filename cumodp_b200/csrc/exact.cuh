@@ -19,6 +19,9 @@ struct TwoConvBufs {
 };
 
 void twoconv_buffer_sizes(long long la, long long lb, size_t* eval_words, size_t* ws_words, size_t* job_bytes);
+// The same for the plan the product will use (exact, not the worst case).
+void twoconv_buffer_sizes_plan(long long la, long long lb, const TwoConvPlan& pl, size_t* eval_words,
+                               size_t* ws_words, size_t* job_bytes);
 int twoconv_plan(int ba, int bb, long long la, long long lb, bool force_two_prime, TwoConvPlan* out);
 // c (lo, hi pairs, la+lb-1 coefficients) = a * b exactly, device pointers;
 // bufs == nullptr uses the library workspace and graph-launched batches.

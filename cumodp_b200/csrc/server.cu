@@ -28,6 +28,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <thread>
 #include <unordered_map>
 #include <unordered_set>
@@ -122,6 +123,10 @@ struct PinnedPool {
         }
         free_blocks[o].insert(blk);
     }
+    size_t used() {
+        std::lock_guard<std::mutex> g(m);
+        return in_use;
+    }
     ~PinnedPool() {
         for (char* ch : chunks) cudaFreeHost(ch);
     }
@@ -135,7 +140,14 @@ struct Req {
     void* in = nullptr;   // pinned: operands (kind 0: u32 A then B; kind 1: int64 A then B)
     void* res = nullptr;  // pinned: result (kind 0: la+lb-1 u32; kind 1: 2(la+lb-1) int64)
     size_t in_bytes = 0, res_bytes = 0;
+    // operands in memory registered with the server: copied to the device
+    // from there (in stays null); res_direct: the result goes straight into out
+    const void* a_src = nullptr;
+    const void* b_src = nullptr;
+    bool res_direct = false;
+    size_t direct_bytes = 0;  // bytes of this request counted in Server::direct_inflight
     int bw = 1;
+    TwoConvPlan plan{0, 0, 0, 0};  // exact products: the plan (sizes the lane buffers)
     void* out;
     size_t bytes;
     double t_submit = 0, t_done = 0;
@@ -223,6 +235,10 @@ struct Server {
     std::unordered_map<long long, Req*> reqs;
     std::vector<Lane> lanes;
     PinnedPool pool;
+    // host ranges registered by the caller (cumodp_server_register): start -> bytes
+    std::mutex reg_m;
+    std::map<uintptr_t, size_t> regs;
+    std::atomic<size_t> direct_inflight{0};  // operand and result bytes of unfinished direct requests
     std::deque<int> dispatched;  // lane indices in dispatch order
     size_t inflight = 0;
     long long next_id = 1, lane_seq = 0;
@@ -239,6 +255,8 @@ struct Server {
 
 namespace {
 
+constexpr size_t kBatchBytes = 1ull << 30;
+
 size_t req_bytes(const Req& r) {
     const long long lc = r.la + r.lb - 1;
     if (r.kind == 0) {
@@ -247,8 +265,70 @@ size_t req_bytes(const Req& r) {
         return (size_t)(r.la + r.lb + lc + ws) * 4 + 256;
     }
     size_t ev, ws, jb;
-    twoconv_buffer_sizes(r.la, r.lb, &ev, &ws, &jb);
+    twoconv_buffer_sizes_plan(r.la, r.lb, r.plan, &ev, &ws, &jb);
     return (r.la + r.lb + 2 * lc) * 8 + (ev + ws) * 4 + jb;
+}
+
+// Whether [p, p + n) lies in one range registered with the server.
+bool registered(Server& S, const void* p, size_t n) {
+    const uintptr_t a = (uintptr_t)p;
+    std::lock_guard<std::mutex> g(S.reg_m);
+    auto it = S.regs.upper_bound(a);
+    if (it == S.regs.begin()) return false;
+    --it;
+    return a >= it->first && a + n <= it->first + it->second;
+}
+
+// Records [p, p + n) (already page-locked) as registered; false if it
+// overlaps a recorded range.
+bool register_range(Server& S, const void* p, size_t n) {
+    const uintptr_t a = (uintptr_t)p;
+    std::lock_guard<std::mutex> g(S.reg_m);
+    auto it = S.regs.lower_bound(a);
+    if (it != S.regs.end() && it->first < a + n) return false;
+    if (it != S.regs.begin()) {
+        auto pr = std::prev(it);
+        if (pr->first + pr->second > a) return false;
+    }
+    S.regs[a] = n;
+    return true;
+}
+
+// Places a request's operands and result: straight from and into the
+// caller's memory where it lies in registered ranges (no copy on the host),
+// else in pinned slabs (the operands copied there now).  Unfinished requests
+// may hold at most the host budget -- slab bytes plus the bytes of direct
+// requests -- beyond which the request is shed (CUMODP_OUT_OF_MEMORY).
+void stage_request(Server& S, Req* r, const void* a, size_t abytes, const void* b, size_t bbytes) {
+    const bool in_reg = registered(S, a, abytes) && registered(S, b, bbytes);
+    const bool out_reg = registered(S, r->out, r->res_bytes);
+    const size_t direct = (in_reg ? abytes + bbytes : 0) + (out_reg ? r->res_bytes : 0);
+    const size_t slab = (in_reg ? 0 : r->in_bytes) + (out_reg ? 0 : r->res_bytes);
+    if (S.pool.used() + S.direct_inflight.load() + direct + slab > S.pool.limit) {
+        r->status = OUT_OF_MEMORY;  // shed: the backlog already holds the whole budget
+        return;
+    }
+    if (in_reg) {
+        r->a_src = a;
+        r->b_src = b;
+    } else if (!(r->in = S.pool.get(r->in_bytes))) {
+        r->status = OUT_OF_MEMORY;
+        return;
+    }
+    if (out_reg) {
+        r->res_direct = true;
+    } else if (!(r->res = S.pool.get(r->res_bytes))) {
+        S.pool.put(r->in, r->in_bytes);
+        r->in = nullptr;
+        r->status = OUT_OF_MEMORY;
+        return;
+    }
+    if (r->in) {
+        memcpy(r->in, a, abytes);
+        memcpy((char*)r->in + abytes, b, bbytes);
+    }
+    r->direct_bytes = direct;
+    S.direct_inflight += direct;
 }
 
 void finish(Server& S, Req* r, int status) {
@@ -296,7 +376,14 @@ int run_batch(Server& S, Lane& L) {
         size_t o = 0, q = 0;
         for (int i = 0; i < cnt; ++i) {
             Req* r = L.reqs[i];
-            cudaError_t ce = cudaMemcpyAsync(L.din.p + o, r->in, (r->la + r->lb) * 4, cudaMemcpyHostToDevice, L.st);
+            cudaError_t ce;
+            if (r->a_src) {  // straight from the caller's registered memory
+                ce = cudaMemcpyAsync(L.din.p + o, r->a_src, r->la * 4, cudaMemcpyHostToDevice, L.st);
+                if (ce == cudaSuccess)
+                    ce = cudaMemcpyAsync(L.din.p + o + r->la, r->b_src, r->lb * 4, cudaMemcpyHostToDevice, L.st);
+            } else {
+                ce = cudaMemcpyAsync(L.din.p + o, r->in, (r->la + r->lb) * 4, cudaMemcpyHostToDevice, L.st);
+            }
             if (ce != cudaSuccess) return cuda_err(ce);
             pa[i] = L.din.p + o;
             pb[i] = L.din.p + o + r->la;
@@ -310,7 +397,9 @@ int run_batch(Server& S, Lane& L) {
                            L.djobs.p, L.hjobs.p, L.st, false);
         if (err != OK) return err;
         for (int i = 0; i < cnt; ++i) {
-            cudaError_t ce = cudaMemcpyAsync(L.reqs[i]->res, ph[i], lh[i] * 4, cudaMemcpyDeviceToHost, L.st);
+            Req* r = L.reqs[i];
+            cudaError_t ce = cudaMemcpyAsync(r->res_direct ? r->out : r->res, ph[i], lh[i] * 4,
+                                             cudaMemcpyDeviceToHost, L.st);
             if (ce != cudaSuccess) return cuda_err(ce);
         }
     } else {
@@ -320,7 +409,7 @@ int run_batch(Server& S, Lane& L) {
             nin += r->la + r->lb;
             nout += 2 * (r->la + r->lb - 1);
             size_t e, w, j;
-            twoconv_buffer_sizes(r->la, r->lb, &e, &w, &j);
+            twoconv_buffer_sizes_plan(r->la, r->lb, r->plan, &e, &w, &j);
             evw = std::max(evw, e);
             wsw = std::max(wsw, w);
             jbb += j;
@@ -329,26 +418,36 @@ int run_batch(Server& S, Lane& L) {
         if ((err = L.din.ensure(2 * nin, L.st)) || (err = L.dout.ensure(2 * nout + evw, L.st)) ||
             (err = L.ws.ensure(wsw + 1, L.st)) || (err = L.djobs.ensure(jbb, L.st)) || (err = L.hjobs.ensure(jbb)))
             return err;
+        L.t_alloc = now_us();
         size_t o = 0, q = 0, jo = 0;
         u32* eval = L.dout.p + 2 * nout;
         long long* din64 = (long long*)L.din.p;
         long long* dout64 = (long long*)L.dout.p;
         for (int i = 0; i < cnt; ++i) {
             Req* r = L.reqs[i];
-            cudaError_t ce = cudaMemcpyAsync(din64 + o, r->in, (r->la + r->lb) * 8, cudaMemcpyHostToDevice, L.st);
+            cudaError_t ce;
+            if (r->a_src) {
+                ce = cudaMemcpyAsync(din64 + o, r->a_src, r->la * 8, cudaMemcpyHostToDevice, L.st);
+                if (ce == cudaSuccess)
+                    ce = cudaMemcpyAsync(din64 + o + r->la, r->b_src, r->lb * 8, cudaMemcpyHostToDevice, L.st);
+            } else {
+                ce = cudaMemcpyAsync(din64 + o, r->in, (r->la + r->lb) * 8, cudaMemcpyHostToDevice, L.st);
+            }
             if (ce != cudaSuccess) return cuda_err(ce);
             TwoConvBufs B{eval, L.ws.p, L.djobs.p + jo, L.hjobs.p + jo};
             size_t e, w, j;
-            twoconv_buffer_sizes(r->la, r->lb, &e, &w, &j);
+            twoconv_buffer_sizes_plan(r->la, r->lb, r->plan, &e, &w, &j);
             err = twoconv_mul_dev(din64 + o, r->la, din64 + o + r->la, r->lb, dout64 + 2 * q, r->bw, r->bw, false,
                                   L.st, nullptr, &B);
             if (err != OK) return err;
-            ce = cudaMemcpyAsync(r->res, dout64 + 2 * q, (r->la + r->lb - 1) * 16, cudaMemcpyDeviceToHost, L.st);
+            ce = cudaMemcpyAsync(r->res_direct ? r->out : r->res, dout64 + 2 * q, (r->la + r->lb - 1) * 16,
+                                 cudaMemcpyDeviceToHost, L.st);
             if (ce != cudaSuccess) return cuda_err(ce);
             o += r->la + r->lb;
             q += r->la + r->lb - 1;
             jo += j;
         }
+        L.t_copies = now_us();
     }
     return cuda_err(cudaEventRecord(L.ev, L.st));
 }
@@ -393,6 +492,9 @@ void batcher_loop(Server* Sp) {
             Req* r = *it;
             if (r->kind == kind && r->p == p) {
                 if (S.inflight + add + r->bytes > S.cfg.memory_budget && !(L.reqs.empty() && S.inflight == 0)) break;
+                // a batch holds at most kBatchBytes of device memory (or one request): lane buffers stay
+                // within the memory pool backed at creation, and no batch delays the others for long
+                if (!L.reqs.empty() && add + r->bytes > kBatchBytes) break;
                 L.reqs.push_back(r);
                 add += r->bytes;
                 it = S.pending.erase(it);
@@ -459,6 +561,8 @@ void completer_loop(Server* Sp) {
                                  st == OUT_OF_MEMORY ? st : FFT_ERROR);
             S.pool.put(r->in, r->in_bytes);  // the operands' copy has completed
             r->in = nullptr;
+            S.direct_inflight -= r->direct_bytes;  // operands read, result in the caller's buffer
+            r->direct_bytes = 0;
         }
         S.inflight -= std::min(S.inflight, freed);
         L.reqs.clear();
@@ -507,10 +611,11 @@ int wait_request(Server* S, long long id, long long timeout_us, double* t_ready)
     S->reqs.erase(it);
     lk.unlock();
     const double c0 = now_us();
-    if (st == OK) memcpy(r->out, r->res, r->res_bytes);
+    if (st == OK && !r->res_direct && r->out) memcpy(r->out, r->res, r->res_bytes);
     if (t_ready) *t_ready = t_done + (now_us() - c0);
     S->pool.put(r->in, r->in_bytes);
     S->pool.put(r->res, r->res_bytes);
+    S->direct_inflight -= r->direct_bytes;
     delete r;
     return st;
 }
@@ -532,40 +637,59 @@ struct Replay {
     double t0;
 };
 
-// Result buffers for requests whose caller gave none, recycled.
-struct ScratchPool {
-    std::mutex m;
-    std::vector<std::pair<size_t, void*>> free_list;
-    void* get(size_t bytes) {
-        std::lock_guard<std::mutex> g(m);
-        for (size_t i = 0; i < free_list.size(); ++i)
-            if (free_list[i].first >= bytes) {
-                void* q = free_list[i].second;
-                free_list.erase(free_list.begin() + i);
-                return q;
-            }
-        return malloc(bytes);
+// Request submission; H / c may be null (replayed requests: the result is dropped).
+long long submit_mod_req(Server& Sr, sfixn p, sfixn df, const sfixn* F, sfixn dg, const sfixn* G, sfixn* H) {
+    Server* S = &Sr;
+    if (!F || !G || df < 0 || dg < 0) return -1;
+    Req* r = new Req();
+    r->kind = 0;
+    r->p = (u32)p;
+    r->la = (long long)df + 1;
+    r->lb = (long long)dg + 1;
+    r->out = H;
+    int err = OK;
+    const PrimeCtx* pc = prime_ctx((u32)p, &err);
+    if (!pc) r->status = err;
+    else if (product_logn(r->la, r->lb) > std::min(pc->info.two_adic, kMaxLog)) r->status = FFT_SIZE_TOO_LARGE;
+    else {
+        r->in_bytes = (size_t)(r->la + r->lb) * 4;
+        r->res_bytes = (size_t)(r->la + r->lb - 1) * 4;
+        stage_request(*S, r, F, (size_t)r->la * 4, G, (size_t)r->lb * 4);
     }
-    void put(void* q, size_t bytes) {
-        std::lock_guard<std::mutex> g(m);
-        free_list.emplace_back(bytes, q);
+    return submit(*S, r);
+}
+
+long long submit_i64_req(Server& Sr, long long na, const int64_t* a, long long nb, const int64_t* b, int64_t* c) {
+    Server* S = &Sr;
+    if (!a || !b || na <= 0 || nb <= 0) return -1;
+    Req* r = new Req();
+    r->kind = 1;
+    r->p = 0;
+    r->la = na;
+    r->lb = nb;
+    r->out = c;
+    unsigned long long m = 0;
+    for (long long i = 0; i < na; ++i) m |= a[i] < 0 ? 0ull - (unsigned long long)a[i] : (unsigned long long)a[i];
+    for (long long i = 0; i < nb; ++i) m |= b[i] < 0 ? 0ull - (unsigned long long)b[i] : (unsigned long long)b[i];
+    r->bw = m ? 64 - __builtin_clzll(m) : 1;
+    const int e = na + nb - 1 > (1ll << 21) ? FFT_SIZE_TOO_LARGE : twoconv_plan(r->bw, r->bw, na, nb, false, &r->plan);
+    if (e != OK) r->status = e;
+    else {
+        r->in_bytes = (size_t)(na + nb) * 8;
+        r->res_bytes = (size_t)(na + nb - 1) * 16;
+        stage_request(*S, r, a, (size_t)na * 8, b, (size_t)nb * 8);
     }
-    ~ScratchPool() {
-        for (auto& e : free_list) free(e.second);
-    }
-};
+    return submit(*S, r);
+}
 
 void replay_thread(const Replay& R, int t, int threads) {
     struct Item {
         long long i, id;
-        void* scratch;
-        size_t bytes;
     };
     std::mutex qm;
     std::condition_variable qcv;
     std::deque<Item> q;
     bool done = false;
-    ScratchPool scratch;
     std::thread collector([&] {
         for (;;) {
             Item it;
@@ -584,7 +708,6 @@ void replay_thread(const Replay& R, int t, int threads) {
                 R.status[it.i] = wait_request(R.S, it.id, -1, &t_ready);
                 R.lat[it.i] = t_ready - (R.t0 + R.arrival[it.i]);
             }
-            if (it.scratch) scratch.put(it.scratch, it.bytes);
         }
     });
     for (long long i = t; i < R.count; i += threads) {
@@ -595,21 +718,18 @@ void replay_thread(const Replay& R, int t, int threads) {
             if (d > 200) std::this_thread::sleep_for(std::chrono::microseconds((long long)(d - 100)));
             else std::this_thread::yield();
         }
-        const long long n = R.la[i] + R.lb[i] - 1;
-        const size_t bytes = (size_t)std::max<long long>(n, 1) * (R.kind[i] ? 16 : 4);
+        // without an output buffer the result stays in the server's pinned slab (dropped when collected)
         void* out = R.h ? R.h[i] : nullptr;
-        void* scr = nullptr;
-        if (!out) out = scr = scratch.get(bytes);
         long long id;
         if (R.kind[i] == 0)
-            id = cumodp_server_submit_mod((cumodp_server*)R.S, R.p[i], (sfixn)(R.la[i] - 1), (const sfixn*)R.a[i],
-                                          (sfixn)(R.lb[i] - 1), (const sfixn*)R.b[i], (sfixn*)out);
+            id = submit_mod_req(*R.S, R.p[i], (sfixn)(R.la[i] - 1), (const sfixn*)R.a[i], (sfixn)(R.lb[i] - 1),
+                                (const sfixn*)R.b[i], (sfixn*)out);
         else
-            id = cumodp_server_submit_i64((cumodp_server*)R.S, R.la[i], (const int64_t*)R.a[i], R.lb[i],
-                                          (const int64_t*)R.b[i], (int64_t*)out);
+            id = submit_i64_req(*R.S, R.la[i], (const int64_t*)R.a[i], R.lb[i], (const int64_t*)R.b[i],
+                                (int64_t*)out);
         {
             std::lock_guard<std::mutex> g(qm);
-            q.push_back(Item{i, id, scr, bytes});
+            q.push_back(Item{i, id});
         }
         qcv.notify_one();
     }
@@ -669,16 +789,30 @@ cumodp_server* cumodp_server_create(const cumodp_server_config* cfg) {
         cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &keep);
         // back the pool with physical memory now (growing it later maps new
         // memory inside a batch's launch, which took up to a second)
-        const size_t reserve = std::min<size_t>(c.memory_budget, 8ull << 30);
+        const size_t reserve = std::min<size_t>(c.memory_budget, 16ull << 30);
         void* tmp = nullptr;
         cudaStream_t s0 = S->lanes[0].st;
         if (cudaMallocAsync(&tmp, reserve, s0) == cudaSuccess) cudaFreeAsync(tmp, s0);
         cudaStreamSynchronize(s0);
     }
     cudaGetLastError();
-    // job tables for a full batch, so that pinned memory is not reallocated
-    // (cudaFreeHost waits for the device) while serving
-    for (Lane& L : S->lanes) L.hjobs.ensure(direct_job_bytes(c.max_batch));
+    // lane buffers for a full batch, allocated now so that serving does not
+    // grow them: job tables (pinned memory is not reallocated while serving,
+    // cudaFreeHost waits for the device) for max_batch modular products or
+    // max_batch exact ones (up to 3 primes x 8 evaluation points each), and
+    // device operand, result and workspace buffers of kBatchBytes each (a
+    // batch holds at most kBatchBytes; only a single larger request grows them)
+    const size_t jobs = std::max(direct_job_bytes(c.max_batch), (size_t)c.max_batch * 3 * direct_job_bytes(8));
+    const size_t words = std::min<size_t>(kBatchBytes, c.memory_budget / (3 * (size_t)c.lanes)) / 4;
+    for (Lane& L : S->lanes) {
+        L.hjobs.ensure(jobs);
+        L.djobs.ensure(jobs, L.st);
+        L.din.ensure(words, L.st);
+        L.dout.ensure(words, L.st);
+        L.ws.ensure(words, L.st);
+    }
+    for (Lane& L : S->lanes) cudaStreamSynchronize(L.st);
+    cudaGetLastError();
     // pinned slabs: the whole host budget is pinned now, so that serving never
     // calls cudaHostAlloc (slow, and it stalls other CUDA calls)
     S->pool.set_limit(c.host_budget ? c.host_budget : (2ull << 30));
@@ -691,68 +825,14 @@ cumodp_server* cumodp_server_create(const cumodp_server_config* cfg) {
 
 long long cumodp_server_submit_mod(cumodp_server* h, sfixn p, sfixn df, const sfixn* F, sfixn dg, const sfixn* G,
                                    sfixn* H) {
-    Server* S = (Server*)h;
-    if (!S || !F || !G || !H || df < 0 || dg < 0) return -1;
-    Req* r = new Req();
-    r->kind = 0;
-    r->p = (u32)p;
-    r->la = (long long)df + 1;
-    r->lb = (long long)dg + 1;
-    r->out = H;
-    int err = OK;
-    const PrimeCtx* pc = prime_ctx((u32)p, &err);
-    if (!pc) r->status = err;
-    else if (product_logn(r->la, r->lb) > std::min(pc->info.two_adic, kMaxLog)) r->status = FFT_SIZE_TOO_LARGE;
-    else {
-        r->in_bytes = (size_t)(r->la + r->lb) * 4;
-        r->res_bytes = (size_t)(r->la + r->lb - 1) * 4;
-        r->in = S->pool.get(r->in_bytes);
-        r->res = r->in ? S->pool.get(r->res_bytes) : nullptr;
-        if (!r->in || !r->res) {
-            // pinned budget exhausted: shed the request
-            S->pool.put(r->in, r->in_bytes);
-            r->in = nullptr;
-            r->status = OUT_OF_MEMORY;
-        } else {
-            memcpy(r->in, F, (size_t)r->la * 4);
-            memcpy((u32*)r->in + r->la, G, (size_t)r->lb * 4);
-        }
-    }
-    return submit(*S, r);
+    if (!h || !H) return -1;
+    return submit_mod_req(*(Server*)h, p, df, F, dg, G, H);
 }
 
 long long cumodp_server_submit_i64(cumodp_server* h, long long na, const int64_t* a, long long nb, const int64_t* b,
                                    int64_t* c) {
-    Server* S = (Server*)h;
-    if (!S || !a || !b || !c || na <= 0 || nb <= 0) return -1;
-    Req* r = new Req();
-    r->kind = 1;
-    r->p = 0;
-    r->la = na;
-    r->lb = nb;
-    r->out = c;
-    unsigned long long m = 0;
-    for (long long i = 0; i < na; ++i) m |= a[i] < 0 ? 0ull - (unsigned long long)a[i] : (unsigned long long)a[i];
-    for (long long i = 0; i < nb; ++i) m |= b[i] < 0 ? 0ull - (unsigned long long)b[i] : (unsigned long long)b[i];
-    r->bw = m ? 64 - __builtin_clzll(m) : 1;
-    TwoConvPlan pl;
-    const int e = na + nb - 1 > (1ll << 21) ? FFT_SIZE_TOO_LARGE : twoconv_plan(r->bw, r->bw, na, nb, false, &pl);
-    if (e != OK) r->status = e;
-    else {
-        r->in_bytes = (size_t)(na + nb) * 8;
-        r->res_bytes = (size_t)(na + nb - 1) * 16;
-        r->in = S->pool.get(r->in_bytes);
-        r->res = r->in ? S->pool.get(r->res_bytes) : nullptr;
-        if (!r->in || !r->res) {
-            S->pool.put(r->in, r->in_bytes);
-            r->in = nullptr;
-            r->status = OUT_OF_MEMORY;
-        } else {
-            memcpy(r->in, a, (size_t)na * 8);
-            memcpy((long long*)r->in + na, b, (size_t)nb * 8);
-        }
-    }
-    return submit(*S, r);
+    if (!h || !c) return -1;
+    return submit_i64_req(*(Server*)h, na, a, nb, b, c);
 }
 
 int cumodp_server_poll(cumodp_server* h, long long id) {
@@ -789,6 +869,37 @@ cumodp_err cumodp_server_replay(cumodp_server* s, long long count, const double*
         if (status[i] != -1) last = std::max(last, R.t0 + arrival_us[i] + lat_us[i]);
     if (span_us) *span_us = last - R.t0;
     return CUMODP_SUCCESS;
+}
+
+cumodp_err cumodp_server_register(cumodp_server* h, void* ptr, size_t bytes) {
+    Server* S = (Server*)h;
+    if (!S || !ptr || bytes == 0) return CUMODP_ASSUMPTION_ERROR;
+    if (registered(*S, ptr, 1) || registered(*S, (char*)ptr + bytes - 1, 1)) return CUMODP_ASSUMPTION_ERROR;
+    cudaSetDevice(S->dev);
+    if (cudaHostRegister(ptr, bytes, cudaHostRegisterPortable) != cudaSuccess) {
+        cudaGetLastError();
+        return CUMODP_FAILURE;
+    }
+    if (!register_range(*S, ptr, bytes)) {
+        cudaHostUnregister(ptr);
+        return CUMODP_ASSUMPTION_ERROR;
+    }
+    return CUMODP_SUCCESS;
+}
+
+cumodp_err cumodp_server_unregister(cumodp_server* h, void* ptr) {
+    Server* S = (Server*)h;
+    if (!S || !ptr) return CUMODP_ASSUMPTION_ERROR;
+    {
+        std::lock_guard<std::mutex> g(S->reg_m);
+        auto it = S->regs.find((uintptr_t)ptr);
+        if (it == S->regs.end()) return CUMODP_ASSUMPTION_ERROR;
+        S->regs.erase(it);
+    }
+    cudaSetDevice(S->dev);
+    const cudaError_t e = cudaHostUnregister(ptr);
+    cudaGetLastError();
+    return e == cudaSuccess ? CUMODP_SUCCESS : CUMODP_FAILURE;
 }
 
 void cumodp_server_get_stats(cumodp_server* h, cumodp_server_stats* out) {
@@ -848,6 +959,8 @@ void cumodp_server_destroy(cumodp_server* h) {
         if (L.ev) cudaEventDestroy(L.ev);
     }
     if (S->trace) fclose(S->trace);
+    for (auto& kv : S->regs) cudaHostUnregister((void*)kv.first);  // ranges the caller left registered
+    cudaGetLastError();
     for (auto& kv : S->reqs) {
         S->pool.put(kv.second->in, kv.second->in_bytes);
         S->pool.put(kv.second->res, kv.second->res_bytes);

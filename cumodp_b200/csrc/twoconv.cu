@@ -202,6 +202,16 @@ int twoconv_plan(int ba, int bb, long long la, long long lb, bool force_two_prim
     return OK;
 }
 
+void twoconv_buffer_sizes_plan(long long la, long long lb, const TwoConvPlan& pl, size_t* eval_words,
+                               size_t* ws_words, size_t* job_bytes) {
+    const int np = pl.nprimes, npts = pl.K == 1 ? 1 : 2 * pl.K;
+    const long long lc = la + lb - 1;
+    *eval_words = (size_t)np * npts * (la + lb + lc);
+    std::vector<long long> A(npts, la), B(npts, lb);
+    *ws_words = (size_t)np * direct_ws_words(npts, A.data(), B.data());
+    *job_bytes = (size_t)np * direct_job_bytes(npts);
+}
+
 void twoconv_buffer_sizes(long long la, long long lb, size_t* eval_words, size_t* ws_words, size_t* job_bytes) {
     // worst case over plans: 3 primes x 8 points
     const int np = 3, npts = 8;

@@ -230,13 +230,16 @@ cumodp_err cumodp_twoconv_plan(int bit_width_a, int bit_width_b, long long na, l
 /* A request loop with continuous batching.  Requests (modular products, or
  * exact int64 products) are copied at submission; a batcher thread admits
  * them in arrival order while the device-memory budget allows, groups them
- * by (kind, prime) and runs each group as one batch on a free lane (stream
- * plus device buffers); batches on different lanes overlap on the GPU, and
+ * by (kind, prime) and runs each group as one batch (at most max_batch
+ * requests and 1 GiB of device buffers, or one larger request) on a free
+ * lane (stream plus device buffers); batches on different lanes overlap on the GPU, and
  * requests arriving meanwhile join the next batch.  Operands are copied at
  * submission into pinned memory owned by the server; the result is copied
  * into the caller's output buffer by cumodp_server_wait, which must be
- * called once per request (the buffer must stay valid until then).  No
- * counterpart in the reference. */
+ * called once per request (the buffer must stay valid until then).  Memory
+ * the caller registers (cumodp_server_register) skips both copies: operands
+ * go to the device from it and results come back into it.  No counterpart in
+ * the reference. */
 typedef struct cumodp_server cumodp_server;
 typedef struct {
     int device;              /* CUDA device ordinal */
@@ -248,7 +251,8 @@ typedef struct {
     size_t host_budget;      /* pinned host memory for the operand and result slabs of unfinished
                                 requests (power-of-two slabs carved from chunks pinned when the
                                 server is created); a submission that finds no room completes at
-                                once with CUMODP_OUT_OF_MEMORY (load shedding).  0 = 2 GiB */
+                                once with CUMODP_OUT_OF_MEMORY (load shedding).  Requests in
+                                registered memory count against it too.  0 = 2 GiB */
 } cumodp_server_config;
 typedef struct {
     long long completed, failed, batches, pending;
@@ -275,8 +279,9 @@ int cumodp_server_wait(cumodp_server *s, long long id, long long timeout_us);
  * (a submitter that falls behind submits at once): kind[i] = 0 is the
  * product mod p[i] of la[i] and lb[i] sfixn coefficients a[i], b[i] into
  * h[i] (la+lb-1 words); kind[i] = 1 the exact product of int64 operands into
- * h[i] (2(la+lb-1) int64 words).  h may be NULL (results are then written to
- * recycled scratch buffers and dropped).  `threads` submitters share the
+ * h[i] (2(la+lb-1) int64 words).  h may be NULL (each result then lands in
+ * the server's pinned slab and is dropped when collected: no host copy).
+ * `threads` submitters share the
  * trace round-robin, each with a collector thread.  On return status[i] is
  * the request's cumodp_err (-1: refused by the server), lat_us[i] the time
  * from the scheduled arrival to the result in the output buffer, and
@@ -285,6 +290,19 @@ cumodp_err cumodp_server_replay(cumodp_server *s, long long count, const double 
                                 const sfixn *p, const long long *la, const long long *lb, const void *const *a,
                                 const void *const *b, void *const *h, int threads, double *lat_us, int *status,
                                 double *span_us);
+/* Addition.  Registers the caller's host memory [ptr, ptr + bytes) with the
+ * server (page-locked in place, cudaHostRegister).  A request whose two
+ * operands lie in registered memory is copied to the device straight from
+ * there, and a result buffer that lies in registered memory receives the
+ * result straight from the device: no copy through the server's pinned slabs
+ * and no host memcpy on either side.  The caller leaves such operands
+ * unchanged until the request completes.  Unfinished requests still count
+ * their operand and result bytes against host_budget, which keeps bounding
+ * the backlog (shedding beyond it).  Ranges may not overlap.  Unregister only
+ * when no unfinished request uses the range; cumodp_server_destroy
+ * unregisters what is left. */
+cumodp_err cumodp_server_register(cumodp_server *s, void *ptr, size_t bytes);
+cumodp_err cumodp_server_unregister(cumodp_server *s, void *ptr);
 void cumodp_server_get_stats(cumodp_server *s, cumodp_server_stats *out);
 void cumodp_server_reset_stats(cumodp_server *s);
 /* Drains queued and in-flight work, then frees everything. */

@@ -167,3 +167,60 @@ def test_host_budget_sheds_and_server_continues(cm, oracle_mod):
         assert np.array_equal(h1[1], oracle_mod.polymul(big[0], big[1], p))
         h3 = srv.submit_mod(big[0], big[1], p)  # slabs returned: admitted again
         assert srv.wait(h3[0]) == 0
+
+
+def test_registered_memory_gives_the_same_results(cm):
+    """Operands and outputs in memory registered with the server (no staging copies) give the same
+    words as the copied path, for modular and exact requests, alone and in a concurrent mix."""
+    r = SplitMix64(2031)
+    reqs = _mix(r, 60, max_log=16)
+    # every operand and output placed in one registered arena
+    sizes = []
+    for q in reqs:
+        if q[0] == "mod":
+            sizes += [len(q[2]) * 4, len(q[3]) * 4, (len(q[2]) + len(q[3]) - 1) * 4]
+        else:
+            sizes += [len(q[1]) * 8, len(q[2]) * 8, (len(q[1]) + len(q[2]) - 1) * 16]
+    total = sum((s + 63) // 64 * 64 for s in sizes)
+    raw = np.zeros(total + 8192, np.uint8)
+    base = (-raw.ctypes.data) % 4096
+    arena = raw[base:base + total + 4096]
+    cursor = [0]
+
+    def place(nbytes, dtype, values=None):
+        a = arena[cursor[0]:cursor[0] + nbytes].view(dtype)
+        cursor[0] += (nbytes + 63) // 64 * 64
+        if values is not None:
+            a[:] = values
+        return a
+
+    with cm.Server(max_batch=32, batch_window_us=100) as srv:
+        srv.register(arena)
+        L = cm.lib()
+        want, got, ids = [], [], []
+        for q in reqs:
+            rid, out = _submit(srv, q)  # copied path (unregistered host arrays)
+            assert srv.wait(rid) == 0
+            want.append(out.copy())
+        for q in reqs:
+            if q[0] == "mod":
+                a = place(len(q[2]) * 4, np.uint32, q[2])
+                b = place(len(q[3]) * 4, np.uint32, q[3])
+                o = place((len(a) + len(b) - 1) * 4, np.uint32)
+                rid = L.cumodp_server_submit_mod(srv._h, q[1], len(a) - 1, a.ctypes.data, len(b) - 1, b.ctypes.data,
+                                                 o.ctypes.data)
+            else:
+                a = place(len(q[1]) * 8, np.int64, q[1])
+                b = place(len(q[2]) * 8, np.int64, q[2])
+                o = place((len(a) + len(b) - 1) * 16, np.int64)
+                rid = L.cumodp_server_submit_i64(srv._h, len(a), a.ctypes.data, len(b), b.ctypes.data, o.ctypes.data)
+            assert rid > 0
+            ids.append(rid)
+            got.append(o)
+        for rid in ids:
+            assert L.cumodp_server_wait(srv._h, rid, -1) == 0
+        for w, g in zip(want, got):
+            assert np.array_equal(w.view(g.dtype), g)
+        srv.unregister(arena)
+        with pytest.raises(cm.CumodpError):
+            srv.unregister(arena)  # already gone
