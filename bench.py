@@ -900,6 +900,9 @@ def serving_c5(cm, rates=(1000, 3000, 10000, 30000, 100000), max_requests=20000,
             in_bytes = sum(a.nbytes + b.nbytes for a, b, _ in reqs)
             res_bytes = sum((len(a) + len(b) - 1) * (16 if p is None else 4) for a, b, p in reqs)
             ceiling = n / max(in_bytes / link_bps, res_bytes / link_bps)
+            done_in = sum(reqs[i][0].nbytes + reqs[i][1].nbytes for i in np.flatnonzero(ok))
+            done_res = sum((len(reqs[i][0]) + len(reqs[i][1]) - 1) * (16 if reqs[i][2] is None else 4)
+                           for i in np.flatnonzero(ok))
             out[str(rate)] = {"requests": n, "completed": int(ok.sum()),
                               "rejected_size": int((st == cm.FFT_SIZE_TOO_LARGE).sum()),
                               "shed": int((st == cm.OUT_OF_MEMORY).sum()),
@@ -908,7 +911,9 @@ def serving_c5(cm, rates=(1000, 3000, 10000, 30000, 100000), max_requests=20000,
                               "p50_ms": pct(0.5), "p99_ms": pct(0.99), "max_ms": pct(1.0),
                               "products_per_s": round(ok.sum() / (span_us * 1e-6), 1),
                               "offered_per_s": round(n / (arrival[-1] * 1e-6), 1),
-                              "operand_gb_per_s": round(in_bytes / (span_us * 1e3), 2),
+                              "operand_gb_per_s": round(done_in / (span_us * 1e3), 2),
+                              "result_gb_per_s": round(done_res / (span_us * 1e3), 2),
+                              "link_gbs_per_direction": link["gbs_per_direction"],
                               "link_ceiling_per_s": round(ceiling, 1),
                               "batches": srv.stats()["batches"], "replay_threads": threads,
                               "copies": "registered operand pools, results in pinned slabs: no host copy"}

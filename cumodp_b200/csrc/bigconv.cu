@@ -260,11 +260,33 @@ int grid_of(long long n) { return (int)std::max<long long>(1, std::min<long long
 
 }  // namespace
 
+// Scratch of one product (bigconv_mul_dev with caller buffers): the
+// magnitudes, signs, split operands and products per prime, then the
+// products' workspace and job tables (as direct_batch takes them).
+struct BigSizes {
+    size_t mag_bytes, sign_bytes, words, ws_words, job_bytes;
+};
+
+BigSizes big_sizes(const BigPlan& pl, long long na, long long nb, int in_words) {
+    const long long la = (2ll * pl.K - 1) * (na - 1) + pl.K, lb = (2ll * pl.K - 1) * (nb - 1) + pl.K;
+    BigSizes z;
+    z.mag_bytes = ((size_t)(na + nb) * in_words * 8 + 255) & ~(size_t)255;
+    z.sign_bytes = ((size_t)(na + nb) + 255) & ~(size_t)255;
+    z.words = (size_t)pl.nprimes * (la + lb + la + lb - 1);
+    const long long LA[1] = {la}, LB[1] = {lb};
+    z.ws_words = (size_t)pl.nprimes * direct_ws_words(1, LA, LB);
+    z.job_bytes = (size_t)pl.nprimes * ((direct_job_bytes(1) + 255) & ~(size_t)255);
+    return z;
+}
+
 // c (lc = na + nb - 1 coefficients of out_words words) = a * b exactly;
 // device pointers, coefficients of in_words two's-complement words, bw the
-// largest magnitude bit width of any coefficient.
+// largest magnitude bit width of any coefficient.  bufs == nullptr: library
+// workspace, one product per prime on side streams; else the caller's
+// buffers (sizes from big_sizes), everything on st.
 int bigconv_mul_dev(const unsigned long long* a, long long na, const unsigned long long* b, long long nb,
-                    int in_words, unsigned long long* c, int out_words, int bw, cudaStream_t st, BigPlan* used) {
+                    int in_words, unsigned long long* c, int out_words, int bw, cudaStream_t st, BigPlan* used,
+                    const TwoConvBufs* bufs = nullptr) {
     if (in_words <= 0 || in_words > kBigMaxInWords || out_words <= 0 || na <= 0 || nb <= 0)
         return ASSUMPTION_ERROR;
     if (bw < 0 || bw > 64 * in_words) return ASSUMPTION_ERROR;
@@ -277,11 +299,10 @@ int bigconv_mul_dev(const unsigned long long* a, long long na, const unsigned lo
     const long long lp = la + lb - 1;
     const int r = pl.nprimes;
     // scratch: |a|, |b| (64-bit words), signs, split operands and products per prime
-    const size_t mag_bytes = (size_t)(na + nb) * in_words * 8;
-    const size_t sign_bytes = ((size_t)(na + nb) + 255) & ~(size_t)255;
-    const size_t words = (size_t)r * (la + lb + lp);
+    const BigSizes z = big_sizes(pl, na, nb, in_words);
+    const size_t mag_bytes = z.mag_bytes, sign_bytes = z.sign_bytes, words = z.words;
     const int dev = current_device();
-    char* ws = (char*)workspace(dev, kWsBig, mag_bytes + sign_bytes + words * 4, &err);
+    char* ws = bufs ? (char*)bufs->eval : (char*)workspace(dev, kWsBig, mag_bytes + sign_bytes + words * 4, &err);
     if (!ws) return err;
     unsigned long long* mag = (unsigned long long*)ws;
     unsigned char* sg = (unsigned char*)(ws + mag_bytes);
@@ -314,7 +335,7 @@ int bigconv_mul_dev(const unsigned long long* a, long long na, const unsigned lo
     if ((err = cuda_err(cudaGetLastError())) != OK) return err;
     // one product per prime, on side streams (each batch plan owns its
     // workspace), joined before the CRT
-    {
+    if (!bufs) {
         const sfixn df = (sfixn)(la - 1), dg = (sfixn)(lb - 1);
         const int64_t zero = 0;
         aux_fork(dev, st, r);
@@ -322,6 +343,17 @@ int bigconv_mul_dev(const unsigned long long* a, long long na, const unsigned lo
             err = batch_mul_dev(1, &df, &zero, ap[k], &dg, &zero, bp[k], &zero, cp[k], pl.p[k], aux_stream(dev, k));
         aux_join(dev, st, r);
         if (err != OK) return err;
+    } else {
+        const long long LA[1] = {la}, LB[1] = {lb}, LH[1] = {lp};
+        const size_t wsw = z.ws_words / r, jb = z.job_bytes / r;
+        for (int k = 0; k < r; ++k) {
+            const u32* pa[1] = {ap[k]};
+            const u32* pb[1] = {bp[k]};
+            u32* ph[1] = {cp[k]};
+            err = direct_batch(1, pa, LA, pb, LB, ph, LH, pl.p[k], bufs->ws + k * wsw, (char*)bufs->djobs + k * jb,
+                               (char*)bufs->hjobs + k * jb, st, false);
+            if (err != OK) return err;
+        }
     }
     BigCrtArgs C;
     memset(&C, 0, sizeof(C));
@@ -339,6 +371,33 @@ int bigconv_mul_dev(const unsigned long long* a, long long na, const unsigned lo
     C.c = c;
     k_big_crt<<<(unsigned)((lc + 127) / 128), 128, 0, st>>>(C);
     return cuda_err(cudaGetLastError());
+}
+
+int exact_i64_long_dev_bufs(const long long* a, long long la, const long long* b, long long lb, long long* c, int bw,
+                            cudaStream_t st, const TwoConvBufs* bufs) {
+    return bigconv_mul_dev((const unsigned long long*)a, la, (const unsigned long long*)b, lb, 1,
+                           (unsigned long long*)c, 2, bw, st, nullptr, bufs);
+}
+
+void exact_i64_long_sizes(long long la, long long lb, int bw, size_t* eval_words, size_t* ws_words,
+                          size_t* job_bytes) {
+    BigPlan pl;
+    if (big_plan(bw, la, lb, &pl) != OK) {
+        *eval_words = *ws_words = *job_bytes = 0;
+        return;
+    }
+    const BigSizes z = big_sizes(pl, la, lb, 1);
+    *eval_words = (z.mag_bytes + z.sign_bytes) / 4 + z.words;
+    *ws_words = z.ws_words;
+    *job_bytes = z.job_bytes;
+}
+
+int exact_i64_long_cost(long long la, long long lb, int bw, double* cost) {
+    BigPlan pl;
+    const int err = big_plan(bw, la, lb, &pl);
+    if (err != OK) return err;
+    *cost = (double)pl.nprimes * std::ldexp(1.0, pl.logn) * pl.logn;
+    return OK;
 }
 
 int exact_i64_long_dev(const long long* a, long long la, const long long* b, long long lb, long long* c, int bw,

@@ -34,5 +34,16 @@ int twoconv_mul_dev(const long long* a, long long la, const long long* b, long l
 // Fourier primes of 2-adic order >= 22 (bigconv.cu); library workspace.
 int exact_i64_long_dev(const long long* a, long long la, const long long* b, long long lb, long long* c, int bw,
                        cudaStream_t st);
+// Transform work of that path (primes x 2^logn x logn), or its planner's error.
+int exact_i64_long_cost(long long la, long long lb, int bw, double* cost);
+// The same on caller buffers (bufs->eval holds eval_words, bufs->ws ws_words,
+// the job tables job_bytes; exact_i64_long_sizes), everything on st.
+int exact_i64_long_dev_bufs(const long long* a, long long la, const long long* b, long long lb, long long* c, int bw,
+                            cudaStream_t st, const TwoConvBufs* bufs);
+void exact_i64_long_sizes(long long la, long long lb, int bw, size_t* eval_words, size_t* ws_words,
+                          size_t* job_bytes);
+// Whether the exact product of (la, lb) with bit widths (ba, bb) takes the
+// big-coefficient path (method 0): no two-convolution plan, or a dearer one.
+bool exact_i64_prefers_long(int ba, int bb, long long la, long long lb);
 
 }  // namespace cmb

@@ -148,6 +148,7 @@ struct Req {
     size_t direct_bytes = 0;  // bytes of this request counted in Server::direct_inflight
     int bw = 1;
     TwoConvPlan plan{0, 0, 0, 0};  // exact products: the plan (sizes the lane buffers)
+    bool long_path = false;         // exact products on the big-coefficient path (exact_i64_prefers_long)
     void* out;
     size_t bytes;
     double t_submit = 0, t_done = 0;
@@ -257,6 +258,12 @@ namespace {
 
 constexpr size_t kBatchBytes = 1ull << 30;
 
+// Lane buffers an exact product takes on its path (words, words, bytes).
+void exact_sizes(const Req& r, size_t* eval_words, size_t* ws_words, size_t* job_bytes) {
+    if (r.long_path) exact_i64_long_sizes(r.la, r.lb, r.bw, eval_words, ws_words, job_bytes);
+    else twoconv_buffer_sizes_plan(r.la, r.lb, r.plan, eval_words, ws_words, job_bytes);
+}
+
 size_t req_bytes(const Req& r) {
     const long long lc = r.la + r.lb - 1;
     if (r.kind == 0) {
@@ -265,7 +272,7 @@ size_t req_bytes(const Req& r) {
         return (size_t)(r.la + r.lb + lc + ws) * 4 + 256;
     }
     size_t ev, ws, jb;
-    twoconv_buffer_sizes_plan(r.la, r.lb, r.plan, &ev, &ws, &jb);
+    exact_sizes(r, &ev, &ws, &jb);
     return (r.la + r.lb + 2 * lc) * 8 + (ev + ws) * 4 + jb;
 }
 
@@ -409,7 +416,7 @@ int run_batch(Server& S, Lane& L) {
             nin += r->la + r->lb;
             nout += 2 * (r->la + r->lb - 1);
             size_t e, w, j;
-            twoconv_buffer_sizes_plan(r->la, r->lb, r->plan, &e, &w, &j);
+            exact_sizes(*r, &e, &w, &j);
             evw = std::max(evw, e);
             wsw = std::max(wsw, w);
             jbb += j;
@@ -436,9 +443,12 @@ int run_batch(Server& S, Lane& L) {
             if (ce != cudaSuccess) return cuda_err(ce);
             TwoConvBufs B{eval, L.ws.p, L.djobs.p + jo, L.hjobs.p + jo};
             size_t e, w, j;
-            twoconv_buffer_sizes_plan(r->la, r->lb, r->plan, &e, &w, &j);
-            err = twoconv_mul_dev(din64 + o, r->la, din64 + o + r->la, r->lb, dout64 + 2 * q, r->bw, r->bw, false,
-                                  L.st, nullptr, &B);
+            exact_sizes(*r, &e, &w, &j);
+            err = r->long_path
+                      ? exact_i64_long_dev_bufs(din64 + o, r->la, din64 + o + r->la, r->lb, dout64 + 2 * q, r->bw, L.st,
+                                                &B)
+                      : twoconv_mul_dev(din64 + o, r->la, din64 + o + r->la, r->lb, dout64 + 2 * q, r->bw, r->bw,
+                                        false, L.st, nullptr, &B);
             if (err != OK) return err;
             ce = cudaMemcpyAsync(r->res_direct ? r->out : r->res, dout64 + 2 * q, (r->la + r->lb - 1) * 16,
                                  cudaMemcpyDeviceToHost, L.st);
@@ -530,11 +540,30 @@ void completer_loop(Server* Sp) {
         S.cv_done.wait(lk, [&] { return S.stop || !S.dispatched.empty(); });
         if (S.dispatched.empty() && S.stop) return;
         if (S.dispatched.empty()) continue;
-        const int li = S.dispatched.front();
-        S.dispatched.pop_front();
+        // the first lane whose batch has finished: batches of different lanes
+        // finish in any order, and a lane whose batch is done must not wait
+        // behind an older, longer batch to be freed
+        size_t pos = 0;
+        while (S.dispatched.size() > 1) {
+            bool found = false;
+            for (size_t k = 0; k < S.dispatched.size() && !found; ++k) {
+                if (cudaEventQuery(S.lanes[S.dispatched[k]].ev) != cudaErrorNotReady) {
+                    pos = k;
+                    found = true;
+                }
+            }
+            cudaGetLastError();  // a not-ready query leaves its status as the thread's last error
+            if (found) break;
+            lk.unlock();
+            std::this_thread::sleep_for(std::chrono::microseconds(10));
+            lk.lock();
+        }
+        if (S.dispatched.empty()) continue;
+        const int li = S.dispatched[pos];
+        S.dispatched.erase(S.dispatched.begin() + pos);
         Lane& L = S.lanes[li];
         lk.unlock();
-        cudaError_t ce = cudaEventSynchronize(L.ev);
+        cudaError_t ce = cudaEventSynchronize(L.ev);  // done (several lanes) or the only one in flight
         int st = L.status != OK ? L.status : cuda_err(ce);
         if (st == OK) st = cuda_err(cudaGetLastError());
         if (st != OK) {
@@ -672,7 +701,13 @@ long long submit_i64_req(Server& Sr, long long na, const int64_t* a, long long n
     for (long long i = 0; i < na; ++i) m |= a[i] < 0 ? 0ull - (unsigned long long)a[i] : (unsigned long long)a[i];
     for (long long i = 0; i < nb; ++i) m |= b[i] < 0 ? 0ull - (unsigned long long)b[i] : (unsigned long long)b[i];
     r->bw = m ? 64 - __builtin_clzll(m) : 1;
-    const int e = na + nb - 1 > (1ll << 21) ? FFT_SIZE_TOO_LARGE : twoconv_plan(r->bw, r->bw, na, nb, false, &r->plan);
+    // the two-convolution plan, or the big-coefficient path where it is the
+    // only or the cheaper one (up to 2^22 coefficients here)
+    int e = na + nb - 1 > (1ll << 22) ? FFT_SIZE_TOO_LARGE : OK;
+    if (e == OK) {
+        r->long_path = exact_i64_prefers_long(r->bw, r->bw, na, nb);
+        if (!r->long_path) e = twoconv_plan(r->bw, r->bw, na, nb, false, &r->plan);
+    }
     if (e != OK) r->status = e;
     else {
         r->in_bytes = (size_t)(na + nb) * 8;

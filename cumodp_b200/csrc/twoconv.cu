@@ -26,6 +26,7 @@
 // K = 1 is the degenerate case with no limb split (u = v = the product).
 // The planner picks the cheapest (K, M, primes) whose exactness bound holds.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 
 #include "../../include/cumodp.h"
@@ -345,20 +346,37 @@ int bw_host(const int64_t* x, long long n) {
 }  // namespace
 
 namespace cmb {
+
+// Transforms past 2^21 points, which the reference's primes do not have, and
+// 2^21-point products, where those primes need a limb split into 2 x 4
+// transforms and primes of higher order 3, take the big-coefficient path
+// (results are the same integers either way); ties keep the reference's
+// primes.
+bool exact_i64_prefers_long(int ba, int bb, long long la, long long lb) {
+    TwoConvPlan pl;
+    const int pe = twoconv_plan(ba, bb, la, lb, false, &pl);
+    double big = 0;
+    if (exact_i64_long_cost(la, lb, std::max(ba, bb), &big) != OK) return false;
+    if (pe == FFT_SIZE_TOO_LARGE) return true;
+    if (pe != OK) return false;
+    const double tc = (double)pl.nprimes * (pl.K == 1 ? 1 : 2 * pl.K) * std::ldexp(1.0, pl.logn) * pl.logn;
+    return big < tc;
+}
+
 namespace {
 
 // The two-convolution product (the reference's primes, 962592769,
-// 950009857, 940572673) where its plan exists; longer products (transforms
-// past 2^21, which those primes do not have) through the big-coefficient
-// path over primes of higher 2-adic order.  method 1 (the forced two-prime
-// split of the reference's scheme) has no such fallback.
+// 950009857, 940572673) where its plan exists and is the cheaper one; else
+// the big-coefficient path over primes of higher 2-adic order (see
+// exact_i64_prefers_long).  method 1 (the forced two-prime split of the
+// reference's scheme) always takes the first.
 int exact_i64_any_len(const int64_t* a, long long na, const int64_t* b, long long nb, int64_t* c, int ba, int bb,
                       int method, cudaStream_t st) {
-    TwoConvPlan pl;
-    const int pe = twoconv_plan(ba, bb, na, nb, method == 1, &pl);
-    if (pe == FFT_SIZE_TOO_LARGE && method != 1)
+    if (method != 1 && exact_i64_prefers_long(ba, bb, na, nb))
         return exact_i64_long_dev((const long long*)a, na, (const long long*)b, nb, (long long*)c, std::max(ba, bb),
                                   st);
+    TwoConvPlan pl;
+    const int pe = twoconv_plan(ba, bb, na, nb, method == 1, &pl);
     if (pe != OK) return pe;
     return twoconv_mul_dev((const long long*)a, na, (const long long*)b, nb, (long long*)c, ba, bb, method == 1, st,
                            nullptr, nullptr);

@@ -201,10 +201,12 @@ cumodp_err cumodp_fftmul_batch(int count, const sfixn *df, const int64_t *f_off,
  * negacyclic x-convolutions mod Fourier primes 962592769, 950009857,
  * 940572673, CRT, (u+v)/2 + 2^N (u-v)/2.  method 0 picks the cheapest exact
  * (K, M, primes); method 1 forces the smallest limb split that needs only
- * two primes.  Products longer than those primes' transforms allow (past
- * 2^21 coefficients, or past 2^20 where the plan needs 940572673) run, for
- * method 0, on the big-coefficient path (cumodp_twoconv_mul_big's planner,
- * Fourier primes of 2-adic order >= 22), up to 2^25 coefficients.  Host
+ * two primes.  With method 0, products longer than those primes'
+ * transforms allow (past 2^21 coefficients) or that they make dearer (2^21
+ * points, which need 2 x 4 transforms there against 3 over primes of
+ * higher order) run on the big-coefficient path (cumodp_twoconv_mul_big's
+ * planner, Fourier primes of 2-adic order >= 22), up to 2^25 coefficients:
+ * the same integers, fewer transforms.  Host
  * arrays pass through pinned staging (one copy each way).  Returns
  * CUMODP_ASSUMPTION_ERROR when the exact product does not fit 127 bits or
  * na + nb - 1 > 2^25, CUMODP_FFT_SIZE_TOO_LARGE when no plan exists. */

@@ -224,3 +224,21 @@ def test_registered_memory_gives_the_same_results(cm):
         srv.unregister(arena)
         with pytest.raises(cm.CumodpError):
             srv.unregister(arena)  # already gone
+
+
+def test_long_exact_requests_match_the_host_entry(cm):
+    """Exact requests on both paths (two-convolution and, for 2^21-point products, the big-coefficient one)
+    return the same words as cumodp_twoconv_mul_i64, alone and together in one batch."""
+    r = SplitMix64(2032)
+    shapes = [((1 << 20) - 3, (1 << 20) - 7), ((1 << 19) + 5, 1000), (300000, 600000), (70, 90)]
+    ops = [(r.int64_in(na, 10**10), r.int64_in(nb, 10**10)) for na, nb in shapes]
+    want = [cm.twoconv_mul(a, b, raw=True) for a, b in ops]
+    with cm.Server(max_batch=8, batch_window_us=2000) as srv:
+        for (a, b), w in zip(ops, want):  # alone
+            rid, out = srv.submit_i64(a, b)
+            assert srv.wait(rid) == 0
+            assert np.array_equal(out, w)
+        subs = [srv.submit_i64(a, b) for a, b in ops]  # together
+        for (rid, out), w in zip(subs, want):
+            assert srv.wait(rid) == 0
+            assert np.array_equal(out, w)
