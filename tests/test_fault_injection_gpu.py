@@ -47,11 +47,13 @@ def test_batch_plan_allocation_failure_then_recovery(cm, oracle_mod, failures):
 
 
 def test_server_lane_allocation_failure_is_contained(cm, oracle_mod):
+    """A lane's buffers are sized at creation (here for a 3 MB device budget, about 1 MB each); a request
+    larger than that grows them, and that growth is made to fail."""
     p = 469762049
     r = SplitMix64(0xC0DA0603)
-    a, b = r.residues(5000, p), r.residues(6000, p)
-    with cm.Server(lanes=1) as srv:
-        cm.inject_alloc_failures(1)  # the lane's first buffer
+    a, b = r.residues(300000, p), r.residues(300000, p)
+    with cm.Server(lanes=1, memory_budget=3 << 20) as srv:
+        cm.inject_alloc_failures(1)  # the lane's growth for this request
         rid, _ = srv.submit_mod(a, b, p)
         assert srv.wait(rid) == cm.OUT_OF_MEMORY
         rid, out = srv.submit_mod(a, b, p)
