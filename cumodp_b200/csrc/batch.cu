@@ -153,6 +153,7 @@ namespace {
 struct ClassPlan {
     int logn = 0;
     bool large = false;
+    bool queued = false;       // runs in the batch's single work-queue launch (k_small_queue)
     int l2 = 0;
     std::vector<int> members;  // job indices of the batch
     size_t job_off = 0;        // byte offset of this class's job table
@@ -164,6 +165,9 @@ struct BatchPlan {
     int dev = 0;
     std::vector<long long> la, lb;
     std::vector<ClassPlan> classes;
+    int nitems = 0;            // work items of the queued classes (0: no queue launch)
+    size_t items_off = 0;      // byte offsets in djobs of the items and of the queue counter
+    size_t counter_off = 0;
     void* djobs = nullptr;     // device job tables
     size_t jobs_bytes = 0;
     std::vector<unsigned char> hjobs;  // host copy of what djobs holds
@@ -219,6 +223,8 @@ int build_plan(BatchPlan& P, const PrimeCtx& pc, cudaStream_t st) {
         // a few products of a length one CTA could hold still run faster
         // spread over many CTAs (the three-pass kernels)
         c.large = c.logn > kMaxSmallLog || (c.logn >= single_large_min_log() && c.members.size() <= 16);
+        c.queued = !c.large && c.logn >= kQueueMinLog && c.logn <= kQueueMaxLog;
+        if (c.queued) P.nitems += (int)((c.members.size() + small_ppc(c.logn) - 1) / small_ppc(c.logn));
         c.job_off = jb;
         jb += c.members.size() * (c.large ? sizeof(LargeJob) : sizeof(ProdJob));
         jb = (jb + 255) & ~(size_t)255;
@@ -229,6 +235,11 @@ int build_plan(BatchPlan& P, const PrimeCtx& pc, cudaStream_t st) {
         }
         P.classes.push_back(c);
     }
+    P.items_off = jb;
+    jb += (size_t)P.nitems * sizeof(SmallItem);
+    jb = (jb + 255) & ~(size_t)255;
+    P.counter_off = jb;
+    jb += 256;
     P.jobs_bytes = std::max<size_t>(jb, 256);
     if (dev_malloc(&P.djobs, P.jobs_bytes) != cudaSuccess) {
         cudaGetLastError();
@@ -281,12 +292,34 @@ int prepare_capture(BatchPlan& P, const PrimeCtx& pc) {
 int enqueue_classes(BatchPlan& P, const PrimeCtx& pc, cudaStream_t st) {
     int err = OK;
     cudaEventRecord(P.fork, st);
+    bool queue_done = false;
     for (size_t ci = 0; ci < P.classes.size(); ++ci) {
         const ClassPlan& c = P.classes[ci];
+        if (c.queued && queue_done) continue;
         cudaStream_t s = P.side[ci];
         cudaStreamWaitEvent(s, P.fork, 0);
         const u32 root = canonical_root(pc, c.logn);
-        if (!c.large) {
+        if (c.queued) {
+            // every queued class in one persistent launch on this branch
+            SmallQueueArgs Q;
+            memset(&Q, 0, sizeof(Q));
+            Q.pk = pc.pk;
+            for (const ClassPlan& d : P.classes) {
+                if (!d.queued) continue;
+                SmallArgs A;
+                if ((err = small_args(pc, canonical_root(pc, d.logn), d.logn, P.dev, &A)) != OK) return err;
+                Q.tw[d.logn] = A.tw;
+                Q.tw_inv_off[d.logn] = A.tw_inv_off;
+                Q.scale[d.logn] = A.scale;
+            }
+            Q.items = (const SmallItem*)((char*)P.djobs + P.items_off);
+            Q.nitems = P.nitems;
+            Q.counter = (int*)((char*)P.djobs + P.counter_off);
+            cudaMemsetAsync(Q.counter, 0, sizeof(int), s);
+            const int grid = std::min(P.nitems, sm_count(P.dev) * kQueueCtas);
+            k_small_queue<kQueueMaxLog><<<grid, kQueueThreads, kQueueSmemWords * sizeof(u32), s>>>(Q);
+            queue_done = true;
+        } else if (!c.large) {
             SmallArgs A;
             if ((err = small_args(pc, root, c.logn, P.dev, &A)) != OK) return err;
             A.jobs = (const ProdJob*)((char*)P.djobs + c.job_off);
@@ -309,6 +342,19 @@ int enqueue_classes(BatchPlan& P, const PrimeCtx& pc, cudaStream_t st) {
 void fill_jobs(BatchPlan& P, const u32* F, const int64_t* f_off, const u32* G, const int64_t* g_off, u32* H,
                const int64_t* h_off, std::vector<unsigned char>& out) {
     out.assign(P.jobs_bytes, 0);
+    // the queue's items, largest class first (pointers into this plan's job tables)
+    {
+        int it = 0;
+        for (auto c = P.classes.rbegin(); c != P.classes.rend(); ++c) {
+            if (!c->queued) continue;
+            const int ppc = small_ppc(c->logn), n = (int)c->members.size();
+            for (int k = 0; k < n; k += ppc) {
+                SmallItem I{(const ProdJob*)((char*)P.djobs + c->job_off + (size_t)k * sizeof(ProdJob)), c->logn,
+                            std::min(ppc, n - k)};
+                memcpy(out.data() + P.items_off + (size_t)it++ * sizeof(SmallItem), &I, sizeof(I));
+            }
+        }
+    }
     for (const ClassPlan& c : P.classes) {
         for (size_t k = 0; k < c.members.size(); ++k) {
             const int i = c.members[k];
@@ -484,7 +530,15 @@ int batch_launch_count(int count, const sfixn* df, const sfixn* dg) {
     std::map<int, int> cls;
     for (int i = 0; i < count; ++i) cls[product_logn((long long)df[i] + 1, (long long)dg[i] + 1)]++;
     int n = 0;
-    for (auto& kv : cls) n += kv.first > kMaxSmallLog ? 3 : 1;
+    bool queue = false;
+    for (auto& kv : cls) {
+        if (kv.first >= kQueueMinLog && kv.first <= kQueueMaxLog) {
+            n += queue ? 0 : 1;  // the queued classes share one launch
+            queue = true;
+        } else {
+            n += kv.first > kMaxSmallLog ? 3 : 1;
+        }
+    }
     return n;
 }
 

@@ -210,24 +210,24 @@ __device__ __forceinline__ void store_row32(u32* sm, int base, const u32 (&x)[32
             make_uint4(x[4 * c], x[4 * c + 1], x[4 * c + 2], x[4 * c + 3]);
 }
 
-template <int LOGL>
-__global__ void __launch_bounds__(small_threads(LOGL), small_ctas(LOGL))
-k_small_product(const __grid_constant__ SmallArgs A) {
+// The whole product of up to PPC jobs of one size class in one CTA of T =
+// small_threads(LOGL) threads: gjobs[0, njobs) (device job table), shared
+// memory sm (PPC * 2 * L words) and jobs (PPC entries).  C gives the prime
+// constants and the plan tables (pk, tw, tw_inv_off); scale = 2^32 / L.
+template <int LOGL, class Ctx>
+__device__ __forceinline__ void small_product_body(const Ctx& C, Tw scale, const ProdJob* __restrict__ gjobs,
+                                                   int njobs, u32* sm, ProdJob* jobs) {
     constexpr int L = 1 << LOGL;
     constexpr int T = small_threads(LOGL);
     constexpr int PPC = small_ppc(LOGL);
     constexpr LevelPlan PL = row_plan(LOGL);
-    extern __shared__ __align__(16) u32 sm[];
-    __shared__ ProdJob jobs[PPC];
-
-    const int job0 = blockIdx.x * PPC;
     for (int q = threadIdx.x; q < PPC; q += T) {
-        if (job0 + q < A.njobs) jobs[q] = A.jobs ? A.jobs[job0 + q] : A.job0;
+        if (q < njobs) jobs[q] = gjobs[q];
         else jobs[q] = ProdJob{nullptr, nullptr, nullptr, 0, 0, 0, 0};
     }
     __syncthreads();
 
-    const u32 p = A.pk.p, p2 = A.pk.p2, oneq = A.pk.one_q;
+    const u32 p = C.pk.p, p2 = C.pk.p2, oneq = C.pk.one_q;
     // load + zero pad + reduce to [0, 2p)
     for (int idx = threadIdx.x; idx < PPC * 2 * L; idx += T) {
         const int q = idx / (2 * L);
@@ -241,7 +241,7 @@ k_small_product(const __grid_constant__ SmallArgs A) {
     }
     __syncthreads();
 
-    small_fwd_levels<LOGL, 0, T, PPC>(sm, A);
+    small_fwd_levels<LOGL, 0, T, PPC>(sm, C);
 
     // last level (radix 32) forward on both operands, pointwise, inverse
     for (int id = threadIdx.x; id < PPC * (L / 32); id += T) {
@@ -251,25 +251,111 @@ k_small_product(const __grid_constant__ SmallArgs A) {
         u32 xf[32], xg[32];
         load_row32(xf, sm, base);
         load_row32(xg, sm, base + L);
-        dif_regs<32>(xf, A.pk.rc.f, p, p2);
-        dif_regs<32>(xg, A.pk.rc.f, p, p2);
+        dif_regs<32>(xf, C.pk.rc.f, p, p2);
+        dif_regs<32>(xg, C.pk.rc.f, p, p2);
 #pragma unroll
         for (int j = 0; j < 32; ++j) {
-            u32 h = mul_mont(xf[j], xg[j], p, A.pk.pinv_neg);
-            xf[j] = mul_shoup(h, A.scale.w, A.scale.wq, p);
+            u32 h = mul_mont(xf[j], xg[j], p, C.pk.pinv_neg);
+            xf[j] = mul_shoup(h, scale.w, scale.wq, p);
         }
-        dit_regs<32>(xf, A.pk.rc.i, p, p2);
+        dit_regs<32>(xf, C.pk.rc.i, p, p2);
         store_row32(sm, base, xf);
     }
     __syncthreads();
 
-    small_inv_levels<LOGL, PL.nlev - 2, T, PPC, 0>(sm, A);
+    small_inv_levels<LOGL, PL.nlev - 2, T, PPC, 0>(sm, C);
 
     // truncate + canonical residues
     for (int idx = threadIdx.x; idx < PPC * L; idx += T) {
         const int q = idx / L, i = idx % L;
         const ProdJob& J = jobs[q];
         if (i < J.lh) J.h[i] = red1(red2(sm[swz(q * 2 * L + i)], p2), p);
+    }
+}
+
+template <int LOGL>
+__global__ void __launch_bounds__(small_threads(LOGL), small_ctas(LOGL))
+k_small_product(const __grid_constant__ SmallArgs A) {
+    constexpr int PPC = small_ppc(LOGL);
+    extern __shared__ __align__(16) u32 sm[];
+    __shared__ ProdJob jobs[PPC];
+    const int job0 = blockIdx.x * PPC;
+    if (A.jobs) {
+        small_product_body<LOGL>(A, A.scale, A.jobs + job0, A.njobs - job0, sm, jobs);
+    } else {
+        small_product_body<LOGL>(A, A.scale, &A.job0, 1, sm, jobs);
+    }
+}
+
+// ------------------------------------------------------------ work queue --
+// All the small size classes of a batch (transforms of 2^5 .. 2^12 words:
+// the classes whose CTA is 128 threads with 32 KiB of products in shared
+// memory) in ONE persistent launch: each CTA takes the next work item -- up
+// to small_ppc(logn) products of one class -- from a device counter until
+// the queue is empty, so the classes share the SMs with no launch or tail
+// per class, larger items first.
+constexpr int kQueueMinLog = 5, kQueueMaxLog = 12;
+constexpr int kQueueThreads = 128;  // small_threads(logn) for every queued class
+constexpr int kQueueCtas = 6;       // small_ctas(logn) for every queued class
+constexpr int kQueueSmemWords = 2 << kQueueMaxLog;  // small_ppc(logn) * 2 * 2^logn for every queued class
+
+struct SmallItem {
+    const ProdJob* jobs;  // the item's jobs (device job table of its class)
+    int logn, njobs;      // njobs <= small_ppc(logn)
+};
+
+struct SmallQueueArgs {
+    PrimeK pk;
+    const Tw* tw[kQueueMaxLog + 1];  // plan tables of each class (forward then inverse)
+    int tw_inv_off[kQueueMaxLog + 1];
+    Tw scale[kQueueMaxLog + 1];      // 2^32 / 2^logn
+    const SmallItem* __restrict__ items;
+    int nitems;
+    int* counter;                    // next item; zero before the launch
+};
+
+// The level functions' view of one class: the prime constants stay in the
+// kernel parameters, the tables are the class's.
+struct SmallQueueCtx {
+    const PrimeK& pk;
+    const Tw* __restrict__ tw;
+    int tw_inv_off;
+};
+
+template <int LOGL>
+__device__ __forceinline__ void small_queue_item(const SmallQueueArgs& Q, const SmallItem& I, u32* sm,
+                                                 ProdJob* jobs) {
+    static_assert(small_threads(LOGL) == kQueueThreads, "queued classes run on 128 threads");
+    static_assert(small_ppc(LOGL) * 2 * (1 << LOGL) == kQueueSmemWords, "queued classes fill 32 KiB");
+    const SmallQueueCtx C{Q.pk, Q.tw[LOGL], Q.tw_inv_off[LOGL]};
+    small_product_body<LOGL>(C, Q.scale[LOGL], I.jobs, I.njobs, sm, jobs);
+}
+
+// (a template only so that every file including this header shares one kernel)
+template <int MAXLOG>
+__global__ void __launch_bounds__(kQueueThreads, kQueueCtas) k_small_queue(const __grid_constant__ SmallQueueArgs Q) {
+    static_assert(MAXLOG == kQueueMaxLog, "the queued classes");
+    extern __shared__ __align__(16) u32 sm[];
+    __shared__ ProdJob jobs[small_ppc(kQueueMinLog)];
+    __shared__ int item;
+    for (;;) {
+        if (threadIdx.x == 0) item = atomicAdd(Q.counter, 1);
+        __syncthreads();
+        const int it = item;
+        if (it >= Q.nitems) return;
+        const SmallItem I = Q.items[it];
+        switch (I.logn) {
+            case 5: small_queue_item<5>(Q, I, sm, jobs); break;
+            case 6: small_queue_item<6>(Q, I, sm, jobs); break;
+            case 7: small_queue_item<7>(Q, I, sm, jobs); break;
+            case 8: small_queue_item<8>(Q, I, sm, jobs); break;
+            case 9: small_queue_item<9>(Q, I, sm, jobs); break;
+            case 10: small_queue_item<10>(Q, I, sm, jobs); break;
+            case 11: small_queue_item<11>(Q, I, sm, jobs); break;
+            case 12: small_queue_item<12>(Q, I, sm, jobs); break;
+            default: break;
+        }
+        __syncthreads();  // the item's shared memory, jobs and `item` are free again
     }
 }
 

@@ -113,3 +113,24 @@ def test_device_batch_of_large_classes(cm):
         fa = F[f_off[i]:f_off[i] + a + 1]
         gb = G[g_off[i]:g_off[i] + b + 1]
         assert np.array_equal(H[h_off[i]:h_off[i] + a + b + 1], cm.fftmul_uni(fa, gb, P0)), i
+
+
+def test_queued_small_classes_many_items(cm, oracle_mod):
+    """Every product of transform length 2^5 .. 2^12 runs in the batch's one work-queue launch: thousands
+    of items of all eight classes, partial last items (counts not multiples of a class's products per
+    CTA), with large classes beside them; every product checked against the oracle's schoolbook."""
+    r = SplitMix64(14)
+    degs = []
+    for logn, count in [(5, 300), (6, 129), (7, 65), (8, 33), (9, 300), (10, 17), (11, 9), (12, 41)]:
+        hi = (1 << logn) - 1  # da + db + 1 <= 2^logn, > 2^(logn-1)
+        for _ in range(count):
+            da = int(r.next_u64(1)[0] % np.uint64(hi))
+            db = max(0, hi - 1 - da - int(r.next_u64(1)[0] % np.uint64(max(1, hi // 4))))
+            degs.append((da, db))
+    degs += [(20000, 30000), (8191, 8191)]
+    pairs = make_pairs(r, degs, P0)
+    for rep in range(2):  # the graph replayed: the queue counter is reset every launch
+        outs = cm.fftmul_batch(pairs, P0)
+        for (a, b), h in zip(pairs, outs):
+            want = oracle_mod.polymul_school(a, b, P0) if len(a) * len(b) < 1 << 22 else oracle_mod.polymul(a, b, P0)
+            assert np.array_equal(h, want)
