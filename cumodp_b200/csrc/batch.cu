@@ -8,14 +8,18 @@
 // (src/list_pointwise_mul.cu:43-194), each a separate synchronised launch.
 // Here a batch of any degrees is planned once per shape:
 //   * products are grouped by transform length n = 2^ceil(log2(la+lb-1));
-//   * a class with n <= 2^14 is one launch of the fused single-CTA kernel
-//     (several products per CTA below 2^12);
+//   * all classes with n <= 2^12 run in ONE persistent launch of the fused
+//     kernel (k_small_queue): CTAs pull work items (up to small_ppc(n)
+//     products of one class) from a device counter until none is left;
+//   * a class of 2^13 or 2^14 runs on the fused single-CTA kernel or on the
+//     three-pass kernels, as the autotuner measured faster for its size;
 //   * a larger class is the three-pass product over all its jobs at once,
 //     with the column/row split chosen by the autotuner;
-//   * every class runs on its own branch of one CUDA graph (classes are
-//     independent, so their kernels overlap on the device), captured once and
-//     replayed; job tables live in device memory and are refreshed with one
-//     copy when the caller's pointers change.
+//   * the queue and every other class run on their own branches of one CUDA
+//     graph (classes are independent, so their kernels overlap on the
+//     device), captured once and replayed; job tables and work items live in
+//     device memory and are refreshed with one copy when the caller's
+//     pointers change.
 #include <algorithm>
 #include <map>
 #include <chrono>
@@ -23,6 +27,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <string>
+#include <tuple>
 #include <unordered_map>
 
 #include "../../include/cumodp.h"
@@ -31,16 +37,25 @@
 namespace cmb {
 
 // ------------------------------------------------------------ autotuner ----
-// Chooses the row length 2^l2 of the three-pass split for a size class by
-// timing each legal split on a synthetic class of the same shape.  Results
-// are cached per (device, logn, job bucket) in memory and, when
-// CUMODP_TUNE_FILE names a file, appended to it and reloaded at start-up.
+// Per size class of a batch the autotuner chooses, by timing on a synthetic
+// class of the same shape (`jobs` products of two length-n/2 operands):
+//   * kind 0: the row length 2^l2 of the three-pass split (every legal split);
+//   * kind 1: for transforms of 2^13 and 2^14 words, one CTA per product
+//     (the fused kernel: 256 / 512 threads, 64 / 128 KiB of shared memory)
+//     or the three-pass kernels spread over the whole GPU (at the best split).
+// Results are cached per (device model, kind, logn, job bucket) in memory and,
+// when CUMODP_TUNE_FILE names a file, appended to it and reloaded at start-up;
+// the device model (name, SM count, compute capability) keys the cache, so a
+// file written on one GPU model is not used on another.
+std::vector<int> legal_row_logs(int logn);
+
 namespace {
 
 struct TuneKey {
-    int dev, logn, bucket;
+    std::string device;
+    int kind, logn, bucket;
     bool operator<(const TuneKey& o) const {
-        return std::tie(dev, logn, bucket) < std::tie(o.dev, o.logn, o.bucket);
+        return std::tie(device, kind, logn, bucket) < std::tie(o.device, o.kind, o.logn, o.bucket);
     }
 };
 
@@ -54,6 +69,28 @@ int job_bucket(int njobs) {
     return b;
 }
 
+// "name/SMs/sm_major.minor" of device dev (cached).
+const std::string& device_model(int dev) {
+    static std::mutex m;
+    static std::map<int, std::string> names;
+    std::lock_guard<std::mutex> g(m);
+    auto it = names.find(dev);
+    if (it != names.end()) return it->second;
+    cudaDeviceProp pr;
+    std::string key = "unknown";
+    if (cudaGetDeviceProperties(&pr, dev) == cudaSuccess) {
+        char buf[320];
+        snprintf(buf, sizeof(buf), "%s/%d/sm_%d.%d", pr.name, pr.multiProcessorCount, pr.major, pr.minor);
+        key = buf;
+        for (char& c : key)
+            if (c == ' ') c = '_';
+    } else {
+        cudaGetLastError();
+    }
+    return names[dev] = key;
+}
+
+// File lines: "kind logn bucket value device-model".
 void tune_load_locked() {
     if (g_tune_loaded) return;
     g_tune_loaded = true;
@@ -61,9 +98,103 @@ void tune_load_locked() {
     if (!f) return;
     FILE* fh = fopen(f, "r");
     if (!fh) return;
-    int dev, logn, bucket, l2;
-    while (fscanf(fh, "%d %d %d %d", &dev, &logn, &bucket, &l2) == 4) g_tune[TuneKey{dev, logn, bucket}] = l2;
+    int kind, logn, bucket, value;
+    char model[320];
+    while (fscanf(fh, "%d %d %d %d %319s", &kind, &logn, &bucket, &value, model) == 5)
+        g_tune[TuneKey{model, kind, logn, bucket}] = value;
     fclose(fh);
+}
+
+bool tune_lookup(const TuneKey& key, int* value) {
+    std::lock_guard<std::mutex> g(g_tune_m);
+    tune_load_locked();
+    auto it = g_tune.find(key);
+    if (it == g_tune.end()) return false;
+    *value = it->second;
+    return true;
+}
+
+void tune_store(const TuneKey& key, int value) {
+    std::lock_guard<std::mutex> g(g_tune_m);
+    g_tune[key] = value;
+    if (const char* f = getenv("CUMODP_TUNE_FILE")) {
+        if (FILE* fh = fopen(f, "a")) {
+            fprintf(fh, "%d %d %d %d %s\n", key.kind, key.logn, key.bucket, value, key.device.c_str());
+            fclose(fh);
+        }
+    }
+}
+
+// A synthetic class for timing: `jobs` products of two length-n/2 operands
+// (zeros: the work does not depend on the values), as three-pass jobs and as
+// single-CTA jobs.
+struct TuneBufs {
+    u32* buf = nullptr;
+    LargeJob* djl = nullptr;
+    ProdJob* djs = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    bool ok = false;
+    TuneBufs(int jobs, long long n, cudaStream_t st) {
+        if (dev_malloc((void**)&buf, (size_t)jobs * 4 * n * sizeof(u32)) != cudaSuccess ||
+            dev_malloc((void**)&djl, jobs * sizeof(LargeJob)) != cudaSuccess ||
+            dev_malloc((void**)&djs, jobs * sizeof(ProdJob)) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        cudaMemsetAsync(buf, 0, (size_t)jobs * 4 * n * sizeof(u32), st);
+        std::vector<LargeJob> hl(jobs);
+        std::vector<ProdJob> hs(jobs);
+        for (int j = 0; j < jobs; ++j) {
+            u32* base = buf + (size_t)j * 4 * n;
+            hl[j] = LargeJob{base, base + n / 2, base + n, (int)(n / 2), (int)(n / 2), (int)(n - 1), 0,
+                             base + 2 * n, base + 3 * n};
+            hs[j] = ProdJob{base, base + n / 2, base + n, (int)(n / 2), (int)(n / 2), (int)(n - 1), 0};
+        }
+        cudaMemcpyAsync(djl, hl.data(), jobs * sizeof(LargeJob), cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(djs, hs.data(), jobs * sizeof(ProdJob), cudaMemcpyHostToDevice, st);
+        cudaStreamSynchronize(st);
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        ok = true;
+    }
+    ~TuneBufs() {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (buf) cudaFree(buf);
+        if (djl) cudaFree(djl);
+        if (djs) cudaFree(djs);
+    }
+    // mean ms of three launches of `launch` after one warm-up (1e30 on error)
+    template <class F>
+    float time(F launch, cudaStream_t st) {
+        launch();
+        cudaEventRecord(e0, st);
+        for (int r = 0; r < 3; ++r) launch();
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        return cudaGetLastError() == cudaSuccess ? ms : 1e30f;
+    }
+};
+
+// Best split for a class of `jobs` products and its time.
+int tune_split(const PrimeCtx& pc, int logn, int jobs, int dev, cudaStream_t st, TuneBufs& T, float* best_ms) {
+    int best = default_row_log(logn);
+    *best_ms = 1e30f;
+    const u32 root = canonical_root(pc, logn);
+    for (int l2 : legal_row_logs(logn)) {
+        LargeArgs A;
+        if (large_args(pc, root, logn, l2, dev, &A) != OK) continue;
+        A.jobs = T.djl;
+        A.njobs = jobs;
+        const float ms = T.time([&] { launch_large(A, jobs, st); }, st);
+        if (ms < *best_ms) {
+            *best_ms = ms;
+            best = l2;
+        }
+    }
+    return best;
 }
 
 }  // namespace
@@ -80,71 +211,45 @@ std::vector<int> legal_row_logs(int logn) {
 int tune_row_log(const PrimeCtx& pc, int logn, int njobs, int dev, cudaStream_t st, bool allow_tuning) {
     const char* off = getenv("CUMODP_AUTOTUNE");
     if (off && off[0] == '0') return default_row_log(logn);
-    const TuneKey key{dev, logn, job_bucket(njobs)};
-    {
-        std::lock_guard<std::mutex> g(g_tune_m);
-        tune_load_locked();
-        auto it = g_tune.find(key);
-        if (it != g_tune.end()) return it->second;
-    }
+    const TuneKey key{device_model(dev), 0, logn, job_bucket(njobs)};
+    int v;
+    if (tune_lookup(key, &v)) return v;
     if (!allow_tuning) return default_row_log(logn);
     const std::vector<int> cands = legal_row_logs(logn);
     if (cands.size() <= 1) return cands.empty() ? default_row_log(logn) : cands[0];
-    // synthetic class: `jobs` products of two length-n/2 operands
     const int jobs = std::min(key.bucket, 32);
-    const long long n = 1ll << logn;
-    u32* buf = nullptr;
-    LargeJob* djobs = nullptr;
-    if (dev_malloc((void**)&buf, (size_t)jobs * 4 * n * sizeof(u32)) != cudaSuccess ||
-        dev_malloc((void**)&djobs, jobs * sizeof(LargeJob)) != cudaSuccess) {
-        cudaGetLastError();
-        if (buf) cudaFree(buf);
-        return default_row_log(logn);
-    }
-    cudaMemsetAsync(buf, 0, (size_t)jobs * 4 * n * sizeof(u32), st);
-    std::vector<LargeJob> hj(jobs);
-    for (int j = 0; j < jobs; ++j) {
-        u32* base = buf + (size_t)j * 4 * n;
-        hj[j] = LargeJob{base, base + n / 2, base + n, (int)(n / 2), (int)(n / 2), (int)(n - 1), 0,
-                         base + 2 * n, base + 3 * n};
-    }
-    cudaMemcpyAsync(djobs, hj.data(), jobs * sizeof(LargeJob), cudaMemcpyHostToDevice, st);
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    int best = default_row_log(logn);
-    float best_ms = 1e30f;
-    const u32 root = canonical_root(pc, logn);
-    for (int l2 : cands) {
-        LargeArgs A;
-        if (large_args(pc, root, logn, l2, dev, &A) != OK) continue;
-        A.jobs = djobs;
-        A.njobs = jobs;
-        launch_large(A, jobs, st);  // warm-up
-        cudaEventRecord(e0, st);
-        for (int r = 0; r < 3; ++r) launch_large(A, jobs, st);
-        cudaEventRecord(e1, st);
-        cudaEventSynchronize(e1);
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (cudaGetLastError() == cudaSuccess && ms < best_ms) {
-            best_ms = ms;
-            best = l2;
-        }
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaFree(buf);
-    cudaFree(djobs);
-    std::lock_guard<std::mutex> g(g_tune_m);
-    g_tune[key] = best;
-    if (const char* f = getenv("CUMODP_TUNE_FILE")) {
-        if (FILE* fh = fopen(f, "a")) {
-            fprintf(fh, "%d %d %d %d\n", key.dev, key.logn, key.bucket, best);
-            fclose(fh);
-        }
-    }
+    TuneBufs T(jobs, 1ll << logn, st);
+    if (!T.ok) return default_row_log(logn);
+    float ms;
+    const int best = tune_split(pc, logn, jobs, dev, st, T, &ms);
+    tune_store(key, best);
     return best;
+}
+
+bool tune_single_cta(const PrimeCtx& pc, int logn, int njobs, int dev, cudaStream_t st, bool allow_tuning) {
+    // the rule measured before tuning: a few products spread over the GPU, many on one CTA each
+    const bool rule = njobs > 16;
+    if (logn < single_large_min_log() || logn > kMaxSmallLog) return logn <= kMaxSmallLog;
+    const char* off = getenv("CUMODP_AUTOTUNE");
+    if (off && off[0] == '0') return rule;
+    const TuneKey key{device_model(dev), 1, logn, job_bucket(njobs)};
+    int v;
+    if (tune_lookup(key, &v)) return v != 0;
+    if (!allow_tuning) return rule;
+    const int jobs = key.bucket;  // the class's own size (up to 256 products: 64 MiB at 2^14)
+    TuneBufs T(jobs, 1ll << logn, st);
+    if (!T.ok) return rule;
+    float large_ms;
+    tune_split(pc, logn, jobs, dev, st, T, &large_ms);
+    SmallArgs A;
+    if (small_args(pc, canonical_root(pc, logn), logn, dev, &A) != OK) return rule;
+    A.jobs = T.djs;
+    A.njobs = jobs;
+    ensure_kernel_attrs();
+    const float small_ms = T.time([&] { launch_small(logn, A, jobs, st); }, st);
+    const bool single = small_ms <= large_ms;
+    tune_store(key, single ? 1 : 0);
+    return single;
 }
 
 // --------------------------------------------------------------- plans ----
@@ -222,7 +327,7 @@ int build_plan(BatchPlan& P, const PrimeCtx& pc, cudaStream_t st) {
         ClassPlan c = kv.second;
         // a few products of a length one CTA could hold still run faster
         // spread over many CTAs (the three-pass kernels)
-        c.large = c.logn > kMaxSmallLog || (c.logn >= single_large_min_log() && c.members.size() <= 16);
+        c.large = !tune_single_cta(pc, c.logn, (int)c.members.size(), P.dev, st, true);
         c.queued = !c.large && c.logn >= kQueueMinLog && c.logn <= kQueueMaxLog;
         if (c.queued) P.nitems += (int)((c.members.size() + small_ppc(c.logn) - 1) / small_ppc(c.logn));
         c.job_off = jb;
