@@ -874,7 +874,7 @@ def serving_c5(cm, rates=(1000, 3000, 10000, 30000, 100000), max_requests=20000,
     link = host_link_bound(torch, torch.device("cuda", torch.cuda.current_device()), 64 << 20, 64 << 20)
     link_bps = link["gbs_per_direction"] * 1e9
     out = {}
-    with cm.Server(max_batch=256, batch_window_us=50, lanes=4, host_budget=4 << 30) as srv:
+    with cm.Server(max_batch=256, batch_window_us=50, lanes=8, host_budget=4 << 30) as srv:
         srv.register(pool_u)
         srv.register(pool_i)
         # warm-up: tables for every prime and size class, lane buffers

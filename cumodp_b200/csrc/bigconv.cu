@@ -33,6 +33,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "../../include/cumodp.h"
 #include "exact.cuh"
@@ -404,6 +405,142 @@ int exact_i64_long_dev(const long long* a, long long la, const long long* b, lon
                        cudaStream_t st) {
     return bigconv_mul_dev((const unsigned long long*)a, la, (const unsigned long long*)b, lb, 1,
                            (unsigned long long*)c, 2, bw, st, nullptr);
+}
+
+// ------------------------------------------------- batches of one-limb products ----
+// With one limb (K = 1) the split is the residue of the whole coefficient and
+// the CRT of every output coefficient stands alone (no shifted sum across
+// x-coefficients), so the products of a batch that share their three primes
+// run as three elementwise kernels around one batched product per prime.
+
+bool exact_i64_long_one_limb(int bw, long long la, long long lb, u32* primes) {
+    BigPlan pl;
+    if (big_plan(bw, la, lb, &pl) != OK || pl.K != 1 || pl.nprimes != 3) return false;
+    for (int k = 0; k < 3; ++k) primes[k] = pl.p[k];
+    return true;
+}
+
+namespace {
+
+struct Prime3 {
+    u32 p[3];
+};
+
+// r_k[j] = x[j] mod p_k in [0, p_k), one word per thread and step.
+__global__ void k_i64_residues(const long long* __restrict__ x, long long n, Prime3 P, u32* __restrict__ r0,
+                               u32* __restrict__ r1, u32* __restrict__ r2) {
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n;
+         j += (long long)gridDim.x * blockDim.x) {
+        const long long v = x[j];
+        const unsigned long long m = v < 0 ? 0ull - (unsigned long long)v : (unsigned long long)v;
+        u32 r[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const u32 t = (u32)(m % P.p[k]);
+            r[k] = (v < 0 && t) ? P.p[k] - t : t;
+        }
+        r0[j] = r[0];
+        r1[j] = r[1];
+        r2[j] = r[2];
+    }
+}
+
+struct Crt3Args {
+    const u32* prod[3];  // canonical residues of each output coefficient
+    long long n;
+    u32 p[3];
+    u32 inv01, inv02, inv12;  // p0^-1 mod p1, p0^-1 mod p2, p1^-1 mod p2
+    long long* c;             // lo, hi words of each signed 128-bit result
+};
+
+// Garner's CRT of three residues to the x in [0, P), stored as the signed
+// value x - P when x > P / 2 (128-bit two's complement); one coefficient per
+// thread and step.  The big-coefficient CRT (k_big_crt) with one limb.
+__global__ void k_crt3_i128(const __grid_constant__ Crt3Args A) {
+    const unsigned __int128 P01 = (unsigned __int128)A.p[0] * A.p[1];
+    const unsigned __int128 P = P01 * A.p[2];
+    const unsigned __int128 half = P >> 1;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < A.n;
+         j += (long long)gridDim.x * blockDim.x) {
+        const u32 v0 = A.prod[0][j];
+        const u32 r1 = A.prod[1][j], r2 = A.prod[2][j];
+        const u32 v1 = (u32)((u64)((r1 + A.p[1] - v0 % A.p[1]) % A.p[1]) * A.inv01 % A.p[1]);
+        const u64 t2 = (u64)((r2 + A.p[2] - v0 % A.p[2]) % A.p[2]) * A.inv02 % A.p[2];
+        const u32 v2 = (u32)((t2 + A.p[2] - v1 % A.p[2]) % A.p[2] * A.inv12 % A.p[2]);
+        unsigned __int128 x = (unsigned __int128)v0 + (unsigned __int128)v1 * A.p[0] + (unsigned __int128)v2 * P01;
+        if (x > half) x -= P;  // wraps to the two's complement of x - P
+        A.c[2 * j] = (long long)(unsigned long long)x;
+        A.c[2 * j + 1] = (long long)(unsigned long long)(x >> 64);
+    }
+}
+
+size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+}  // namespace
+
+void exact_i64_batch_sizes(int cnt, const long long* la, const long long* lb, size_t* eval_words, size_t* ws_words,
+                           size_t* job_bytes) {
+    long long nin = 0, nout = 0;
+    for (int i = 0; i < cnt; ++i) {
+        nin += la[i] + lb[i];
+        nout += la[i] + lb[i] - 1;
+    }
+    *eval_words = 3 * (size_t)(nin + nout);
+    *ws_words = direct_ws_words(cnt, la, lb);
+    *job_bytes = 3 * round256(direct_job_bytes(cnt));
+}
+
+int exact_i64_long_batch(int cnt, const long long* x, const long long* la, const long long* lb, long long* c,
+                         const u32* primes, cudaStream_t st, const TwoConvBufs& B) {
+    if (cnt <= 0) return OK;
+    long long nin = 0, nout = 0;
+    std::vector<long long> lh(cnt), ia(cnt), ih(cnt);
+    for (int i = 0; i < cnt; ++i) {
+        if (la[i] <= 0 || lb[i] <= 0) return ASSUMPTION_ERROR;
+        ia[i] = nin;
+        ih[i] = nout;
+        lh[i] = la[i] + lb[i] - 1;
+        nin += la[i] + lb[i];
+        nout += lh[i];
+    }
+    u32* res[3];
+    u32* prod[3];
+    for (int k = 0; k < 3; ++k) {
+        res[k] = B.eval + (size_t)k * nin;
+        prod[k] = B.eval + 3 * (size_t)nin + (size_t)k * nout;
+    }
+    Prime3 P3;
+    for (int k = 0; k < 3; ++k) P3.p[k] = primes[k];
+    k_i64_residues<<<grid_of(nin), 256, 0, st>>>(x, nin, P3, res[0], res[1], res[2]);
+    int err = cuda_err(cudaGetLastError());
+    if (err != OK) return err;
+    const size_t jb = round256(direct_job_bytes(cnt));
+    std::vector<const u32*> pa(cnt), pb(cnt);
+    std::vector<u32*> ph(cnt);
+    for (int k = 0; k < 3; ++k) {
+        for (int i = 0; i < cnt; ++i) {
+            pa[i] = res[k] + ia[i];
+            pb[i] = res[k] + ia[i] + la[i];
+            ph[i] = prod[k] + ih[i];
+        }
+        // one workspace (stream-ordered reuse), a job table region per prime
+        // (the host writes each before its copy to the device has run)
+        err = direct_batch(cnt, pa.data(), la, pb.data(), lb, ph.data(), lh.data(), primes[k], B.ws,
+                           (char*)B.djobs + k * jb, (char*)B.hjobs + k * jb, st, false);
+        if (err != OK) return err;
+    }
+    Crt3Args C;
+    for (int k = 0; k < 3; ++k) {
+        C.prod[k] = prod[k];
+        C.p[k] = primes[k];
+    }
+    C.n = nout;
+    C.inv01 = powmod_exact(primes[0] % primes[1], primes[1] - 2, primes[1]);
+    C.inv02 = powmod_exact(primes[0] % primes[2], primes[2] - 2, primes[2]);
+    C.inv12 = powmod_exact(primes[1] % primes[2], primes[2] - 2, primes[2]);
+    C.c = c;
+    k_crt3_i128<<<grid_of(nout), 256, 0, st>>>(C);
+    return cuda_err(cudaGetLastError());
 }
 
 }  // namespace cmb

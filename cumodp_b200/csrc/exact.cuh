@@ -42,6 +42,19 @@ int exact_i64_long_dev_bufs(const long long* a, long long la, const long long* b
                             cudaStream_t st, const TwoConvBufs* bufs);
 void exact_i64_long_sizes(long long la, long long lb, int bw, size_t* eval_words, size_t* ws_words,
                           size_t* job_bytes);
+// Whether the big-coefficient plan of (la, lb, bw) has one limb and three
+// primes (written to primes[0..3)): the plan exact_i64_long_batch runs.
+bool exact_i64_long_one_limb(int bw, long long la, long long lb, u32* primes);
+// Buffers of exact_i64_long_batch for cnt products of lengths la, lb.
+void exact_i64_batch_sizes(int cnt, const long long* la, const long long* lb, size_t* eval_words, size_t* ws_words,
+                           size_t* job_bytes);
+// cnt exact products whose one-limb plans share the three primes, together:
+// x holds each product's a then b (la[i] + lb[i] words, products in order),
+// c receives each product's la[i] + lb[i] - 1 coefficients as (lo, hi)
+// pairs, in order; one residue kernel, one batched product per prime, one
+// CRT kernel, all on st and on the caller's buffers.
+int exact_i64_long_batch(int cnt, const long long* x, const long long* la, const long long* lb, long long* c,
+                         const u32* primes, cudaStream_t st, const TwoConvBufs& B);
 // Whether the exact product of (la, lb) with bit widths (ba, bb) takes the
 // big-coefficient path (method 0): no two-convolution plan, or a dearer one.
 bool exact_i64_prefers_long(int ba, int bb, long long la, long long lb);

@@ -236,6 +236,31 @@ cudaError_t dev_malloc_async(void** p, size_t bytes, cudaStream_t st) {
     return cudaMallocAsync(p, bytes, st);
 }
 
+// Host-to-device upload of a cached table that has landed when it returns.
+// cudaMemcpy from pageable memory may return once the words are staged,
+// before the DMA lands, and the kernels that read the table run on
+// non-blocking streams, which do not wait for it.
+static cudaError_t upload_now(void* d, const void* h, size_t bytes) {
+    static std::mutex m;
+    static std::map<int, cudaStream_t> streams;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaStream_t s;
+    {
+        std::lock_guard<std::mutex> g(m);
+        auto it = streams.find(dev);
+        if (it == streams.end()) {
+            cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+            streams[dev] = s;
+        } else {
+            s = it->second;
+        }
+    }
+    cudaError_t e = cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return e;
+}
+
 static const Tw* level_tables(int dev, u32 p, u32 root, int logl, int kind, int* err) {
     Caches& C = caches();
     std::lock_guard<std::mutex> g(C.m);
@@ -250,8 +275,13 @@ static const Tw* level_tables(int dev, u32 p, u32 root, int logl, int kind, int*
         *err = OUT_OF_MEMORY;
         return nullptr;
     }
+    if (upload_now(d, t.data(), t.size() * sizeof(Tw)) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(d);
+        *err = FFT_ERROR;
+        return nullptr;
+    }
     C.bytes += (long long)(t.size() * sizeof(Tw));
-    cudaMemcpy(d, t.data(), t.size() * sizeof(Tw), cudaMemcpyHostToDevice);
     C.tables[key] = d;
     return d;
 }
@@ -296,8 +326,13 @@ const u32* seed_tables(int dev, u32 p, u32 root, int logn, int* err) {
         *err = OUT_OF_MEMORY;
         return nullptr;
     }
+    if (upload_now(d, s.data(), s.size() * sizeof(u32)) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(d);
+        *err = FFT_ERROR;
+        return nullptr;
+    }
     C.bytes += (long long)(s.size() * sizeof(u32));
-    cudaMemcpy(d, s.data(), s.size() * sizeof(u32), cudaMemcpyHostToDevice);
     C.seeds[key] = d;
     return d;
 }

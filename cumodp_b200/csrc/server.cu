@@ -32,6 +32,7 @@
 #include <thread>
 #include <unordered_map>
 #include <unordered_set>
+#include <vector>
 
 #include "../../include/cumodp.h"
 #include "exact.cuh"
@@ -51,11 +52,14 @@ double now_us() {
 // from them in power-of-two sizes and coalesce with their buddies when freed,
 // so a shift in request sizes reuses the same memory.  `limit` bounds the
 // pinned bytes: beyond it get() fails (the server sheds the request).
+// Chunks are mapped into the device's address space, so kernels can read
+// and write slabs directly (dev_of).
 struct PinnedPool {
     static constexpr int kMinOrder = 12, kMaxChunkOrder = 28;
     int kChunkOrder = kMaxChunkOrder;  // chunk size: 256 MiB, or less under a smaller limit
     std::mutex m;
     std::vector<char*> chunks;
+    std::vector<char*> dchunks;  // each chunk's device address (null: not mapped)
     std::vector<std::unordered_set<uintptr_t>> free_blocks =
         std::vector<std::unordered_set<uintptr_t>>(kMaxChunkOrder + 1);
     size_t in_use = 0;          // bytes of slabs handed out and not yet returned
@@ -68,11 +72,17 @@ struct PinnedPool {
     bool add_chunk() {  // with m held
         if ((chunks.size() + 1) << kChunkOrder > limit) return false;
         void* p = nullptr;
-        if (cudaHostAlloc(&p, (size_t)1 << kChunkOrder, cudaHostAllocDefault) != cudaSuccess) {
+        if (cudaHostAlloc(&p, (size_t)1 << kChunkOrder, cudaHostAllocPortable | cudaHostAllocMapped) != cudaSuccess) {
             cudaGetLastError();
             return false;
         }
+        void* d = nullptr;
+        if (cudaHostGetDevicePointer(&d, p, 0) != cudaSuccess) {
+            cudaGetLastError();
+            d = nullptr;
+        }
         chunks.push_back((char*)p);
+        dchunks.push_back((char*)d);
         free_blocks[kChunkOrder].insert((uintptr_t)p);
         return true;
     }
@@ -127,6 +137,15 @@ struct PinnedPool {
         std::lock_guard<std::mutex> g(m);
         return in_use;
     }
+    // Device address of host address h inside a chunk, or null.
+    void* dev_of(const void* h) {
+        std::lock_guard<std::mutex> g(m);
+        const uintptr_t a = (uintptr_t)h;
+        for (size_t i = 0; i < chunks.size(); ++i)
+            if (a >= (uintptr_t)chunks[i] && a < (uintptr_t)chunks[i] + ((uintptr_t)1 << kChunkOrder))
+                return dchunks[i] ? dchunks[i] + (a - (uintptr_t)chunks[i]) : nullptr;
+        return nullptr;
+    }
     ~PinnedPool() {
         for (char* ch : chunks) cudaFreeHost(ch);
     }
@@ -149,6 +168,10 @@ struct Req {
     int bw = 1;
     TwoConvPlan plan{0, 0, 0, 0};  // exact products: the plan (sizes the lane buffers)
     bool long_path = false;         // exact products on the big-coefficient path (exact_i64_prefers_long)
+    // exact products with a one-limb plan over three primes: batched together
+    // (exact_i64_long_batch) whatever the single-product path
+    bool one_limb = false;
+    u32 primes[3] = {0, 0, 0};
     void* out;
     size_t bytes;
     double t_submit = 0, t_done = 0;
@@ -211,18 +234,74 @@ struct PinBuf {
     }
 };
 
+// Host <-> device copies of a batch.  A cudaMemcpyAsync costs the copy
+// engine about 4 us on top of its bytes (B200, PCIe host link: 1.1 GB/s for
+// 4 KiB copies, 31 GB/s for 256 KiB, 46-53 GB/s from 1 MiB), so a batch's
+// many small operands and results move instead through one kernel each way
+// that reads or writes the mapped host memory directly (41-43 GB/s at any
+// size).  Copies of kDmaMinBytes and more keep the copy engines: with
+// log-uniform request sizes they are a third of the copies and nearly all
+// the bytes, and a copy kernel holds SM slots while it waits on the link.
+constexpr size_t kDmaMinBytes = 128 << 10;
+constexpr u32 kCopyChunkWords = 8192;  // 32 KiB per table entry
+
+struct CopyChunk {
+    const u32* src;
+    u32* dst;
+    u32 words;
+    u32 pad;
+};
+
+// Copies every table entry (4-byte words; source or destination may be
+// mapped host memory), a block per entry and step, eight words in flight per
+// thread.  One 256-thread block per SM at most (kCopyBlocks): the blocks
+// spend their time waiting on the host link, and more of them would hold
+// SM slots that other lanes' product kernels need, for no more bandwidth.
+constexpr int kCopyBlocks = 148, kCopyInflight = 8;
+__global__ void __launch_bounds__(256) k_copy_chunks(const CopyChunk* __restrict__ t, int n) {
+    for (int c = blockIdx.x; c < n; c += gridDim.x) {
+        const CopyChunk ch = t[c];
+        for (u32 i = threadIdx.x; i < ch.words; i += kCopyInflight * blockDim.x) {
+            u32 v[kCopyInflight];
+#pragma unroll
+            for (int k = 0; k < kCopyInflight; ++k) {
+                const u32 j = i + k * blockDim.x;
+                if (j < ch.words) v[k] = ch.src[j];
+            }
+#pragma unroll
+            for (int k = 0; k < kCopyInflight; ++k) {
+                const u32 j = i + k * blockDim.x;
+                if (j < ch.words) ch.dst[j] = v[k];
+            }
+        }
+    }
+}
+
+void add_copy(std::vector<CopyChunk>& t, const void* src, void* dst, size_t bytes) {
+    const u32* s = (const u32*)src;
+    u32* d = (u32*)dst;
+    const size_t w = bytes / 4;
+    for (size_t i = 0; i < w; i += kCopyChunkWords)
+        t.push_back(CopyChunk{s + i, d + i, (u32)std::min<size_t>(kCopyChunkWords, w - i), 0});
+}
+
 struct Lane {
     cudaStream_t st = nullptr;
     cudaEvent_t ev = nullptr;
     DevBuf<u32> din, dout, ws;
     DevBuf<unsigned char> djobs;
     PinBuf<unsigned char> hjobs;
+    // the batch's copy tables (operands in, then results out)
+    PinBuf<CopyChunk> hcopy;
+    DevBuf<CopyChunk> dcopy;
     std::vector<Req*> reqs;
     int status = OK;
     bool busy = false;
     long long seq = 0;
     double t_start = 0, t_launched = 0;  // batch timing for the trace log
     double t_alloc = 0, t_copies = 0;    // after the buffer checks, after the operand copies
+    // trace only: device timestamps of the batch's start, operands in, kernels done, results out
+    cudaEvent_t tev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
 }  // namespace
@@ -236,9 +315,14 @@ struct Server {
     std::unordered_map<long long, Req*> reqs;
     std::vector<Lane> lanes;
     PinnedPool pool;
-    // host ranges registered by the caller (cumodp_server_register): start -> bytes
+    // host ranges registered by the caller (cumodp_server_register): start ->
+    // bytes and the range's device address (mapped registration)
+    struct RegRange {
+        size_t n;
+        uintptr_t dev;
+    };
     std::mutex reg_m;
-    std::map<uintptr_t, size_t> regs;
+    std::map<uintptr_t, RegRange> regs;
     std::atomic<size_t> direct_inflight{0};  // operand and result bytes of unfinished direct requests
     std::deque<int> dispatched;  // lane indices in dispatch order
     size_t inflight = 0;
@@ -246,6 +330,7 @@ struct Server {
     bool stop = false;
     std::thread batcher, completer;
     FILE* trace = nullptr;  // CUMODP_SERVER_TRACE: per-batch timing log
+    cudaEvent_t t_origin = nullptr;  // trace: device time origin of the lanes' timestamps
     // statistics
     std::vector<double> lat;
     long long completed = 0, failed = 0, batches = 0;
@@ -258,10 +343,19 @@ namespace {
 
 constexpr size_t kBatchBytes = 1ull << 30;
 
-// Lane buffers an exact product takes on its path (words, words, bytes).
+// Lane buffers an exact product takes on its own path, or (one-limb plans)
+// the larger of that and its share of a batched group (words, words, bytes).
 void exact_sizes(const Req& r, size_t* eval_words, size_t* ws_words, size_t* job_bytes) {
     if (r.long_path) exact_i64_long_sizes(r.la, r.lb, r.bw, eval_words, ws_words, job_bytes);
     else twoconv_buffer_sizes_plan(r.la, r.lb, r.plan, eval_words, ws_words, job_bytes);
+    if (r.one_limb) {
+        const long long la[1] = {r.la}, lb[1] = {r.lb};
+        size_t e, w, j;
+        exact_i64_batch_sizes(1, la, lb, &e, &w, &j);
+        *eval_words = std::max(*eval_words, e);
+        *ws_words = std::max(*ws_words, w);
+        *job_bytes = std::max(*job_bytes, j);
+    }
 }
 
 size_t req_bytes(const Req& r) {
@@ -276,29 +370,59 @@ size_t req_bytes(const Req& r) {
     return (r.la + r.lb + 2 * lc) * 8 + (ev + ws) * 4 + jb;
 }
 
-// Whether [p, p + n) lies in one range registered with the server.
-bool registered(Server& S, const void* p, size_t n) {
+// Whether [p, p + n) lies in one range registered with the server; if so
+// and dev is given, *dev = its device address (null when not mapped).
+bool registered(Server& S, const void* p, size_t n, void** dev = nullptr) {
     const uintptr_t a = (uintptr_t)p;
     std::lock_guard<std::mutex> g(S.reg_m);
     auto it = S.regs.upper_bound(a);
     if (it == S.regs.begin()) return false;
     --it;
-    return a >= it->first && a + n <= it->first + it->second;
+    if (!(a >= it->first && a + n <= it->first + it->second.n)) return false;
+    if (dev) *dev = it->second.dev ? (void*)(it->second.dev + (a - it->first)) : nullptr;
+    return true;
 }
 
-// Records [p, p + n) (already page-locked) as registered; false if it
-// overlaps a recorded range.
-bool register_range(Server& S, const void* p, size_t n) {
+// Records [p, p + n) (already page-locked; device address dev) as
+// registered; false if it overlaps a recorded range.
+bool register_range(Server& S, const void* p, size_t n, const void* dev) {
     const uintptr_t a = (uintptr_t)p;
     std::lock_guard<std::mutex> g(S.reg_m);
     auto it = S.regs.lower_bound(a);
     if (it != S.regs.end() && it->first < a + n) return false;
     if (it != S.regs.begin()) {
         auto pr = std::prev(it);
-        if (pr->first + pr->second > a) return false;
+        if (pr->first + pr->second.n > a) return false;
     }
-    S.regs[a] = n;
+    S.regs[a] = Server::RegRange{n, (uintptr_t)dev};
     return true;
+}
+
+// Device address of host memory [p, p + n) that a kernel may read or write:
+// inside a registered range or a pinned slab; null otherwise.
+void* dev_view(Server& S, const void* p, size_t n) {
+    void* d = nullptr;
+    if (registered(S, p, n, &d)) return d;
+    return S.pool.dev_of(p);
+}
+
+// Moves the batch's copy tables to the device (one copy) and launches the
+// copies of entries [0, nin); the entries after them are the results'.
+int stage_copies(Lane& L, const std::vector<CopyChunk>& t, int nin) {
+    if (t.empty()) return OK;
+    int err = OK;
+    if ((err = L.hcopy.ensure(t.size())) || (err = L.dcopy.ensure(t.size(), L.st))) return err;
+    std::memcpy(L.hcopy.p, t.data(), t.size() * sizeof(CopyChunk));
+    cudaError_t ce = cudaMemcpyAsync(L.dcopy.p, L.hcopy.p, t.size() * sizeof(CopyChunk), cudaMemcpyHostToDevice, L.st);
+    if (ce != cudaSuccess) return cuda_err(ce);
+    if (nin > 0) k_copy_chunks<<<std::min(nin, kCopyBlocks), 256, 0, L.st>>>(L.dcopy.p, nin);
+    return cuda_err(cudaGetLastError());
+}
+
+int launch_result_copies(Lane& L, int first, int count) {
+    if (count <= 0) return OK;
+    k_copy_chunks<<<std::min(count, kCopyBlocks), 256, 0, L.st>>>(L.dcopy.p + first, count);
+    return cuda_err(cudaGetLastError());
 }
 
 // Places a request's operands and result: straight from and into the
@@ -362,6 +486,26 @@ int run_batch(Server& S, Lane& L) {
     const u32 p = L.reqs[0]->p;
     const int cnt = (int)L.reqs.size();
     int err = OK;
+    auto mark = [&](int i) {
+        if (L.tev[i]) cudaEventRecord(L.tev[i], L.st);
+    };
+    // an operand copy: a table entry of the copy kernel when small and
+    // mapped, else the copy engines now
+    auto copy_in = [&](std::vector<CopyChunk>& t, const void* h, void* d, size_t bytes) -> cudaError_t {
+        void* v = bytes < kDmaMinBytes ? dev_view(S, h, bytes) : nullptr;
+        if (v) {
+            add_copy(t, v, d, bytes);
+            return cudaSuccess;
+        }
+        return cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, L.st);
+    };
+    // a result copy as a table entry; false: it goes by the copy engines
+    auto copy_out_table = [&](std::vector<CopyChunk>& t, const void* d, void* h, size_t bytes) {
+        void* v = bytes < kDmaMinBytes ? dev_view(S, h, bytes) : nullptr;
+        if (v) add_copy(t, d, v, bytes);
+        return v != nullptr;
+    };
+    mark(0);
     if (kind == 0) {
         std::vector<long long> la(cnt), lb(cnt), lh(cnt);
         size_t nin = 0, nout = 0;
@@ -380,16 +524,17 @@ int run_batch(Server& S, Lane& L) {
         L.t_alloc = now_us();
         std::vector<const u32*> pa(cnt), pb(cnt);
         std::vector<u32*> ph(cnt);
+        std::vector<CopyChunk> tab, tout;
+        std::vector<int> dma_out;  // requests whose results go by the copy engines
         size_t o = 0, q = 0;
         for (int i = 0; i < cnt; ++i) {
             Req* r = L.reqs[i];
             cudaError_t ce;
             if (r->a_src) {  // straight from the caller's registered memory
-                ce = cudaMemcpyAsync(L.din.p + o, r->a_src, r->la * 4, cudaMemcpyHostToDevice, L.st);
-                if (ce == cudaSuccess)
-                    ce = cudaMemcpyAsync(L.din.p + o + r->la, r->b_src, r->lb * 4, cudaMemcpyHostToDevice, L.st);
+                ce = copy_in(tab, r->a_src, L.din.p + o, r->la * 4);
+                if (ce == cudaSuccess) ce = copy_in(tab, r->b_src, L.din.p + o + r->la, r->lb * 4);
             } else {
-                ce = cudaMemcpyAsync(L.din.p + o, r->in, (r->la + r->lb) * 4, cudaMemcpyHostToDevice, L.st);
+                ce = copy_in(tab, r->in, L.din.p + o, (r->la + r->lb) * 4);
             }
             if (ce != cudaSuccess) return cuda_err(ce);
             pa[i] = L.din.p + o;
@@ -397,24 +542,55 @@ int run_batch(Server& S, Lane& L) {
             o += r->la + r->lb;
             ph[i] = L.dout.p + q;
             q += lh[i];
+            if (!copy_out_table(tout, ph[i], r->res_direct ? r->out : r->res, lh[i] * 4)) dma_out.push_back(i);
         }
+        const int nt_in = (int)tab.size();
+        tab.insert(tab.end(), tout.begin(), tout.end());
+        if ((err = stage_copies(L, tab, nt_in)) != OK) return err;
         L.t_copies = now_us();
+        mark(1);
         // no autotuning on the serving path: cached or default splits only
         err = direct_batch(cnt, pa.data(), la.data(), pb.data(), lb.data(), ph.data(), lh.data(), p, L.ws.p,
                            L.djobs.p, L.hjobs.p, L.st, false);
         if (err != OK) return err;
-        for (int i = 0; i < cnt; ++i) {
+        mark(2);
+        if ((err = launch_result_copies(L, nt_in, (int)tout.size())) != OK) return err;
+        for (int i : dma_out) {
             Req* r = L.reqs[i];
             cudaError_t ce = cudaMemcpyAsync(r->res_direct ? r->out : r->res, ph[i], lh[i] * 4,
                                              cudaMemcpyDeviceToHost, L.st);
             if (ce != cudaSuccess) return cuda_err(ce);
         }
     } else {
-        // exact products, one after another on the lane's stream
-        size_t nin = 0, nout = 0, evw = 0, wsw = 0, jbb = 0;
+        // exact products: those with a one-limb plan over the batch's first
+        // such prime triple run together (exact_i64_long_batch: their operands
+        // first in the buffers, one residue kernel, one batched product per
+        // prime, one CRT kernel); the others one after another
+        std::vector<Req*> grp, rest;
+        u32 gp[3] = {0, 0, 0};
+        for (Req* r : L.reqs) {
+            const u32* pp = r->primes;
+            if (r->one_limb && (grp.empty() || (pp[0] == gp[0] && pp[1] == gp[1] && pp[2] == gp[2]))) {
+                if (grp.empty()) std::copy(pp, pp + 3, gp);
+                grp.push_back(r);
+            } else {
+                rest.push_back(r);
+            }
+        }
+        const int ng = (int)grp.size();
+        std::vector<long long> gla(ng), glb(ng);
+        for (int i = 0; i < ng; ++i) {
+            gla[i] = grp[i]->la;
+            glb[i] = grp[i]->lb;
+        }
+        size_t nin = 0, nout = 0, evw = 0, wsw = 0, jbb = 0;  // eval and workspace: the largest of the steps
+        if (ng) exact_i64_batch_sizes(ng, gla.data(), glb.data(), &evw, &wsw, &jbb);
+        const size_t jb_grp = jbb;
         for (Req* r : L.reqs) {
             nin += r->la + r->lb;
             nout += 2 * (r->la + r->lb - 1);
+        }
+        for (Req* r : rest) {
             size_t e, w, j;
             exact_sizes(*r, &e, &w, &j);
             evw = std::max(evw, e);
@@ -430,16 +606,58 @@ int run_batch(Server& S, Lane& L) {
         u32* eval = L.dout.p + 2 * nout;
         long long* din64 = (long long*)L.din.p;
         long long* dout64 = (long long*)L.dout.p;
-        for (int i = 0; i < cnt; ++i) {
-            Req* r = L.reqs[i];
+        auto copy_in_dma = [&](Req* r, size_t at) {
             cudaError_t ce;
             if (r->a_src) {
-                ce = cudaMemcpyAsync(din64 + o, r->a_src, r->la * 8, cudaMemcpyHostToDevice, L.st);
+                ce = cudaMemcpyAsync(din64 + at, r->a_src, r->la * 8, cudaMemcpyHostToDevice, L.st);
                 if (ce == cudaSuccess)
-                    ce = cudaMemcpyAsync(din64 + o + r->la, r->b_src, r->lb * 8, cudaMemcpyHostToDevice, L.st);
+                    ce = cudaMemcpyAsync(din64 + at + r->la, r->b_src, r->lb * 8, cudaMemcpyHostToDevice, L.st);
             } else {
-                ce = cudaMemcpyAsync(din64 + o, r->in, (r->la + r->lb) * 8, cudaMemcpyHostToDevice, L.st);
+                ce = cudaMemcpyAsync(din64 + at, r->in, (r->la + r->lb) * 8, cudaMemcpyHostToDevice, L.st);
             }
+            return ce;
+        };
+        auto copy_out = [&](Req* r, size_t at) {
+            return cudaMemcpyAsync(r->res_direct ? r->out : r->res, dout64 + 2 * at, (r->la + r->lb - 1) * 16,
+                                   cudaMemcpyDeviceToHost, L.st);
+        };
+        if (ng) {
+            std::vector<CopyChunk> tab, tout;
+            std::vector<std::pair<Req*, size_t>> dma_out;  // results that go by the copy engines
+            for (Req* r : grp) {
+                cudaError_t ce;
+                if (r->a_src) {
+                    ce = copy_in(tab, r->a_src, din64 + o, r->la * 8);
+                    if (ce == cudaSuccess) ce = copy_in(tab, r->b_src, din64 + o + r->la, r->lb * 8);
+                } else {
+                    ce = copy_in(tab, r->in, din64 + o, (r->la + r->lb) * 8);
+                }
+                if (ce != cudaSuccess) return cuda_err(ce);
+                if (!copy_out_table(tout, dout64 + 2 * q, r->res_direct ? r->out : r->res, (r->la + r->lb - 1) * 16))
+                    dma_out.emplace_back(r, q);
+                o += r->la + r->lb;
+                q += r->la + r->lb - 1;
+            }
+            const int nt_in = (int)tab.size();
+            tab.insert(tab.end(), tout.begin(), tout.end());
+            if ((err = stage_copies(L, tab, nt_in)) != OK) return err;
+            mark(1);
+            TwoConvBufs B{eval, L.ws.p, L.djobs.p, L.hjobs.p};
+            err = exact_i64_long_batch(ng, din64, gla.data(), glb.data(), dout64, gp, L.st, B);
+            if (err != OK) return err;
+            mark(2);
+            if ((err = launch_result_copies(L, nt_in, (int)tout.size())) != OK) return err;
+            for (auto& rq : dma_out) {
+                cudaError_t ce = copy_out(rq.first, rq.second);
+                if (ce != cudaSuccess) return cuda_err(ce);
+            }
+            jo = jb_grp;
+        } else {
+            mark(1);
+            mark(2);
+        }
+        for (Req* r : rest) {
+            cudaError_t ce = copy_in_dma(r, o);
             if (ce != cudaSuccess) return cuda_err(ce);
             TwoConvBufs B{eval, L.ws.p, L.djobs.p + jo, L.hjobs.p + jo};
             size_t e, w, j;
@@ -450,15 +668,15 @@ int run_batch(Server& S, Lane& L) {
                       : twoconv_mul_dev(din64 + o, r->la, din64 + o + r->la, r->lb, dout64 + 2 * q, r->bw, r->bw,
                                         false, L.st, nullptr, &B);
             if (err != OK) return err;
-            ce = cudaMemcpyAsync(r->res_direct ? r->out : r->res, dout64 + 2 * q, (r->la + r->lb - 1) * 16,
-                                 cudaMemcpyDeviceToHost, L.st);
+            ce = copy_out(r, q);
             if (ce != cudaSuccess) return cuda_err(ce);
             o += r->la + r->lb;
             q += r->la + r->lb - 1;
             jo += j;
         }
-        L.t_copies = now_us();
+        L.t_copies = now_us();  // the group's phases are marked; the others run in the last one
     }
+    mark(3);
     return cuda_err(cudaEventRecord(L.ev, L.st));
 }
 
@@ -574,13 +792,22 @@ void completer_loop(Server* Sp) {
         }
         if (S.trace) {
             // one line per batch: start, host launch time, completion seen,
-            // kind, prime, requests, operand words, status
+            // kind, prime, requests, operand words, status, host time to the
+            // buffer checks and to the operand copies issued (us)
             long long words = 0;
             for (Req* r : L.reqs) words += r->la + r->lb;
-            std::fprintf(S.trace, "%.1f %.1f %.1f %d %u %zu %lld %d %.1f %.1f\n", L.t_start, L.t_launched - L.t_start,
-                         now_us() - L.t_start, L.reqs.empty() ? -1 : L.reqs[0]->kind,
+            // then the device side: start after the origin, operands in, kernels, results out (us)
+            float d[4] = {-1.f, -1.f, -1.f, -1.f};
+            if (st == OK && L.tev[0] && S.t_origin) {
+                cudaEventElapsedTime(&d[0], S.t_origin, L.tev[0]);
+                for (int i = 1; i < 4; ++i) cudaEventElapsedTime(&d[i], L.tev[i - 1], L.tev[i]);
+                cudaGetLastError();
+            }
+            std::fprintf(S.trace, "%.1f %.1f %.1f %d %u %zu %lld %d %.1f %.1f %.1f %.1f %.1f %.1f\n", L.t_start,
+                         L.t_launched - L.t_start, now_us() - L.t_start, L.reqs.empty() ? -1 : L.reqs[0]->kind,
                          L.reqs.empty() ? 0u : L.reqs[0]->p, L.reqs.size(), words, st,
-                         L.t_alloc ? L.t_alloc - L.t_start : -1.0, L.t_copies ? L.t_copies - L.t_start : -1.0);
+                         L.t_alloc ? L.t_alloc - L.t_start : -1.0, L.t_copies ? L.t_copies - L.t_start : -1.0,
+                         d[0] * 1e3, d[1] * 1e3, d[2] * 1e3, d[3] * 1e3);
         }
         lk.lock();
         size_t freed = 0;
@@ -707,6 +934,7 @@ long long submit_i64_req(Server& Sr, long long na, const int64_t* a, long long n
     if (e == OK) {
         r->long_path = exact_i64_prefers_long(r->bw, r->bw, na, nb);
         if (!r->long_path) e = twoconv_plan(r->bw, r->bw, na, nb, false, &r->plan);
+        r->one_limb = e == OK && exact_i64_long_one_limb(r->bw, na, nb, r->primes);
     }
     if (e != OK) r->status = e;
     else {
@@ -839,9 +1067,13 @@ cumodp_server* cumodp_server_create(const cumodp_server_config* cfg) {
     // batch holds at most kBatchBytes; only a single larger request grows them)
     const size_t jobs = std::max(direct_job_bytes(c.max_batch), (size_t)c.max_batch * 3 * direct_job_bytes(8));
     const size_t words = std::min<size_t>(kBatchBytes, c.memory_budget / (3 * (size_t)c.lanes)) / 4;
+    // copy tables: up to three copies per request below kDmaMinBytes, 16 entries each
+    const size_t copy_entries = 3 * (size_t)c.max_batch * (kDmaMinBytes / (4 * kCopyChunkWords));
     for (Lane& L : S->lanes) {
         L.hjobs.ensure(jobs);
         L.djobs.ensure(jobs, L.st);
+        L.hcopy.ensure(copy_entries);
+        L.dcopy.ensure(copy_entries, L.st);
         L.din.ensure(words, L.st);
         L.dout.ensure(words, L.st);
         L.ws.ensure(words, L.st);
@@ -853,6 +1085,14 @@ cumodp_server* cumodp_server_create(const cumodp_server_config* cfg) {
     S->pool.set_limit(c.host_budget ? c.host_budget : (2ull << 30));
     S->pool.reserve(S->pool.limit);
     if (const char* tf = getenv("CUMODP_SERVER_TRACE")) S->trace = fopen(tf, "a");
+    if (S->trace) {
+        cudaEventCreate(&S->t_origin);
+        cudaEventRecord(S->t_origin, S->lanes[0].st);
+        for (Lane& L : S->lanes)
+            for (cudaEvent_t& e : L.tev) cudaEventCreate(&e);
+        cudaStreamSynchronize(S->lanes[0].st);
+        cudaGetLastError();
+    }
     S->batcher = std::thread(batcher_loop, S);
     S->completer = std::thread(completer_loop, S);
     return (cumodp_server*)S;
@@ -911,11 +1151,16 @@ cumodp_err cumodp_server_register(cumodp_server* h, void* ptr, size_t bytes) {
     if (!S || !ptr || bytes == 0) return CUMODP_ASSUMPTION_ERROR;
     if (registered(*S, ptr, 1) || registered(*S, (char*)ptr + bytes - 1, 1)) return CUMODP_ASSUMPTION_ERROR;
     cudaSetDevice(S->dev);
-    if (cudaHostRegister(ptr, bytes, cudaHostRegisterPortable) != cudaSuccess) {
+    if (cudaHostRegister(ptr, bytes, cudaHostRegisterPortable | cudaHostRegisterMapped) != cudaSuccess) {
         cudaGetLastError();
         return CUMODP_FAILURE;
     }
-    if (!register_range(*S, ptr, bytes)) {
+    void* dev = nullptr;
+    if (cudaHostGetDevicePointer(&dev, ptr, 0) != cudaSuccess) {
+        cudaGetLastError();
+        dev = nullptr;  // copies from this range then go through the copy engines
+    }
+    if (!register_range(*S, ptr, bytes, dev)) {
         cudaHostUnregister(ptr);
         return CUMODP_ASSUMPTION_ERROR;
     }
@@ -989,10 +1234,15 @@ void cumodp_server_destroy(cumodp_server* h) {
     for (Lane& L : S->lanes) {
         if (L.st) cudaStreamSynchronize(L.st);
         L.din.release(L.st); L.dout.release(L.st); L.ws.release(L.st); L.djobs.release(L.st);
+        L.dcopy.release(L.st);
         L.hjobs.release();
+        L.hcopy.release();
         if (L.st) cudaStreamDestroy(L.st);
         if (L.ev) cudaEventDestroy(L.ev);
+        for (cudaEvent_t e : L.tev)
+            if (e) cudaEventDestroy(e);
     }
+    if (S->t_origin) cudaEventDestroy(S->t_origin);
     if (S->trace) fclose(S->trace);
     for (auto& kv : S->regs) cudaHostUnregister((void*)kv.first);  // ranges the caller left registered
     cudaGetLastError();

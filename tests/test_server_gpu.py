@@ -242,3 +242,23 @@ def test_long_exact_requests_match_the_host_entry(cm):
         for (rid, out), w in zip(subs, want):
             assert srv.wait(rid) == 0
             assert np.array_equal(out, w)
+
+
+def test_exact_batch_mixes_plans(cm):
+    """One batch of exact requests on three plans: one-limb big-coefficient products (run together as one
+    batched product per prime), two-limb ones (|c| ~ 2^50) and small coefficients on the two-convolution
+    path (both one after another); every result equals cumodp_twoconv_mul_i64's, in any order of arrival."""
+    r = SplitMix64(2033)
+    ops = []
+    for i in range(18):
+        bound = (10**10, 1 << 50, 100)[i % 3]
+        na, nb = [(3000, 5000), (1, 70000), (40000, 9), (65536, 65536), (17, 33), (123457, 1000)][i % 6]
+        ops.append((r.int64_in(na, bound), r.int64_in(nb, bound)))
+    want = [cm.twoconv_mul(a, b, raw=True) for a, b in ops]
+    with cm.Server(max_batch=64, batch_window_us=20000) as srv:
+        subs = [srv.submit_i64(a, b) for a, b in ops]
+        for (rid, out), w in zip(subs, want):
+            assert srv.wait(rid) == 0
+            assert np.array_equal(out, w)
+        st = srv.stats()
+    assert st["batches"] <= 3  # the burst shared batches
