@@ -34,8 +34,9 @@ def test_product_table_allocation_failure_then_recovery(cm, oracle_mod):
 def test_batch_plan_allocation_failure_then_recovery(cm, oracle_mod, failures):
     p = 377487361  # unused elsewhere; a batch shape of its own
     r = SplitMix64(0xC0DA0602 + failures)
-    # fused single-CTA classes only: no autotuning allocations before the plan's own
-    pairs = [(r.residues(int(d), p), r.residues(int(d) + 7, p)) for d in (100 + failures, 3000, 7000)] * 20
+    # classes of 2^8-2^12 only (the work-queue kernel): the autotuner times the 2^13 and 2^14 classes
+    # (scratch allocations of its own, whose failure only falls back to the default choice), these not
+    pairs = [(r.residues(int(d), p), r.residues(int(d) + 7, p)) for d in (100 + failures, 1000, 2000)] * 20
     cm.inject_alloc_failures(failures)
     with pytest.raises(cm.CumodpError) as e:
         cm.fftmul_batch(pairs, p)

@@ -240,3 +240,46 @@ def test_comparison_switches_give_the_same_products(cm):
         assert out.returncode == 0, out.stderr[-2000:]
         res.append(out.stdout.strip().splitlines()[-1])
     assert res[0] == res[1]
+
+
+_FIRST_USE = r"""
+import sys, numpy as np, torch
+sys.path.insert(0, sys.argv[1])
+import cumodp_b200 as cm
+from cumodp_b200.workloads import SplitMix64
+# the first products of this process, each on a prime and size nothing here has used yet: the
+# library builds and uploads its tables inside the call, then launches on a non-blocking stream
+st = torch.cuda.Stream()
+r = SplitMix64(424242)
+bad = 0
+cases = [(645922817, 300000, 250000), (595591169, 70000, 90000), (377487361, 20000, 30000),
+         (167772161, 500000, 600000), (998244353, 5000, 3000), (897581057, 130000, 1)]
+outs = []
+with torch.cuda.stream(st):
+    for p, na, nb in cases:
+        a, b = r.residues(na, p), r.residues(nb, p)
+        F = torch.from_numpy(a.view(np.int32)).cuda(non_blocking=True)
+        G = torch.from_numpy(b.view(np.int32)).cuda(non_blocking=True)
+        H = torch.empty(na + nb - 1, dtype=torch.int32, device="cuda")
+        cm.fftmul_uni_dev(H.data_ptr(), na + nb - 1, F.data_ptr(), na - 1, G.data_ptr(), nb - 1, p, st.cuda_stream)
+        outs.append((p, a, b, H))
+st.synchronize()
+for p, a, b, H in outs:
+    bad += not np.array_equal(H.cpu().numpy().view(np.uint32), cm.fftmul_uni(a, b, p))
+print("BAD", bad)
+"""
+
+
+def test_first_use_tables_on_a_non_blocking_stream(cm, tmp_path):
+    """A fresh process's first products (new primes and sizes: tables built and uploaded inside the call)
+    launched on a non-blocking stream equal the host entry's products: the upload has landed before the
+    kernels that read it run."""
+    import os
+    import subprocess
+    import sys
+    script = tmp_path / "first_use.py"
+    script.write_text(_FIRST_USE)
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, str(script), root], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert "BAD 0" in out.stdout, out.stdout[-2000:]
