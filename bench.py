@@ -843,7 +843,7 @@ def _page_aligned(values: np.ndarray) -> np.ndarray:
     return out
 
 
-def serving_c5(cm, rates=(1000, 3000, 10000, 30000, 100000), max_requests=20000, max_seconds=2.0, threads=4):
+def serving_c5(cm, rates=(1000, 3000, 10000, 30000, 100000), max_requests=100000, max_seconds=10.0, threads=4):
     """Config 5: Poisson arrivals of mixed requests into the continuous-batching server.
 
     Degrees log-uniform in [2^5, 2^20]; prime uniform over {469762049,
