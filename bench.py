@@ -662,7 +662,19 @@ def batched_c4(cm, torch, dev, stream):
     t_c_wall = (time.perf_counter() - t0) * 1000
     t_c = e0.elapsed_time(e1)
     same_c = bool(torch.equal(H, H1))
+    # algorithmic bytes of the batch: per pair, its operands and result for a transform of n <= 2^14
+    # (one pass), else the pass-aware 24 n ceil(log2 n / 14) of three transforms
+    alg = 0
+    for a, b in zip(da.tolist(), db.tolist()):
+        logn = max(0, int(a + b).bit_length())  # n = 2^ceil(log2(a + b + 1))
+        alg += 4 * (a + 1) + 4 * (b + 1) + 4 * (a + b + 1) if logn <= 14 else 24 * (1 << logn) * -(-logn // 14)
+    peak, kind = peaks()
+    gbs = alg / (t_batch * 1e-3) / 1e9
     return {"pairs": cnt, "ms_batched": round(t_batch, 4), "products_per_s_batched": round(cnt / (t_batch / 1000), 1),
+            "roofline": {"bound": "hbm", "alg_bytes": alg, "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(gbs / peak, 4), "peak_kind": kind,
+                         "how": "per pair 4(da+1)+4(db+1)+4(da+db+1) bytes when n <= 2^14, else "
+                                "24 n ceil(log2 n / 14), over the batched call's CUDA-event time"},
             "ms_one_call_per_pair": round(t_single, 4), "ms_one_call_per_pair_wall": round(t_single_wall, 4),
             "speedup_vs_one_call": round(t_single / t_batch, 2), "batched_equals_single": same,
             "one_call_per_pair_c_loop": {"ms": round(t_c, 4), "ms_wall": round(t_c_wall, 4),
