@@ -24,6 +24,17 @@ struct ProdJob {
     int pad;
 };
 
+// A job as the single-CTA kernels keep it in shared memory: 32 bytes
+// instead of 40 (operand lengths are at most 2^14 there), so that the job
+// slots of a 128-product CTA take 4 KiB and six 32 KiB CTAs fit an SM.
+struct SmemJob {
+    const u32* a;
+    const u32* b;
+    u32* h;
+    unsigned short la, lb;
+    int lh;
+};
+
 // What the shared-memory row levels need: prime constants and the plan's
 // twiddle tables.
 struct RowCtx {
@@ -216,14 +227,18 @@ __device__ __forceinline__ void store_row32(u32* sm, int base, const u32 (&x)[32
 // constants and the plan tables (pk, tw, tw_inv_off); scale = 2^32 / L.
 template <int LOGL, class Ctx>
 __device__ __forceinline__ void small_product_body(const Ctx& C, Tw scale, const ProdJob* __restrict__ gjobs,
-                                                   int njobs, u32* sm, ProdJob* jobs) {
+                                                   int njobs, u32* sm, SmemJob* jobs) {
     constexpr int L = 1 << LOGL;
     constexpr int T = small_threads(LOGL);
     constexpr int PPC = small_ppc(LOGL);
     constexpr LevelPlan PL = row_plan(LOGL);
     for (int q = threadIdx.x; q < PPC; q += T) {
-        if (q < njobs) jobs[q] = gjobs[q];
-        else jobs[q] = ProdJob{nullptr, nullptr, nullptr, 0, 0, 0, 0};
+        if (q < njobs) {
+            const ProdJob g = gjobs[q];
+            jobs[q] = SmemJob{g.a, g.b, g.h, (unsigned short)g.la, (unsigned short)g.lb, g.lh};
+        } else {
+            jobs[q] = SmemJob{nullptr, nullptr, nullptr, 0, 0, 0};
+        }
     }
     __syncthreads();
 
@@ -233,7 +248,7 @@ __device__ __forceinline__ void small_product_body(const Ctx& C, Tw scale, const
         const int q = idx / (2 * L);
         const int op = (idx / L) & 1;
         const int i = idx % L;
-        const ProdJob& J = jobs[q];
+        const SmemJob& J = jobs[q];
         const u32* src = op ? J.b : J.a;
         const int len = op ? J.lb : J.la;
         u32 v = (i < len) ? __ldg(src + i) : 0u;
@@ -268,7 +283,7 @@ __device__ __forceinline__ void small_product_body(const Ctx& C, Tw scale, const
     // truncate + canonical residues
     for (int idx = threadIdx.x; idx < PPC * L; idx += T) {
         const int q = idx / L, i = idx % L;
-        const ProdJob& J = jobs[q];
+        const SmemJob& J = jobs[q];
         if (i < J.lh) J.h[i] = red1(red2(sm[swz(q * 2 * L + i)], p2), p);
     }
 }
@@ -278,7 +293,7 @@ __global__ void __launch_bounds__(small_threads(LOGL), small_ctas(LOGL))
 k_small_product(const __grid_constant__ SmallArgs A) {
     constexpr int PPC = small_ppc(LOGL);
     extern __shared__ __align__(16) u32 sm[];
-    __shared__ ProdJob jobs[PPC];
+    __shared__ SmemJob jobs[PPC];
     const int job0 = blockIdx.x * PPC;
     if (A.jobs) {
         small_product_body<LOGL>(A, A.scale, A.jobs + job0, A.njobs - job0, sm, jobs);
@@ -324,7 +339,7 @@ struct SmallQueueCtx {
 
 template <int LOGL>
 __device__ __forceinline__ void small_queue_item(const SmallQueueArgs& Q, const SmallItem& I, u32* sm,
-                                                 ProdJob* jobs) {
+                                                 SmemJob* jobs) {
     static_assert(small_threads(LOGL) == kQueueThreads, "queued classes run on 128 threads");
     static_assert(small_ppc(LOGL) * 2 * (1 << LOGL) == kQueueSmemWords, "queued classes fill 32 KiB");
     const SmallQueueCtx C{Q.pk, Q.tw[LOGL], Q.tw_inv_off[LOGL]};
@@ -336,7 +351,7 @@ template <int MAXLOG>
 __global__ void __launch_bounds__(kQueueThreads, kQueueCtas) k_small_queue(const __grid_constant__ SmallQueueArgs Q) {
     static_assert(MAXLOG == kQueueMaxLog, "the queued classes");
     extern __shared__ __align__(16) u32 sm[];
-    __shared__ ProdJob jobs[small_ppc(kQueueMinLog)];
+    __shared__ SmemJob jobs[small_ppc(kQueueMinLog)];
     __shared__ int item;
     for (;;) {
         if (threadIdx.x == 0) item = atomicAdd(Q.counter, 1);

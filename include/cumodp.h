@@ -293,11 +293,15 @@ cumodp_err cumodp_server_replay(cumodp_server *s, long long count, const double 
                                 const void *const *b, void *const *h, int threads, double *lat_us, int *status,
                                 double *span_us);
 /* Addition.  Registers the caller's host memory [ptr, ptr + bytes) with the
- * server (page-locked in place, cudaHostRegister).  A request whose two
+ * server (page-locked in place and mapped into the device's address space,
+ * cudaHostRegister with cudaHostRegisterMapped).  A request whose two
  * operands lie in registered memory is copied to the device straight from
  * there, and a result buffer that lies in registered memory receives the
  * result straight from the device: no copy through the server's pinned slabs
- * and no host memcpy on either side.  The caller leaves such operands
+ * and no host memcpy on either side.  Copies under 128 KiB are made by one
+ * kernel per batch that reads or writes the mapped memory (a copy-engine
+ * transfer costs about 4 us of its own, whatever its size); larger ones by
+ * the copy engines.  The caller leaves such operands
  * unchanged until the request completes.  Unfinished requests still count
  * their operand and result bytes against host_budget, which keeps bounding
  * the backlog (shedding beyond it).  Ranges may not overlap.  Unregister only
