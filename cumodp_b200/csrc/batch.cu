@@ -217,7 +217,9 @@ int tune_row_log(const PrimeCtx& pc, int logn, int njobs, int dev, cudaStream_t 
     if (!allow_tuning) return default_row_log(logn);
     const std::vector<int> cands = legal_row_logs(logn);
     if (cands.size() <= 1) return cands.empty() ? default_row_log(logn) : cands[0];
-    const int jobs = std::min(key.bucket, 32);
+    // timed at the class's own size (its bucket), up to 2^25 operand words: a split that wins for a few
+    // products (many small CTAs) can lose for hundreds
+    const int jobs = std::min(key.bucket, std::max(1, (int)((1ll << 25) >> logn)));
     TuneBufs T(jobs, 1ll << logn, st);
     if (!T.ok) return default_row_log(logn);
     float ms;
