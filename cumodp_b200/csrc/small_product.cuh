@@ -243,16 +243,31 @@ __device__ __forceinline__ void small_product_body(const Ctx& C, Tw scale, const
     __syncthreads();
 
     const u32 p = C.pk.p, p2 = C.pk.p2, oneq = C.pk.one_q;
-    // load + zero pad + reduce to [0, 2p)
-    for (int idx = threadIdx.x; idx < PPC * 2 * L; idx += T) {
-        const int q = idx / (2 * L);
-        const int op = (idx / L) & 1;
-        const int i = idx % L;
-        const SmemJob& J = jobs[q];
-        const u32* src = op ? J.b : J.a;
-        const int len = op ? J.lb : J.la;
-        u32 v = (i < len) ? __ldg(src + i) : 0u;
-        sm[swz(idx)] = mul_shoup(v, 1u, oneq, p);
+    // load + zero pad + reduce to [0, 2p), kLoadBatch independent loads in
+    // flight per thread before any is stored (one at a time, a thread waited
+    // out a global-load latency per word)
+    constexpr int TOT = PPC * 2 * L, kLoadBatch = 8;
+    for (int base = threadIdx.x; base < TOT; base += kLoadBatch * T) {
+        u32 v[kLoadBatch];
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            const int idx = base + u * T;
+            v[u] = 0u;
+            if (idx < TOT) {
+                const int q = idx / (2 * L);
+                const int op = (idx / L) & 1;
+                const int i = idx % L;
+                const SmemJob& J = jobs[q];
+                const u32* src = op ? J.b : J.a;
+                const int len = op ? J.lb : J.la;
+                if (i < len) v[u] = __ldg(src + i);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kLoadBatch; ++u) {
+            const int idx = base + u * T;
+            if (idx < TOT) sm[swz(idx)] = mul_shoup(v[u], 1u, oneq, p);
+        }
     }
     __syncthreads();
 
