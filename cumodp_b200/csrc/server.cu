@@ -239,10 +239,12 @@ struct PinBuf {
 // 4 KiB copies, 31 GB/s for 256 KiB, 46-53 GB/s from 1 MiB), so a batch's
 // many small operands and results move instead through one kernel each way
 // that reads or writes the mapped host memory directly (41-43 GB/s at any
-// size).  Copies of kDmaMinBytes and more keep the copy engines: with
-// log-uniform request sizes they are a third of the copies and nearly all
-// the bytes, and a copy kernel holds SM slots while it waits on the link.
-constexpr size_t kDmaMinBytes = 128 << 10;
+// size).  Copies of kDmaMinBytes and more keep the copy engines, which
+// pass the kernel from about 1 MiB on; a copy kernel also holds SM slots
+// while it waits on the link.  With log-uniform request sizes those copies
+// are a fifth of the copies and most of the bytes (serving capacity: 4-5 %
+// more requests/s at 512 KiB than at 128 KiB).
+constexpr size_t kDmaMinBytes = 512 << 10;
 constexpr u32 kCopyChunkWords = 8192;  // 32 KiB per table entry
 
 struct CopyChunk {

@@ -298,7 +298,7 @@ cumodp_err cumodp_server_replay(cumodp_server *s, long long count, const double 
  * operands lie in registered memory is copied to the device straight from
  * there, and a result buffer that lies in registered memory receives the
  * result straight from the device: no copy through the server's pinned slabs
- * and no host memcpy on either side.  Copies under 128 KiB are made by one
+ * and no host memcpy on either side.  Copies under 512 KiB are made by one
  * kernel per batch that reads or writes the mapped memory (a copy-engine
  * transfer costs about 4 us of its own, whatever its size); larger ones by
  * the copy engines.  The caller leaves such operands
